@@ -1,0 +1,369 @@
+"""Benchmark of the moment-regularized D2Q9 cylinder step (one JSON line on rank 0).
+
+Workload: the 2048 x 512 cylinder case (D = 80 at (320.0, 256.5), Re = 200, U = 0.04,
+free-slip walls, seeded-noise start); one bench step = one lattice time step over the whole
+grid, forces reduced every step.  Synthetic, seeded inputs only.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision 32|64] [--case mid|large|small]
+
+`value` is the aggregate MLUPS of the headline precision (FP32 deviation form unless
+--precision 64), each timed step preceded by an L2 flush (a 256 MiB write) outside its CUDA
+event pair; `e2e` is the same metric through the public C ABI with host buffers: upload the
+initial populations, K steps, drain the force history every 100 steps, read the last step's
+rho/ux/uy back.  Under torchrun every rank runs an independent replica (its own seed) on its
+own GPU: weak scaling, no collective on the data path; times are max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_LU = {64: 144, 32: 72}       # one read + one write of 9 populations
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", type=int, choices=[32, 64], default=None)
+    ap.add_argument("--case", choices=["mid", "large", "small"], default="mid")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_case(name, seed):
+    from mrlbm_2d_b200.config import case_large, case_mid, case_small
+    c = {"mid": case_mid, "large": case_large, "small": case_small}[name]()
+    return c.replace(seed=seed)
+
+
+def case_desc(name, cfg):
+    return {"workload": f"cylinder {name}: {cfg.nx}x{cfg.ny}, D={2 * cfg.r_c:g} at ({cfg.x_c:g},{cfg.y_c:g}), "
+                        f"Re={cfg.Re:g}, U={cfg.uo:g}, free-slip walls, zero-gradient outlet, seeded noise",
+            "nx": cfg.nx, "ny": cfg.ny, "nodes": cfg.nx * cfg.ny}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        sm, mx, reasons = [], None, set()
+        for t, line in self.lines:
+            if t < t0 or t > t1:
+                continue
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profiles(precision, case_name):
+    """DRAM bytes per lattice update of the step kernel from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "step_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        e = d.get(f"fp{precision}")
+        return float(e["dram_bytes_per_lu"]), e.get("source", "profiles/step_traffic.json")
+    except Exception:
+        return None, None
+
+
+def cpu_baseline(case_name, seconds, threads=None):
+    """The oracle (reference restatement, OpenMP loops, serial streaming) on the host cores:
+    a bounded sample of the same workload, wall-clock MLUPS."""
+    import oracle
+    cfg = make_case(case_name, 1234)
+    n = threads or os.cpu_count() or 1
+    oracle.set_threads(n)
+    o = oracle.Oracle(cfg.replace(num_threads=n), threads=n)
+    o.step(2)                                   # warm-up
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 100000:
+            break
+    nodes = cfg.nx * cfg.ny
+    o.close()
+    return {"value": nodes * steps / el / 1e6, "unit": "MLUPS", "cores": n, "kind": "port",
+            "sample": f"{steps} steps of the {cfg.nx}x{cfg.ny} case ({el:.1f} s wall clock, "
+                      f"FP64 C++ restatement of 2d_mrlbm.f90 with its OpenMP loops and serial streaming)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    import oracle
+    cfg = make_case(args.case, 1234)
+    n = os.cpu_count() or 1
+    oracle.set_threads(n)
+    o = oracle.Oracle(cfg.replace(num_threads=n), threads=n)
+    o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    el = time.perf_counter() - t0
+    nodes = cfg.nx * cfg.ny
+    v = nodes * args.steps / el / 1e6
+    line = {"metric": "D2Q9 MLUPS", "value": v, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": case_desc(args.case, cfg), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": n, "kind": "port",
+                             "sample": f"{args.steps} timed steps after {args.warmup} warm-up, full grid"},
+            "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from mrlbm_2d_b200 import build
+    if rank == 0:
+        build.build()
+    if world > 1:
+        dist.barrier()
+    import mrlbm_2d_b200 as m
+
+    cfg = make_case(args.case, 1234 + rank)
+    nodes = cfg.nx * cfg.ny
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def time_device(precision, K, W, sampler=None):
+        sim = m.Simulation(cfg, precision=precision, device=dev)
+        sim.set_stream(stream.cuda_stream)
+        sim.step(W)
+        # untimed soak so clock samples see the steady state
+        t_soak = time.time()
+        while time.time() - t_soak < 1.0:
+            sim.step(50)
+            torch.cuda.synchronize()
+        sim.forces()
+        launches0 = sim.launch_count()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        barrier()
+        t_wall0 = time.time()
+        for s in range(K):
+            flush.zero_()
+            starts[s].record(stream)
+            sim.step(1)
+            ends[s].record(stream)
+        barrier()
+        t_wall1 = time.time()
+        launches = sim.launch_count() - launches0
+        per = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+        total_ms = sum(per)
+        # unflushed back-to-back steps (state may stay partly in L2), for reference
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        noflush_ms = e0.elapsed_time(e1) / K
+        st = sim.status()
+        _, fd, fl, _ = sim.forces()
+        sim.close()
+        assert st == 0, "device error flag set"
+        assert np.all(np.isfinite(fd)), "non-finite forces"
+        return total_ms, launches, per, noflush_ms, (t_wall0, t_wall1)
+
+    def time_e2e(precision, K):
+        """Public-API run with host buffers: load state, K steps, force drains, fields back."""
+        sim = m.Simulation(cfg, precision=precision, device=dev)
+        f0 = sim.get_state()                 # host copy of the seeded initial populations
+        sim.step(3)
+        sim.forces()
+        barrier()
+        t0 = time.perf_counter()
+        sim.load_state(f0, iter=0)
+        nrec = 0
+        for s0 in range(0, K, 100):
+            n = min(100, K - s0)
+            sim.step(n, macro=(s0 + n == K))
+            nrec += len(sim.forces()[0])
+        mac = sim.macro()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        el = max_over_ranks(el)
+        sim.close()
+        elem = 8
+        h2d = nodes * 9 * elem / K
+        d2h = (nrec * 4 * 8 + 3 * nodes * 8) / K
+        del mac
+        return {"value": world * nodes * K / el / 1e6, "unit": "MLUPS",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "note": "load_state(host f) + K x step + force drain every 100 steps + rho/ux/uy of the "
+                        "last step, wall clock, max over ranks"}
+
+    precisions = [args.precision] if args.precision else ([32, 64] if _fp32_available(m, cfg) else [64])
+    head = precisions[0]
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    results = {}
+    for prec in precisions:
+        total_ms, launches, per, noflush_ms, win = time_device(prec, args.steps, args.warmup)
+        total_ms = max_over_ranks(total_ms)
+        results[prec] = (total_ms, launches, per, noflush_ms, win)
+    if sampler:
+        time.sleep(0.3)
+        sampler.stop()
+    e2e = time_e2e(head, args.steps)
+
+    total_ms, launches, per, noflush_ms, win = results[head]
+    ms_step = total_ms / args.steps
+    value = world * nodes * args.steps / (total_ms * 1e-3) / 1e6
+    peak, peak_kind = hbm_peak()
+    avg_launch_s = (total_ms / args.steps) * 1e-3
+    achieved = BYTES_PER_LU[head] * nodes / avg_launch_s / 1e9
+    tr, tr_src = traffic_from_profiles(head, args.case)
+    line = {
+        "metric": "D2Q9 MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if head == 32 else "f64", "data": "synthetic (seeded noise init)",
+        "config": dict(case_desc(args.case, cfg), precision=f"fp{head}", l2="flushed before every timed step",
+                       parallelism=f"replicas{world}"),
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (tr * nodes) if tr is not None else None,
+                     "algorithmic_bytes_per_launch": BYTES_PER_LU[head] * nodes,
+                     "traffic_source": tr_src},
+        "e2e": e2e,
+    }
+    for prec in precisions:
+        t, _, _, nf, _ = results[prec]
+        line[f"fp{prec}"] = {"mlups": world * nodes * args.steps / (t * 1e-3) / 1e6, "ms_per_step": t / args.steps,
+                             "ms_per_step_unflushed": nf,
+                             "hbm_gbs_alg": BYTES_PER_LU[prec] * nodes / (t / args.steps * 1e-3) / 1e9}
+    if 32 in results and 64 in results:
+        line["fp32_over_fp64"] = results[64][0] / results[32][0]
+    if sampler:
+        t0 = min(r[4][0] for r in results.values()) - 1.2
+        t1 = max(r[4][1] for r in results.values())
+        line["clocks"] = sampler.summary(t0, t1)
+    if world > 1:
+        dist.barrier()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(args.case, args.cpu_sample_seconds)
+        except Exception as ex:                 # reported, never fatal
+            line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def _fp32_available(m, cfg):
+    try:
+        s = m.Simulation(cfg.replace(nx=64, ny=32, x_c=20.0, y_c=16.5, r_c=4.0), precision=32)
+        s.step(1)
+        s.close()
+        return True
+    except Exception:
+        return False
+
+
+if __name__ == "__main__":
+    sys.exit(main())

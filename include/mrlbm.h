@@ -1,0 +1,181 @@
+/*
+ * mrlbm.h -- C ABI of the B200-native moment-regularized D2Q9 cylinder-flow step.
+ *
+ * The reference (sakthi-lbm/mrlbm_2d) is one Fortran program whose time-loop body
+ * (2d_mrlbm.f90:231-535) is the hot path.  It has no library interface: all state is
+ * program-scope globals (2d_mrlbm.f90:1-73) and every routine is an internal subroutine
+ * (2d_mrlbm.f90:557).  This header is the seam a Fortran host (ISO_C_BINDING), a C/C++
+ * driver or Python ctypes binds to; each entry point names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every function returns int: 0 = OK, >0 = configuration / geometry error,
+ *     <0 = CUDA error or a device-side error flag (NaN / non-positive density).
+ *   - Arrays are contiguous, Fortran order: a field v(nx,ny) has v(i,j) at (i-1)+nx*(j-1);
+ *     populations f(nx,ny,0:8) have f(i,j,k) at (i-1)+nx*(j-1)+nx*ny*k, exactly the
+ *     reference's f(1:nx,1:ny,0:q-1) (2d_mrlbm.f90:2285).
+ *   - The handle owns all device memory.  Host arrays passed in are borrowed for the
+ *     duration of the call only.  One host thread per handle; calls are ordered on the
+ *     handle's stream; every call that returns host data synchronises that stream.
+ *   - D2Q9 order k = 0 rest, 1 +x, 2 +y, 3 -x, 4 -y, 5 (+,+), 6 (-,+), 7 (-,-), 8 (+,-)
+ *     (2d_mrlbm.f90:129-131).
+ */
+#ifndef MRLBM_H
+#define MRLBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------- */
+#define MRLBM_OK              0
+#define MRLBM_EINVAL          1   /* bad argument or configuration value              */
+#define MRLBM_ENAMELIST       2   /* input.dat could not be read (2d_mrlbm.f90:2235-2238) */
+#define MRLBM_EGEOMETRY       3   /* unhandled boundary label / stencil on a non-fluid node */
+#define MRLBM_EUNSUPPORTED    4   /* flag combination the reference leaves undefined   */
+#define MRLBM_ESTATE          5   /* call out of order (e.g. step before init)          */
+#define MRLBM_ECUDA          -1   /* CUDA runtime error                                  */
+#define MRLBM_EDEVICE_NAN    -2   /* device flag: NaN or non-positive density           */
+#define MRLBM_ENODEVICE      -3   /* no CUDA device / kernels not loadable              */
+
+/* ---- precision of a handle ----------------------------------------------------- */
+#define MRLBM_FP64  64            /* populations and arithmetic in FP64 (reference form) */
+#define MRLBM_FP32  32            /* populations stored as FP32 deviations from w_k      */
+
+/* ---- extension switches (0 is always the reference behaviour) -------------------- */
+#define MRLBM_GEOM_REFERENCE   0  /* nx,ny,centre,radius from ncy and L_* (2d_mrlbm.f90:86-92, 946-948) */
+#define MRLBM_GEOM_EXPLICIT    1  /* nx,ny,x_c,y_c,r_c taken as given (real-valued centre)      */
+#define MRLBM_WALL_REFERENCE   0  /* no-slip regularized walls when !y_periodic (2d_mrlbm.f90:263-272, 1305-1359) */
+#define MRLBM_WALL_FREESLIP    1  /* free-slip: halfway specular reflection in streaming        */
+#define MRLBM_LABEL15_REJECT   0  /* label 15 has empty link rows in the reference (2d_mrlbm.f90:2008) */
+#define MRLBM_LABEL15_ALLNINE  1  /* label 15 closes over all nine links                        */
+#define MRLBM_NU_REFERENCE     0  /* nu = U * 2 r_cyl / Re, r_cyl = max boundary radius (2d_mrlbm.f90:134) */
+#define MRLBM_NU_DIAMETER      1  /* nu = U * 2 r_c / Re (nominal diameter)                     */
+#define MRLBM_INIT_REFERENCE   0  /* rho = 1, u = 0, f = w (2d_mrlbm.f90:1220-1235)             */
+#define MRLBM_INIT_NOISE       1  /* rho = 1, u = (U,0) + seeded Gaussian noise, regularized equilibrium */
+
+/*
+ * Run configuration.  The first block mirrors the reference namelists
+ * DomainSize, Cylinder, Numbers, Parallel, Controls and LogicalControls
+ * (2d_mrlbm.f90:2227-2233, input.dat:1-45); the last block holds the extensions
+ * a BASELINE-style case needs.  Field order is part of the ABI.
+ */
+typedef struct mrlbm_config {
+    double   x_c, y_c, r_c;          /* cylinder centre / classification radius (lattice units, node (i,j) sits at (i,j)) */
+    double   Re, uo, rho_infty;      /* &Numbers Re; &Controls uo, rho_infty */
+    double   noise_amp;              /* INIT_NOISE: noise standard deviation as a fraction of uo */
+    uint64_t seed;                   /* INIT_NOISE: counter-based RNG key */
+    int32_t  nx, ny;                 /* &DomainSize (overwritten from ncy/L_* in GEOM_REFERENCE) */
+    int32_t  channel_with_cylinder;
+    int32_t  ncy, L_front, L_back, L_top, L_bot;                     /* &Cylinder */
+    int32_t  iplot, max_iter, isave, irestart, statsbegin, statsend, iplotstats; /* &Controls */
+    int32_t  num_threads, lattice_type;                              /* &Parallel, &DomainSize */
+    int32_t  post_process, x_periodic, y_periodic, channel_with_square;
+    int32_t  incomp_bc, incomp_bulk, vel_interp, mom_interp, rotated_coordinate;
+    int32_t  strong_mass_bc, eq_mass_bc, weak_mass_bc;               /* &LogicalControls */
+    int32_t  geometry_mode, wall_mode, label15_rule, nu_length, init_mode;
+    int32_t  reserved;
+} mrlbm_config;
+
+/* Boundary-node geometry as the reference builds it in get_coord (2d_mrlbm.f90:931-1156). */
+typedef struct mrlbm_geometry_info {
+    int32_t nx, ny, nbct;            /* nbct = number of curved-wall boundary nodes (2d_mrlbm.f90:1004) */
+    int32_t n_label15;               /* boundary nodes whose quadrant label is 15 */
+    double  x_c, y_c, r_c, r_cyl;    /* r_cyl = max boundary-node radius (2d_mrlbm.f90:1038-1050) */
+    double  nu, omega;               /* 2d_mrlbm.f90:133-135 */
+} mrlbm_geometry_info;
+
+typedef struct mrlbm_handle mrlbm_handle;
+
+/* sizeof(mrlbm_config), for bindings that mirror the struct (ctypes, ISO_C_BINDING). */
+size_t mrlbm_config_sizeof(void);
+
+/* Reference defaults: the values of the shipped input.dat (input.dat:1-45). */
+int mrlbm_config_defaults(mrlbm_config* cfg);
+
+/* Read the six namelist groups of an input.dat file into cfg, in the order the reference
+ * reads them; replaces read_input_file (2d_mrlbm.f90:2222-2275).  Returns MRLBM_ENAMELIST
+ * where the reference prints "Error while reading input.dat file..." and stops. */
+int mrlbm_config_from_namelist(const char* path, mrlbm_config* cfg);
+
+/* Fill nx, ny, x_c, y_c, r_c from ncy and L_* as the reference does
+ * (2d_mrlbm.f90:86-92 and 946-948).  No-op unless geometry_mode == GEOM_REFERENCE. */
+int mrlbm_config_resolve_geometry(mrlbm_config* cfg);
+
+/* Build geometry and device state for one case; replaces the setup part of the main
+ * program (2d_mrlbm.f90:83-214: allocate_memory, get_coord, weights, nu/omega, Hermite
+ * and rotated tables, finding_incoming_outgoing_pops).  precision = MRLBM_FP64 or
+ * MRLBM_FP32.  The initial state follows cfg->init_mode (initialize, 2d_mrlbm.f90:1220).
+ * device = -1 creates a host-only handle (configuration and geometry queries only; the
+ * stepping and state calls then return MRLBM_ENODEVICE). */
+int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handle** out);
+int mrlbm_destroy(mrlbm_handle* h);
+
+/* Last error text of a handle (or of the last failed mrlbm_create when h == NULL). */
+int mrlbm_last_error(const mrlbm_handle* h, char* buf, size_t len);
+
+/* Sticky device status: MRLBM_OK or MRLBM_EDEVICE_NAN.  Synchronises. */
+int mrlbm_status(mrlbm_handle* h);
+
+/* Run subsequent work on a caller-owned cudaStream_t (NULL = the handle's own stream). */
+int mrlbm_set_stream(mrlbm_handle* h, void* cuda_stream);
+
+int mrlbm_get_geometry_info(const mrlbm_handle* h, mrlbm_geometry_info* info);
+
+/* Per boundary node l = 1..nbct, in the reference's order (i-major, j-minor,
+ * 2d_mrlbm.f90:1007-1036): bou_i, bou_j, label_bc (int32[nbct]); delta_uk (double[nbct],
+ * 2d_mrlbm.f90:1089-1091); ref_xy = x_ref1..4,y_ref1..4 (double[8*nbct], point-major);
+ * stencil = i_p2,j_p2,i_p3,j_p3,i_p4,j_p4 (int32[24*nbct], 2d_mrlbm.f90:1099-1129).
+ * Any pointer may be NULL. */
+int mrlbm_get_boundary_nodes(const mrlbm_handle* h, int32_t* bou_i, int32_t* bou_j,
+                             int32_t* label_bc, double* delta_uk, double* ref_xy,
+                             int32_t* stencil);
+
+/* Node classes isfluid/issolid/isbound (int32[nx*ny] each, 2d_mrlbm.f90:968-1002). */
+int mrlbm_get_node_classes(const mrlbm_handle* h, int32_t* isfluid, int32_t* issolid,
+                           int32_t* isbound);
+
+/* Replace the state by post-streaming populations f(nx,ny,0:8) (what read_restart_file
+ * loads, 2d_mrlbm.f90:2204-2220) and set the iteration counter. */
+int mrlbm_load_state(mrlbm_handle* h, const double* f, int32_t iter);
+
+/* Post-streaming populations after the last step (the f of write_restart_file,
+ * 2d_mrlbm.f90:2186-2202). */
+int mrlbm_get_state(mrlbm_handle* h, double* f);
+
+/* Per-row inlet velocity u_in(1..ny) replacing the uniform uinlet of 2d_mrlbm.f90:258
+ * (extension; NULL restores the uniform inlet). */
+int mrlbm_set_inlet_profile(mrlbm_handle* h, const double* u_in);
+
+/* Advance nsteps time steps (2d_mrlbm.f90:229-535 per step).  Forces are reduced on
+ * the steps post_process and statsbegin <= iter <= statsend select (2d_mrlbm.f90:461-502).
+ * With flags & MRLBM_STEP_MACRO the last step also stores its post-boundary-condition
+ * macroscopic fields for mrlbm_get_macro. */
+#define MRLBM_STEP_MACRO   1
+int mrlbm_step(mrlbm_handle* h, int32_t nsteps, int32_t flags);
+
+/* Current iteration number (the reference's iter after the last step). */
+int mrlbm_get_iter(const mrlbm_handle* h, int32_t* iter);
+
+/* Macroscopic fields of the last step run with MRLBM_STEP_MACRO, after the Dirichlet and
+ * regularized boundary conditions and before collision (the values write_function_plot3d
+ * writes, 2d_mrlbm.f90:371-386).  Any pointer may be NULL; mxx/myy/mxy are the Hermite
+ * second moments the collision starts from. */
+int mrlbm_get_macro(mrlbm_handle* h, double* rho, double* ux, double* uy,
+                    double* mxx, double* myy, double* mxy);
+
+/* Drain the force history: one record per stats step (the lines of forces_time.dat,
+ * 2d_mrlbm.f90:492-494) plus the inlet-column density sum sum(rho(1,:))
+ * (2d_mrlbm.f90:359).  Copies up to cap records, returns the count in *n and removes them. */
+int mrlbm_get_forces(mrlbm_handle* h, int32_t* iter, double* f_drag, double* f_lift,
+                     double* rho_inlet_sum, int32_t cap, int32_t* n);
+
+/* Number of kernel launches issued by this handle so far (all kinds). */
+int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MRLBM_H */

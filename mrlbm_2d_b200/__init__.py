@@ -1,0 +1,9 @@
+"""B200-native moment-regularized D2Q9 cylinder-flow step (drop-in for mrlbm_2d's hot path).
+
+`Config` mirrors the reference's input.dat namelists; `Simulation` drives one case through
+the C ABI of libmrlbm.so (include/mrlbm.h).  The CUDA library is required: there is no CPU
+fallback.
+"""
+from .config import Config  # noqa: F401
+from .api import (FP32, FP64, MrlbmError, Simulation, config_from_namelist,  # noqa: F401
+                  load_library)

@@ -1,0 +1,229 @@
+"""ctypes binding of include/mrlbm.h and a thin Simulation object over it.
+
+The reference's "API" is its main program driven by input.dat (2d_mrlbm.f90:77-555).
+`Simulation` mirrors that run: it is created from the same configuration, advances with
+`step` (one call per main-loop iteration or a batch of them), and hands back the outputs the
+reference writes: macroscopic fields (the PLOT3D function file, 2d_mrlbm.f90:2163-2184), the
+post-streaming populations (restart.dat, 2d_mrlbm.f90:2186-2202) and the force history
+(data_mean/forces_time.dat, 2d_mrlbm.f90:492-494).  Errors raise `MrlbmError` with the
+library's status code, as the reference stops on bad input (2d_mrlbm.f90:2235-2238).
+
+There is no CPU fallback: without the compiled library or a CUDA device every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .config import Config
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmrlbm.so")
+
+FP64, FP32 = 64, 32
+STEP_MACRO = 1
+
+EXPORTED = [
+    "mrlbm_config_sizeof", "mrlbm_config_defaults", "mrlbm_config_from_namelist", "mrlbm_config_resolve_geometry",
+    "mrlbm_create", "mrlbm_destroy", "mrlbm_last_error", "mrlbm_status", "mrlbm_set_stream",
+    "mrlbm_get_geometry_info", "mrlbm_get_boundary_nodes", "mrlbm_get_node_classes",
+    "mrlbm_load_state", "mrlbm_get_state", "mrlbm_set_inlet_profile", "mrlbm_step",
+    "mrlbm_get_iter", "mrlbm_get_macro", "mrlbm_get_forces", "mrlbm_get_launch_count",
+]
+
+
+class MrlbmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mrlbm error {code}: {msg}")
+        self.code = code
+
+
+class GeometryInfo(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nbct", ctypes.c_int32),
+                ("n_label15", ctypes.c_int32), ("x_c", ctypes.c_double), ("y_c", ctypes.c_double),
+                ("r_c", ctypes.c_double), ("r_cyl", ctypes.c_double), ("nu", ctypes.c_double),
+                ("omega", ctypes.c_double)]
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libmrlbm.so (built by `python -m mrlbm_2d_b200.build`).  Raises if missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise MrlbmError(-3, f"{p} is not built; run `python -m mrlbm_2d_b200.build`")
+    L = ctypes.CDLL(p)
+    vp, i32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
+    sig = {
+        "mrlbm_config_defaults": [vp],
+        "mrlbm_config_from_namelist": [ctypes.c_char_p, vp],
+        "mrlbm_config_resolve_geometry": [vp],
+        "mrlbm_create": [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)],
+        "mrlbm_destroy": [vp],
+        "mrlbm_last_error": [vp, ctypes.c_char_p, ctypes.c_size_t],
+        "mrlbm_status": [vp],
+        "mrlbm_set_stream": [vp, vp],
+        "mrlbm_get_geometry_info": [vp, vp],
+        "mrlbm_get_boundary_nodes": [vp] * 7,
+        "mrlbm_get_node_classes": [vp] * 4,
+        "mrlbm_load_state": [vp, vp, i32],
+        "mrlbm_get_state": [vp, vp],
+        "mrlbm_set_inlet_profile": [vp, vp],
+        "mrlbm_step": [vp, i32, i32],
+        "mrlbm_get_iter": [vp, vp],
+        "mrlbm_get_macro": [vp] * 7,
+        "mrlbm_get_forces": [vp, vp, vp, vp, vp, i32, vp],
+        "mrlbm_get_launch_count": [vp, vp],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    del dbl
+    if path is None:
+        _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def config_from_namelist(path):
+    """Read input.dat the way read_input_file does (2d_mrlbm.f90:2222-2275)."""
+    L = load_library()
+    c = Config()
+    L.mrlbm_config_defaults(ctypes.byref(c))
+    rc = L.mrlbm_config_from_namelist(os.fsencode(path), ctypes.byref(c))
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        L.mrlbm_last_error(None, buf, 512)
+        raise MrlbmError(rc, buf.value.decode())
+    return c
+
+
+class Simulation:
+    """One cylinder-flow case resident on one GPU."""
+
+    def __init__(self, cfg, precision=FP64, device=0):
+        self._L = load_library()
+        self._h = ctypes.c_void_p()
+        rc = self._L.mrlbm_create(ctypes.byref(cfg), int(precision), int(device), ctypes.byref(self._h))
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self._L.mrlbm_last_error(None, buf, 1024)
+            raise MrlbmError(rc, buf.value.decode())
+        self.precision = precision
+        info = GeometryInfo()
+        self._L.mrlbm_get_geometry_info(self._h, ctypes.byref(info))
+        self.info = info
+        self.nx, self.ny, self.nbct = info.nx, info.ny, info.nbct
+
+    # -- lifetime --------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.mrlbm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self._L.mrlbm_last_error(self._h, buf, 1024)
+            raise MrlbmError(rc, buf.value.decode())
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- stepping --------------------------------------------------------------------
+    def step(self, n=1, macro=False):
+        self._check(self._L.mrlbm_step(self._h, int(n), STEP_MACRO if macro else 0))
+
+    def set_stream(self, stream_ptr):
+        self._check(self._L.mrlbm_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def status(self):
+        return self._L.mrlbm_status(self._h)
+
+    @property
+    def iter(self):
+        it = ctypes.c_int32()
+        self._check(self._L.mrlbm_get_iter(self._h, ctypes.byref(it)))
+        return it.value
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        self._check(self._L.mrlbm_get_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    # -- state and outputs -----------------------------------------------------------
+    def get_state(self):
+        """Post-streaming populations f as an (nx, ny, 9) array, f[i-1, j-1, k]."""
+        f = np.empty(self.nx * self.ny * 9)
+        self._check(self._L.mrlbm_get_state(self._h, _ptr(f)))
+        return f.reshape(9, self.ny, self.nx).transpose(2, 1, 0)
+
+    def load_state(self, f, iter=0):
+        a = np.asfortranarray(np.asarray(f, dtype=np.float64).reshape(self.nx, self.ny, 9))
+        flat = np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()
+        self._check(self._L.mrlbm_load_state(self._h, _ptr(flat), int(iter)))
+
+    def set_inlet_profile(self, u_in):
+        if u_in is None:
+            self._check(self._L.mrlbm_set_inlet_profile(self._h, None))
+            return
+        a = np.ascontiguousarray(u_in, dtype=np.float64)
+        assert a.size == self.ny
+        self._check(self._L.mrlbm_set_inlet_profile(self._h, _ptr(a)))
+
+    def macro(self):
+        """dict of (nx, ny) arrays rho, ux, uy, mxx, myy, mxy of the last MACRO step."""
+        N = self.nx * self.ny
+        outs = [np.empty(N) for _ in range(6)]
+        self._check(self._L.mrlbm_get_macro(self._h, *[_ptr(o) for o in outs]))
+        names = ["rho", "ux", "uy", "mxx", "myy", "mxy"]
+        return {n: o.reshape(self.ny, self.nx).T for n, o in zip(names, outs)}
+
+    def forces(self, cap=1 << 22):
+        """Drain the force history: (iter, F_drag_net, F_lift_net, sum(rho(1,:)))."""
+        it = np.empty(cap, np.int32)
+        fd, fl, rin = np.empty(cap), np.empty(cap), np.empty(cap)
+        n = ctypes.c_int32()
+        self._check(self._L.mrlbm_get_forces(self._h, _ptr(it), _ptr(fd), _ptr(fl), _ptr(rin), cap,
+                                             ctypes.byref(n)))
+        m = n.value
+        return it[:m].copy(), fd[:m].copy(), fl[:m].copy(), rin[:m].copy()
+
+    # -- geometry --------------------------------------------------------------------
+    def boundary_nodes(self):
+        nb = self.nbct
+        bi, bj, lab = (np.empty(nb, np.int32) for _ in range(3))
+        delta = np.empty(nb)
+        ref = np.empty(8 * nb)
+        sten = np.empty(24 * nb, np.int32)
+        self._check(self._L.mrlbm_get_boundary_nodes(self._h, _ptr(bi), _ptr(bj), _ptr(lab), _ptr(delta),
+                                                     _ptr(ref), _ptr(sten)))
+        return {"bou_i": bi, "bou_j": bj, "label_bc": lab, "delta_uk": delta,
+                "ref_xy": ref.reshape(nb, 8), "stencil": sten.reshape(nb, 24)}
+
+    def node_classes(self):
+        N = self.nx * self.ny
+        a, b, c = (np.empty(N, np.int32) for _ in range(3))
+        self._check(self._L.mrlbm_get_node_classes(self._h, _ptr(a), _ptr(b), _ptr(c)))
+        return {k: v.reshape(self.ny, self.nx).T for k, v in zip(["isfluid", "issolid", "isbound"], (a, b, c))}

@@ -1,0 +1,556 @@
+// capi.cpp -- the extern "C" surface of include/mrlbm.h: handle lifetime, device memory,
+// state transfer, the time-step loop and the force history ring.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mrlbm.h"
+#include "geometry.h"
+#include "step_params.h"
+
+using namespace mrlbm;
+
+namespace {
+thread_local std::string g_create_error;
+constexpr int RING_CAP = 8192;                // stats records buffered on the device
+}
+
+struct mrlbm_handle {
+    mrlbm_config cfg{};
+    int precision = MRLBM_FP64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    Geometry geo;
+    Lattice64 lat{};
+    double nu = 0, omega = 0;
+    int closure = CLOSURE_STRONG;
+    Layout L{};
+    size_t elem = 8;
+    void* buf[2] = {nullptr, nullptr};
+    int cur = 0;
+    void* d_bgeo = nullptr;
+    int* d_bint = nullptr;
+    int* d_boxmap = nullptr;
+    double* d_partials = nullptr;
+    unsigned* d_counter = nullptr;
+    double* d_ring = nullptr;
+    int ring_n = 0;
+    int* d_err = nullptr;
+    double* d_macro = nullptr;
+    double* d_uin = nullptr;
+    bool has_uin = false;
+    double* h_ring = nullptr;                 // pinned
+    std::vector<double> hist;                 // drained records, REC_WORDS each
+    int iter = 0;
+    int tile_cfg = 1;
+    long long launches = 0;
+    std::string err;
+    DevConsts dc{};
+    bool host_only = false;
+};
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            h->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+            return MRLBM_ECUDA;                                                            \
+        }                                                                                  \
+    } while (0)
+
+namespace {
+
+int fail(mrlbm_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+// Streaming-source slot of population (i,j,k) in the padded buffer.
+inline int64_t slot_of(const mrlbm_handle* h, int i, int j, int k) {
+    const mrlbm_config& c = h->cfg;
+    SrcSlot s = stream_source(h->L.nx, h->L.ny, i, j, k, c.x_periodic != 0, c.y_periodic != 0,
+                              c.wall_mode == MRLBM_WALL_FREESLIP);
+    return h->L.at(s.i, s.j, s.k);
+}
+
+// Deviation-form constants, computed in FP64 from the reference weights and tables.
+void make_dev_consts(mrlbm_handle* h) {
+    const Lattice64& L = h->lat;
+    DevConsts& d = h->dc;
+    double sw = 0, cxx = 0, cyy = 0;
+    for (int k = 0; k < Q; ++k) { sw += L.w[k]; cxx += L.w[k] * L.hxx[k]; cyy += L.w[k] * L.hyy[k]; }
+    d.eps_mass = (float)(sw - 1.0);
+    d.cxx = (float)cxx;
+    d.cyy = (float)cyy;
+    const int masks[4] = {(1 << 0) | (1 << 1) | (1 << 2) | (1 << 4) | (1 << 5) | (1 << 8),
+                          (1 << 0) | (1 << 2) | (1 << 3) | (1 << 4) | (1 << 6) | (1 << 7),
+                          (1 << 0) | (1 << 1) | (1 << 2) | (1 << 3) | (1 << 5) | (1 << 6),
+                          (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | (1 << 8)};
+    for (int e = 0; e < 4; ++e) {
+        double a = 0, bx = 0, by = 0, bxy = 0;
+        for (int k = 0; k < Q; ++k)
+            if ((masks[e] >> k) & 1) { a += L.w[k]; bx += L.w[k] * L.hxx[k]; by += L.w[k] * L.hyy[k]; bxy += L.w[k] * L.hxy[k]; }
+        d.wI[e] = (float)a; d.swxx[e] = (float)bx; d.swyy[e] = (float)by; d.swxy[e] = (float)bxy;
+    }
+    int incs[16], outs[16];
+    link_tables(h->cfg.label15_rule, incs, outs);
+    for (int l = 0; l < 16; ++l) {
+        double a = 0;
+        for (int k = 0; k < Q; ++k) if ((incs[l] >> k) & 1) a += L.w[k];
+        d.lab_wI[l] = (float)a;
+    }
+}
+
+int upload_state(mrlbm_handle* h, const double* f) {
+    const int nx = h->L.nx, ny = h->L.ny;
+    const size_t N = (size_t)nx * ny;
+    const int64_t total = h->L.total();
+    if (h->precision == MRLBM_FP64) {
+        std::vector<double> b((size_t)total, 0.0);
+        for (int k = 0; k < Q; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i)
+                    b[(size_t)slot_of(h, i, j, k)] = f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k];
+        CK(cudaMemcpyAsync(h->buf[0], b.data(), (size_t)total * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->buf[1], b.data(), (size_t)total * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    } else {
+        std::vector<float> b((size_t)total, 0.0f);
+        for (int k = 0; k < Q; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i)
+                    b[(size_t)slot_of(h, i, j, k)] =
+                        (float)(f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k] - h->lat.w[k]);
+        CK(cudaMemcpyAsync(h->buf[0], b.data(), (size_t)total * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->buf[1], b.data(), (size_t)total * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->cur = 0;
+    return MRLBM_OK;
+}
+
+int drain_ring(mrlbm_handle* h) {
+    if (h->ring_n == 0) return MRLBM_OK;
+    CK(cudaMemcpyAsync(h->h_ring, h->d_ring, (size_t)h->ring_n * REC_WORDS * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->hist.insert(h->hist.end(), h->h_ring, h->h_ring + (size_t)h->ring_n * REC_WORDS);
+    h->ring_n = 0;
+    return MRLBM_OK;
+}
+
+template <class T>
+void fill_common(mrlbm_handle* h, StepParams<T>& p) {
+    const mrlbm_config& c = h->cfg;
+    p.L = h->L;
+    for (int k = 0; k < Q; ++k) p.w[k] = (T)h->lat.w[k];
+    p.hm = (T)h->lat.hm;
+    p.hp = (T)h->lat.hp;
+    p.omega = (T)h->omega;
+    p.omega1 = (T)(1.0 - h->omega);
+    p.uinlet = (T)c.uo;
+    p.vinlet = (T)0.0;
+    p.u_in = nullptr;
+    p.xper = c.x_periodic != 0;
+    p.yper = c.y_periodic != 0;
+    p.freeslip = c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic;
+    p.walls_ref = c.wall_mode == MRLBM_WALL_REFERENCE && !c.y_periodic;
+    p.incomp_bc = c.incomp_bc != 0;
+    p.incomp_bulk = c.incomp_bulk != 0;
+    p.nb = h->geo.nb;
+    p.bint = h->d_bint;
+    p.bgeo = (const T*)h->d_bgeo;
+    p.closure = h->closure;
+    p.vel_interp = c.vel_interp != 0;
+    p.mom_interp = c.mom_interp != 0;
+    p.box_x0 = h->geo.box_x0;
+    p.box_y0 = h->geo.box_y0;
+    p.box_w = h->geo.box_w;
+    p.box_h = h->geo.box_h;
+    p.boxmap = h->d_boxmap;
+    p.label15_allnine = c.label15_rule == MRLBM_LABEL15_ALLNINE;
+    p.partials = h->d_partials;
+    p.counter = h->d_counter;
+    p.node_force = nullptr;
+    p.errflag = h->d_err;
+    p.dc = h->dc;
+}
+
+int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
+    const int tc = h->tile_cfg;
+    int rc;
+    if (h->precision == MRLBM_FP64) {
+        StepParams<double> p{};
+        fill_common(h, p);
+        p.src = (const double*)h->buf[h->cur];
+        p.dst = (double*)h->buf[1 - h->cur];
+        p.u_in = h->has_uin ? h->d_uin : nullptr;
+        p.zero_solid_u = plot;
+        p.do_stats = stats;
+        p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
+        p.iter = h->iter;
+        p.macro = macro ? h->d_macro : nullptr;
+        rc = launch_step_f64(p, tc, h->stream);
+    } else {
+        StepParams<float> p{};
+        fill_common(h, p);
+        p.src = (const float*)h->buf[h->cur];
+        p.dst = (float*)h->buf[1 - h->cur];
+        p.u_in = h->has_uin ? (const float*)h->d_uin : nullptr;
+        p.zero_solid_u = plot;
+        p.do_stats = stats;
+        p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
+        p.iter = h->iter;
+        p.macro = macro ? h->d_macro : nullptr;
+        rc = launch_step_f32(p, tc, h->stream);
+    }
+    ++h->launches;
+    if (rc != 0) {
+        h->err = std::string("kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
+        return MRLBM_ECUDA;
+    }
+    h->cur ^= 1;
+    if (stats) ++h->ring_n;
+    return MRLBM_OK;
+}
+
+void free_all(mrlbm_handle* h) {
+    if (h->host_only) return;
+    cudaSetDevice(h->device);
+    for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
+                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin})
+        if (p) cudaFree(p);
+    if (h->h_ring) cudaFreeHost(h->h_ring);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t mrlbm_config_sizeof(void) { return sizeof(mrlbm_config); }
+
+int mrlbm_config_defaults(mrlbm_config* cfg) {
+    if (!cfg) return MRLBM_EINVAL;
+    config_defaults(*cfg);
+    return MRLBM_OK;
+}
+
+int mrlbm_config_from_namelist(const char* path, mrlbm_config* cfg) {
+    if (!path || !cfg) return MRLBM_EINVAL;
+    std::string err;
+    int rc = read_namelist_file(path, *cfg, err);
+    if (rc != MRLBM_OK) g_create_error = "Error while reading input.dat file... (" + err + ")";
+    return rc;
+}
+
+int mrlbm_config_resolve_geometry(mrlbm_config* cfg) {
+    if (!cfg) return MRLBM_EINVAL;
+    if (cfg->geometry_mode != MRLBM_GEOM_REFERENCE || !cfg->channel_with_cylinder) return MRLBM_OK;
+    int nx, ny;
+    double x, y, r;
+    resolve_domain(*cfg, nx, ny, x, y, r);
+    cfg->nx = nx; cfg->ny = ny; cfg->x_c = x; cfg->y_c = y; cfg->r_c = r;
+    return MRLBM_OK;
+}
+
+int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handle** out) {
+    if (!cfg || !out) return MRLBM_EINVAL;
+    *out = nullptr;
+    if (precision != MRLBM_FP64 && precision != MRLBM_FP32) {
+        g_create_error = "precision must be 64 or 32";
+        return MRLBM_EINVAL;
+    }
+    mrlbm_handle* h = new mrlbm_handle();
+    h->cfg = *cfg;
+    h->precision = precision;
+    h->device = device;
+    h->elem = precision == MRLBM_FP64 ? 8 : 4;
+    const mrlbm_config& c = h->cfg;
+    auto bail = [&](int code, const std::string& m) {
+        g_create_error = m;
+        free_all(h);
+        delete h;
+        return code;
+    };
+    if (c.Re <= 0 || !(c.uo == c.uo)) return bail(MRLBM_EINVAL, "Re must be positive");
+    if (c.channel_with_cylinder && c.rotated_coordinate && (c.strong_mass_bc || c.eq_mass_bc || c.weak_mass_bc) &&
+        !c.mom_interp)
+        return bail(MRLBM_EUNSUPPORTED,
+                    "rotated closures read mxxp/myyp, which the reference sets only when mom_interp is true");
+    int nx, ny;
+    double xc, yc, rc;
+    resolve_domain(c, nx, ny, xc, yc, rc);
+    if (nx < 4 || ny < 4) return bail(MRLBM_EINVAL, "nx and ny must be >= 4");
+    h->cfg.nx = nx; h->cfg.ny = ny; h->cfg.x_c = xc; h->cfg.y_c = yc; h->cfg.r_c = rc;
+    std::string err;
+    int grc = build_geometry(c, nx, ny, xc, yc, rc, h->geo, err);
+    if (grc != MRLBM_OK) return bail(grc, err);
+    h->lat = make_lattice();
+    // viscosity and relaxation, 2d_mrlbm.f90:133-135
+    h->nu = c.uo * (double)(ny - 1) / c.Re;
+    if (c.channel_with_cylinder) {
+        const double Lr = c.nu_length == MRLBM_NU_DIAMETER ? rc : h->geo.r_cyl;
+        h->nu = c.uo * (2.0 * Lr) / c.Re;
+    }
+    h->omega = 1.0 / ((3.0 * h->nu) + (1.0 / 2.0));
+    // curved-wall variant actually applied (2d_mrlbm.f90:280-311): the last flag called wins
+    if (!c.rotated_coordinate) h->closure = CLOSURE_UNROTATED;
+    else if (c.weak_mass_bc) h->closure = CLOSURE_WEAK;
+    else if (c.eq_mass_bc) h->closure = CLOSURE_RHOEQ;
+    else if (c.strong_mass_bc) h->closure = CLOSURE_STRONG;
+    else h->closure = CLOSURE_NONE;
+    make_dev_consts(h);
+    h->L = make_layout(nx, ny, precision == MRLBM_FP64 ? 16 : 32);
+    if (h->L.total() >= (int64_t)1 << 31) return bail(MRLBM_EINVAL, "grid too large for one handle (2^31 populations)");
+    const char* tc = std::getenv("MRLBM_TILE_CFG");
+    if (tc) h->tile_cfg = std::max(0, std::min(N_TILE_CFGS - 1, std::atoi(tc)));
+
+    if (device == -1) {            // host-only handle: configuration and geometry, no device state
+        h->host_only = true;
+        *out = h;
+        return MRLBM_OK;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bail(MRLBM_ENODEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return bail(MRLBM_EINVAL, "device index out of range");
+    auto ck = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess) { g_create_error = std::string(what) + ": " + cudaGetErrorString(e); return false; }
+        return true;
+    };
+    bool ok = ck(cudaSetDevice(device), "cudaSetDevice") &&
+              ck(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    h->stream = h->own_stream;
+    const size_t bytes = (size_t)h->L.total() * h->elem;
+    ok = ok && ck(cudaMalloc(&h->buf[0], bytes), "cudaMalloc state") && ck(cudaMalloc(&h->buf[1], bytes), "cudaMalloc state");
+    const int nb = h->geo.nb;
+    const size_t ngeo = (size_t)G_NFIELDS * std::max(nb, 1), nint = (size_t)I_NFIELDS * std::max(nb, 1);
+    ok = ok && ck(cudaMalloc(&h->d_bgeo, ngeo * h->elem), "cudaMalloc tables") &&
+         ck(cudaMalloc((void**)&h->d_bint, nint * sizeof(int)), "cudaMalloc tables");
+    const size_t nbox = std::max<size_t>(h->geo.boxmap.size(), 1);
+    ok = ok && ck(cudaMalloc((void**)&h->d_boxmap, nbox * sizeof(int)), "cudaMalloc boxmap");
+    const int max_blk = nb / 64 + 2;
+    ok = ok && ck(cudaMalloc((void**)&h->d_partials, (size_t)max_blk * 3 * sizeof(double)), "cudaMalloc partials") &&
+         ck(cudaMalloc((void**)&h->d_counter, sizeof(unsigned)), "cudaMalloc counter") &&
+         ck(cudaMalloc((void**)&h->d_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMalloc ring") &&
+         ck(cudaMalloc((void**)&h->d_err, sizeof(int)), "cudaMalloc err") &&
+         ck(cudaMallocHost((void**)&h->h_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMallocHost ring");
+    if (!ok) { std::string m = g_create_error; return bail(MRLBM_ECUDA, m); }
+    if (nb > 0) {
+        if (precision == MRLBM_FP64) {
+            ok = ck(cudaMemcpy(h->d_bgeo, h->geo.tgeo.data(), ngeo * 8, cudaMemcpyHostToDevice), "upload tables");
+        } else {
+            std::vector<float> t(h->geo.tgeo.begin(), h->geo.tgeo.end());
+            ok = ck(cudaMemcpy(h->d_bgeo, t.data(), ngeo * 4, cudaMemcpyHostToDevice), "upload tables");
+        }
+        ok = ok && ck(cudaMemcpy(h->d_bint, h->geo.tint.data(), nint * sizeof(int), cudaMemcpyHostToDevice), "upload tables");
+    }
+    if (!h->geo.boxmap.empty())
+        ok = ok && ck(cudaMemcpy(h->d_boxmap, h->geo.boxmap.data(), h->geo.boxmap.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice), "upload boxmap");
+    ok = ok && ck(cudaMemset(h->d_counter, 0, sizeof(unsigned)), "memset") && ck(cudaMemset(h->d_err, 0, sizeof(int)), "memset");
+    if (!ok) { std::string m = g_create_error; return bail(MRLBM_ECUDA, m); }
+    std::vector<double> f0;
+    initial_state(h->cfg, h->lat, nx, ny, f0);
+    int urc = upload_state(h, f0.data());
+    if (urc != MRLBM_OK) { std::string m = h->err; return bail(urc, m); }
+    h->iter = 0;
+    *out = h;
+    return MRLBM_OK;
+}
+
+int mrlbm_destroy(mrlbm_handle* h) {
+    if (!h) return MRLBM_OK;
+    free_all(h);
+    delete h;
+    return MRLBM_OK;
+}
+
+int mrlbm_last_error(const mrlbm_handle* h, char* buf, size_t len) {
+    if (!buf || len == 0) return MRLBM_EINVAL;
+    const std::string& s = h ? h->err : g_create_error;
+    std::snprintf(buf, len, "%s", s.c_str());
+    return MRLBM_OK;
+}
+
+int mrlbm_status(mrlbm_handle* h) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (e) return fail(h, MRLBM_EDEVICE_NAN, "device flag: NaN or non-positive density");
+    return MRLBM_OK;
+}
+
+int mrlbm_set_stream(mrlbm_handle* h, void* s) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_geometry_info(const mrlbm_handle* h, mrlbm_geometry_info* info) {
+    if (!h || !info) return MRLBM_EINVAL;
+    info->nx = h->L.nx; info->ny = h->L.ny; info->nbct = h->geo.nb; info->n_label15 = h->geo.n_label15;
+    info->x_c = h->geo.x_c; info->y_c = h->geo.y_c; info->r_c = h->geo.r_c; info->r_cyl = h->geo.r_cyl;
+    info->nu = h->nu; info->omega = h->omega;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_boundary_nodes(const mrlbm_handle* h, int32_t* bou_i, int32_t* bou_j, int32_t* label_bc,
+                             double* delta_uk, double* ref_xy, int32_t* stencil) {
+    if (!h) return MRLBM_EINVAL;
+    const Geometry& g = h->geo;
+    for (int l = 0; l < g.nb; ++l) {
+        if (bou_i) bou_i[l] = g.bi[l];
+        if (bou_j) bou_j[l] = g.bj[l];
+        if (label_bc) label_bc[l] = g.label[l];
+        if (delta_uk) delta_uk[l] = g.delta[l];
+    }
+    if (ref_xy) std::copy(g.ref.begin(), g.ref.end(), ref_xy);
+    if (stencil) std::copy(g.sten.begin(), g.sten.end(), stencil);
+    return MRLBM_OK;
+}
+
+int mrlbm_get_node_classes(const mrlbm_handle* h, int32_t* isfluid, int32_t* issolid, int32_t* isbound) {
+    if (!h) return MRLBM_EINVAL;
+    const size_t N = h->geo.cls.size();
+    for (size_t n = 0; n < N; ++n) {
+        const int c = h->geo.cls[n];
+        if (isfluid) isfluid[n] = c == 0;
+        if (issolid) issolid[n] = c == 1;
+        if (isbound) isbound[n] = c == 2;
+    }
+    return MRLBM_OK;
+}
+
+int mrlbm_load_state(mrlbm_handle* h, const double* f, int32_t iter) {
+    if (!h || !f) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    int rc = upload_state(h, f);
+    if (rc != MRLBM_OK) return rc;
+    h->iter = iter;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_state(mrlbm_handle* h, double* f) {
+    if (!h || !f) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    const int nx = h->L.nx, ny = h->L.ny;
+    const size_t N = (size_t)nx * ny;
+    const int64_t total = h->L.total();
+    std::vector<unsigned char> b((size_t)total * h->elem);
+    CK(cudaMemcpyAsync(b.data(), h->buf[h->cur], b.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < Q; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const int64_t s = slot_of(h, i, j, k);
+                double v;
+                if (h->precision == MRLBM_FP64) v = ((const double*)b.data())[s];
+                else v = h->lat.w[k] + (double)((const float*)b.data())[s];
+                f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k] = v;
+            }
+    return MRLBM_OK;
+}
+
+int mrlbm_set_inlet_profile(mrlbm_handle* h, const double* u_in) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    if (!u_in) { h->has_uin = false; return MRLBM_OK; }
+    const int ny = h->L.ny;
+    if (!h->d_uin) CK(cudaMalloc((void**)&h->d_uin, (size_t)ny * sizeof(double)));
+    if (h->precision == MRLBM_FP64) {
+        CK(cudaMemcpyAsync(h->d_uin, u_in, (size_t)ny * 8, cudaMemcpyHostToDevice, h->stream));
+    } else {
+        std::vector<float> t(u_in, u_in + ny);
+        CK(cudaMemcpyAsync(h->d_uin, t.data(), (size_t)ny * 4, cudaMemcpyHostToDevice, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->has_uin = true;
+    return MRLBM_OK;
+}
+
+int mrlbm_step(mrlbm_handle* h, int32_t nsteps, int32_t flags) {
+    if (!h || nsteps < 0) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    const mrlbm_config& c = h->cfg;
+    if ((flags & MRLBM_STEP_MACRO) && !h->d_macro)
+        CK(cudaMalloc((void**)&h->d_macro, (size_t)6 * h->L.nx * h->L.ny * sizeof(double)));
+    for (int s = 0; s < nsteps; ++s) {
+        h->iter += 1;
+        const bool stats = c.post_process && h->iter >= c.statsbegin && h->iter <= c.statsend;
+        const bool plot = c.post_process && c.iplot > 0 && h->iter % c.iplot == 0 &&
+                          (c.channel_with_cylinder || c.channel_with_square);
+        const bool macro = (flags & MRLBM_STEP_MACRO) && s == nsteps - 1;
+        int rc = launch_one(h, stats, plot, macro);
+        if (rc != MRLBM_OK) return rc;
+        if (h->ring_n == RING_CAP) {
+            rc = drain_ring(h);
+            if (rc != MRLBM_OK) return rc;
+        }
+    }
+    return MRLBM_OK;
+}
+
+int mrlbm_get_iter(const mrlbm_handle* h, int32_t* iter) {
+    if (!h || !iter) return MRLBM_EINVAL;
+    *iter = h->iter;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_macro(mrlbm_handle* h, double* rho, double* ux, double* uy, double* mxx, double* myy, double* mxy) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    if (!h->d_macro) return fail(h, MRLBM_ESTATE, "no step has stored macroscopic fields (use MRLBM_STEP_MACRO)");
+    CK(cudaSetDevice(h->device));
+    const size_t N = (size_t)h->L.nx * h->L.ny;
+    double* outs[6] = {rho, ux, uy, mxx, myy, mxy};
+    for (int q = 0; q < 6; ++q)
+        if (outs[q]) CK(cudaMemcpyAsync(outs[q], h->d_macro + q * N, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MRLBM_OK;
+}
+
+int mrlbm_get_forces(mrlbm_handle* h, int32_t* iter, double* fd, double* fl, double* rin, int32_t cap, int32_t* n) {
+    if (!h || !n) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    int rc = drain_ring(h);
+    if (rc != MRLBM_OK) return rc;
+    const int avail = (int)(h->hist.size() / REC_WORDS);
+    const int m = std::min(avail, std::max(cap, 0));
+    for (int t = 0; t < m; ++t) {
+        const double* r = &h->hist[(size_t)t * REC_WORDS];
+        if (iter) iter[t] = (int32_t)r[0];
+        if (fd) fd[t] = r[1];
+        if (fl) fl[t] = r[2];
+        if (rin) rin[t] = r[3];
+    }
+    h->hist.erase(h->hist.begin(), h->hist.begin() + (size_t)m * REC_WORDS);
+    *n = m;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n) {
+    if (!h || !n) return MRLBM_EINVAL;
+    *n = h->launches;
+    return MRLBM_OK;
+}
+
+}  // extern "C"
