@@ -119,7 +119,8 @@ int mrlbm_last_error(const mrlbm_handle* h, char* buf, size_t len);
 /* Sticky device status: MRLBM_OK or MRLBM_EDEVICE_NAN.  Synchronises. */
 int mrlbm_status(mrlbm_handle* h);
 
-/* Run subsequent work on a caller-owned cudaStream_t (NULL = the handle's own stream). */
+/* Run subsequent work on a caller-owned cudaStream_t (NULL = the legacy default stream).
+ * A new handle works on a private non-blocking stream until this is called. */
 int mrlbm_set_stream(mrlbm_handle* h, void* cuda_stream);
 
 int mrlbm_get_geometry_info(const mrlbm_handle* h, mrlbm_geometry_info* info);

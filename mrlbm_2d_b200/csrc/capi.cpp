@@ -54,6 +54,9 @@ struct mrlbm_handle {
     std::string err;
     DevConsts dc{};
     bool host_only = false;
+    std::vector<OvrEntry> ovr;                // loaded-state overrides (see OvrEntry)
+    bool ovr_live = false;                    // true until the first step after a load
+    OvrEntry* d_ovr = nullptr;
 };
 
 #define CK(call)                                                                           \
@@ -81,7 +84,8 @@ inline int64_t slot_of(const mrlbm_handle* h, int i, int j, int k) {
 }
 
 // Deviation-form constants, computed in FP64 from the reference weights and tables.
-void make_dev_consts(mrlbm_handle* h) {
+// Returns false when a label's Is and Os weight sums differ (the FP32 closure relies on it).
+bool make_dev_consts(mrlbm_handle* h) {
     const Lattice64& L = h->lat;
     DevConsts& d = h->dc;
     double sw = 0, cxx = 0, cyy = 0;
@@ -89,23 +93,44 @@ void make_dev_consts(mrlbm_handle* h) {
     d.eps_mass = (float)(sw - 1.0);
     d.cxx = (float)cxx;
     d.cyy = (float)cyy;
+    // incoming masks of apply_bc (2d_mrlbm.f90:1254, 1283, 1311, 1339)
     const int masks[4] = {(1 << 0) | (1 << 1) | (1 << 2) | (1 << 4) | (1 << 5) | (1 << 8),
                           (1 << 0) | (1 << 2) | (1 << 3) | (1 << 4) | (1 << 6) | (1 << 7),
                           (1 << 0) | (1 << 1) | (1 << 2) | (1 << 3) | (1 << 5) | (1 << 6),
                           (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | (1 << 8)};
+    double W[4], Sxx[4], Syy[4];
     for (int e = 0; e < 4; ++e) {
-        double a = 0, bx = 0, by = 0, bxy = 0;
+        W[e] = 0; Sxx[e] = 0; Syy[e] = 0;
         for (int k = 0; k < Q; ++k)
-            if ((masks[e] >> k) & 1) { a += L.w[k]; bx += L.w[k] * L.hxx[k]; by += L.w[k] * L.hyy[k]; bxy += L.w[k] * L.hxy[k]; }
-        d.wI[e] = (float)a; d.swxx[e] = (float)bx; d.swyy[e] = (float)by; d.swxy[e] = (float)bxy;
+            if ((masks[e] >> k) & 1) { W[e] += L.w[k]; Sxx[e] += L.w[k] * L.hxx[k]; Syy[e] += L.w[k] * L.hyy[k]; }
+    }
+    const double om = h->omega;
+    d.k_out_mxx = (float)(1.0 + 9.0 * Sxx[0]);
+    d.sw_out_yy = (float)Syy[0];
+    d.k_in_rho = (float)(4.0 * W[1] + 3.0 * Sxx[1] - 3.0);
+    d.k_in_mxx = (float)(1.0 + 9.0 * Sxx[1]);
+    d.sw_in_yy = (float)Syy[1];
+    d.k_in_rho_inc = (float)(6.0 * W[1] - 5.0);
+    for (int e = 0; e < 2; ++e) {
+        d.k_w_rho[e] = (float)(12.0 * W[2 + e] - 9.0 - om + 9.0 * (1.0 - om) * Syy[2 + e]);
+        d.sw_w_xx[e] = (float)Sxx[2 + e];
+        d.k_w_myy[e] = (float)(1.0 + 9.0 * Syy[2 + e]);
+        d.k_w_rho_inc[e] = (float)(6.0 * W[2 + e] - 5.0);
+        d.w_wall[e] = (float)W[2 + e];
     }
     int incs[16], outs[16];
     link_tables(h->cfg.label15_rule, incs, outs);
+    bool ok = true;
     for (int l = 0; l < 16; ++l) {
-        double a = 0;
-        for (int k = 0; k < Q; ++k) if ((incs[l] >> k) & 1) a += L.w[k];
-        d.lab_wI[l] = (float)a;
+        double a = 0, b = 0;
+        for (int k = 0; k < Q; ++k) {
+            if ((incs[l] >> k) & 1) a += L.w[k];
+            if ((outs[l] >> k) & 1) b += L.w[k];
+        }
+        d.lab_w[l] = (float)a;
+        if (a != b) ok = false;
     }
+    return ok;
 }
 
 int upload_state(mrlbm_handle* h, const double* f) {
@@ -133,6 +158,41 @@ int upload_state(mrlbm_handle* h, const double* f) {
         CK(cudaStreamSynchronize(h->stream));
     }
     h->cur = 0;
+    // destinations whose streaming source slot another destination also uses keep their
+    // own value for the first step (and for get_state until then)
+    h->ovr.clear();
+    auto check = [&](int i, int j) {
+        for (int k = 0; k < Q; ++k) {
+            const size_t src = (size_t)(i - 1) + (size_t)nx * (j - 1) + N * k;
+            const int64_t sl = slot_of(h, i, j, k);
+            double stored;
+            if (h->precision == MRLBM_FP64) {
+                CK(cudaMemcpy(&stored, (const double*)h->buf[0] + sl, 8, cudaMemcpyDeviceToHost));
+            } else {
+                float g;
+                CK(cudaMemcpy(&g, (const float*)h->buf[0] + sl, 4, cudaMemcpyDeviceToHost));
+                stored = h->lat.w[k] + (double)g;
+            }
+            const double want = h->precision == MRLBM_FP64 ? f[src] : h->lat.w[k] + (double)(float)(f[src] - h->lat.w[k]);
+            if (!(stored == want)) {
+                OvrEntry e{i, j, k, 0, h->precision == MRLBM_FP64 ? f[src] : (double)(float)(f[src] - h->lat.w[k])};
+                h->ovr.push_back(e);
+            }
+        }
+        return MRLBM_OK;
+    };
+    const int ci[2] = {1, nx}, cj[2] = {1, ny};
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            int rc = check(ci[a], cj[b]);
+            if (rc != MRLBM_OK) return rc;
+        }
+    if (!h->ovr.empty()) {
+        if (h->d_ovr) cudaFree(h->d_ovr);
+        CK(cudaMalloc((void**)&h->d_ovr, h->ovr.size() * sizeof(OvrEntry)));
+        CK(cudaMemcpy(h->d_ovr, h->ovr.data(), h->ovr.size() * sizeof(OvrEntry), cudaMemcpyHostToDevice));
+    }
+    h->ovr_live = !h->ovr.empty();
     return MRLBM_OK;
 }
 
@@ -192,6 +252,8 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.src = (const double*)h->buf[h->cur];
         p.dst = (double*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? h->d_uin : nullptr;
+        p.ovr = h->ovr_live ? h->d_ovr : nullptr;
+        p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         p.zero_solid_u = plot;
         p.do_stats = stats;
         p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
@@ -204,6 +266,8 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.src = (const float*)h->buf[h->cur];
         p.dst = (float*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? (const float*)h->d_uin : nullptr;
+        p.ovr = h->ovr_live ? h->d_ovr : nullptr;
+        p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         p.zero_solid_u = plot;
         p.do_stats = stats;
         p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
@@ -217,6 +281,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         return MRLBM_ECUDA;
     }
     h->cur ^= 1;
+    h->ovr_live = false;
     if (stats) ++h->ring_n;
     return MRLBM_OK;
 }
@@ -225,7 +290,7 @@ void free_all(mrlbm_handle* h) {
     if (h->host_only) return;
     cudaSetDevice(h->device);
     for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
-                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin})
+                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, (void*)h->d_ovr})
         if (p) cudaFree(p);
     if (h->h_ring) cudaFreeHost(h->h_ring);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -307,7 +372,10 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
     else if (c.eq_mass_bc) h->closure = CLOSURE_RHOEQ;
     else if (c.strong_mass_bc) h->closure = CLOSURE_STRONG;
     else h->closure = CLOSURE_NONE;
-    make_dev_consts(h);
+    if (!make_dev_consts(h) && precision == MRLBM_FP32)
+        return bail(MRLBM_EUNSUPPORTED, "FP32 closure needs equal Is/Os weight sums for every label");
+    if (precision == MRLBM_FP32 && c.channel_with_cylinder && h->closure != CLOSURE_STRONG && h->closure != CLOSURE_NONE)
+        return bail(MRLBM_EUNSUPPORTED, "the FP32 step implements only the default rotated strong-mass closure");
     h->L = make_layout(nx, ny, precision == MRLBM_FP64 ? 16 : 32);
     if (h->L.total() >= (int64_t)1 << 31) return bail(MRLBM_EINVAL, "grid too large for one handle (2^31 populations)");
     const char* tc = std::getenv("MRLBM_TILE_CFG");
@@ -396,7 +464,7 @@ int mrlbm_set_stream(mrlbm_handle* h, void* s) {
     if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
-    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    h->stream = (cudaStream_t)s;
     return MRLBM_OK;
 }
 
@@ -464,6 +532,10 @@ int mrlbm_get_state(mrlbm_handle* h, double* f) {
                 else v = h->lat.w[k] + (double)((const float*)b.data())[s];
                 f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k] = v;
             }
+    if (h->ovr_live)
+        for (const OvrEntry& e : h->ovr)
+            f[(size_t)(e.i - 1) + (size_t)nx * (e.j - 1) + N * e.k] =
+                h->precision == MRLBM_FP64 ? e.v : h->lat.w[e.k] + e.v;
     return MRLBM_OK;
 }
 

@@ -222,6 +222,7 @@ int build_geometry(const mrlbm_config& cfg, int nx, int ny, double x_c, double y
         TI(I_NODEJ, l) = j;
         TI(I_IS, l) = incs[g.label[l]];
         TI(I_OS, l) = outs[g.label[l]];
+        TI(I_LABEL, l) = g.label[l];
     }
     // bounding box of every non-fluid node; edge rows/columns must stay fluid
     int x0 = nx + 1, x1 = 0, y0 = ny + 1, y1 = 0;

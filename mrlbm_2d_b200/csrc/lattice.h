@@ -102,8 +102,8 @@ enum GeoField : int {
     G_SS2 = G_SSS + 8,                              //                        sin2
     G_NFIELDS = G_SS2 + 8
 };
-// Integer table, field-major: node i, node j, Is mask, Os mask, then 12 stencil nodes
-// (ref points 2,3,4 x 4 corners) as i and j.
-enum IntField : int { I_NODEI = 0, I_NODEJ, I_IS, I_OS, I_SI = 4, I_SJ = 4 + 12, I_NFIELDS = 4 + 24 };
+// Integer table, field-major: node i, node j, Is mask, Os mask, quadrant label, then 12
+// stencil nodes (ref points 2,3,4 x 4 corners) as i and j.
+enum IntField : int { I_NODEI = 0, I_NODEJ, I_IS, I_OS, I_LABEL, I_SI = 5, I_SJ = 5 + 12, I_NFIELDS = 5 + 24 };
 
 }  // namespace mrlbm

@@ -1,0 +1,145 @@
+// step_common.cuh -- launch skeleton shared by the FP64 and FP32 fused steps: pull-stream
+// gather, coalesced store, tile mapping, boundary blocks and the per-step force reduction.
+// The arithmetic of a node lives in a "physics" policy (step_fp64.cuh, step_fp32.cuh) with
+//   static void bulk_node(const P&, int i, int j);
+//   static void boundary_node(const P&, int l, double& Fx, double& Fy);
+//   static double inlet_rho(const P&, int j);   // post-closure density of node (1,j)
+#pragma once
+#include <cuda_runtime.h>
+#include "step_params.h"
+
+namespace mrlbm {
+
+// f(i,j,:) of this step = fout of the previous step at the streaming sources
+// (stream_source in lattice.h).  Interior nodes take the branch-free fast path.
+template <class T>
+__device__ __forceinline__ void gather(const StepParams<T>& p, int i, int j, T f[Q]) {
+    const int nx = p.L.nx, ny = p.L.ny;
+    const int pitch = p.L.pitch, plane = (int)p.L.plane;
+    if (i > 1 && i < nx && j > 1 && j < ny) {
+        const T* s = p.src + ((int)(j * pitch + i + p.L.off));
+#pragma unroll
+        for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
+    } else {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            SrcSlot sl = stream_source(nx, ny, i, j, k, p.xper, p.yper, p.freeslip);
+            f[k] = __ldg(p.src + p.L.at(sl.i, sl.j, sl.k));
+        }
+        for (int q = 0; q < p.n_ovr; ++q)
+            if (p.ovr[q].i == i && p.ovr[q].j == j) f[p.ovr[q].k] = (T)p.ovr[q].v;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void store(const StepParams<T>& p, int i, int j, const T fo[Q]) {
+    T* d = p.dst + ((int)(j * p.L.pitch + i + p.L.off));
+    const int plane = (int)p.L.plane;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k * plane] = fo[k];
+}
+
+template <class T>
+__device__ __forceinline__ void store_macro(const StepParams<T>& p, int i, int j, double rho, double ux, double uy,
+                                            double mxx, double myy, double mxy) {
+    const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1);
+    const int64_t N = (int64_t)p.L.nx * p.L.ny;
+    p.macro[n] = rho;
+    p.macro[N + n] = ux;
+    p.macro[2 * N + n] = uy;
+    p.macro[3 * N + n] = mxx;
+    p.macro[4 * N + n] = myy;
+    p.macro[5 * N + n] = mxy;
+}
+
+// Node class inside the cylinder box: CLS_FLUID, CLS_SOLID or a boundary-node index.
+template <class T>
+__device__ __forceinline__ int node_class(const StepParams<T>& p, int i, int j) {
+    const unsigned bx = (unsigned)(i - p.box_x0), by = (unsigned)(j - p.box_y0);
+    if (bx < (unsigned)p.box_w && by < (unsigned)p.box_h) return __ldg(p.boxmap + by * p.box_w + bx);
+    return CLS_FLUID;
+}
+
+// Block reduction of three doubles with warp shuffles; result valid in thread 0.
+__device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, double* sm) {
+    const unsigned full = 0xffffffffu;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(full, a, o);
+        b += __shfl_down_sync(full, b, o);
+        c += __shfl_down_sync(full, c, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) { sm[3 * wid] = a; sm[3 * wid + 1] = b; sm[3 * wid + 2] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a = sm[0]; b = sm[1]; c = sm[2];
+        for (int w = 1; w < nw; ++w) { a += sm[3 * w]; b += sm[3 * w + 1]; c += sm[3 * w + 2]; }
+    }
+}
+
+// Boundary blocks: curved-wall nodes, then (stats steps) the momentum-exchange force and
+// the inlet density sum, reduced across blocks; the last block to arrive writes the record.
+template <class Phys>
+__device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
+    __shared__ double sm[3 * 32];
+    const int nthr = blockDim.x;
+    const int l = blockIdx.x * nthr + threadIdx.x;
+    double Fx = 0.0, Fy = 0.0, rin = 0.0;
+    if (l < p.nb) Phys::boundary_node(p, l, Fx, Fy);
+    if (!p.do_stats) return;
+    if (!p.xper)
+        for (int j = 1 + l; j <= p.L.ny; j += p.nbblk * nthr) rin += Phys::inlet_rho(p, j);
+    block_reduce3(Fx, Fy, rin, sm);
+    if (threadIdx.x == 0) {
+        p.partials[3 * blockIdx.x] = Fx;
+        p.partials[3 * blockIdx.x + 1] = Fy;
+        p.partials[3 * blockIdx.x + 2] = rin;
+        __threadfence();
+        const unsigned ticket = atomicAdd(p.counter, 1u);
+        if (ticket == (unsigned)(p.nbblk - 1)) {
+            __threadfence();
+            double a = 0.0, b = 0.0, c = 0.0;
+            for (int q = 0; q < p.nbblk; ++q) {
+                a += __ldcg(p.partials + 3 * q);
+                b += __ldcg(p.partials + 3 * q + 1);
+                c += __ldcg(p.partials + 3 * q + 2);
+            }
+            if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = a; p.rec[2] = b; p.rec[3] = c; }
+            *p.counter = 0u;
+        }
+    }
+}
+
+// One time step.  Blocks [0, nbblk) are boundary blocks; the rest are bulk tiles of
+// BX x (BY*NJ) nodes, one thread per column and NJ rows.
+template <class Phys, int BX, int BY, int NJ, int MINB>
+__global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const typename Phys::P p) {
+    if ((int)blockIdx.x < p.nbblk) {
+        boundary_block<Phys>(p);
+        return;
+    }
+    const int t = blockIdx.x - p.nbblk;
+    const int tx = t % p.tiles_x, ty = t / p.tiles_x;
+    const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
+    const int i = 1 + tx * BX + lx;
+    if (i > p.L.nx) return;
+#pragma unroll
+    for (int r = 0; r < NJ; ++r) {
+        const int j = 1 + ty * BY * NJ + r * BY + ly;
+        if (j <= p.L.ny) Phys::bulk_node(p, i, j);
+    }
+}
+
+template <class Phys, int BX, int BY, int NJ, int MINB>
+int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
+    const int nthr = BX * BY;
+    p.nbblk = p.nb > 0 ? (p.nb + nthr - 1) / nthr : 1;
+    p.tiles_x = (p.L.nx + BX - 1) / BX;
+    const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
+    const long long nblocks = (long long)p.nbblk + (long long)p.tiles_x * tiles_y;
+    step_kernel<Phys, BX, BY, NJ, MINB><<<(unsigned)nblocks, nthr, 0, s>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace mrlbm

@@ -1,0 +1,311 @@
+// step_fp32.cuh -- FP32 fused step in deviation form.
+//
+// Storage: g_k = f_k - w_k in FP32, w_k the reference's single-rounded weights
+// (2d_mrlbm.f90:129), which are exact FP32 values.  Arithmetic is FP32 on small quantities
+// only: every closure of the FP64 step (2d_mrlbm.f90:232-457) is rearranged so the
+// rest-state parts that cancel (sums of w_k over fixed link sets, which are exact in real
+// arithmetic but not with single-rounded weights) are folded into constants computed once
+// in FP64 on the host (DevConsts).  The mass drift the reference has because
+// sum(w) = 1 + 7.45e-9 is kept (eps_mass).  Forces are accumulated in FP64 from
+// w_k + g_k.  Only the default curved-wall closure (numerical_boundary_cases_rotation,
+// 2d_mrlbm.f90:1635-1765) has an FP32 form.
+#pragma once
+#include "step_common.cuh"
+
+namespace mrlbm {
+namespace fp32 {
+
+using P = StepParams<float>;
+
+struct Mac { float drho, rho, ux, uy, mxx, myy, mxy; };
+
+constexpr float THIRD = 1.0f / 3.0f;
+
+// rho = 1 + sum g + (sum w - 1); u = sum f c / rho; m = sum f H / rho with
+// sum f H_xx = (sum_k w_k H_xx,k) + sum g c_x^2 - sum g / 3.
+__device__ __forceinline__ Mac moments(const P& p, const float g[Q]) {
+    Mac m;
+    const float dg = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) + g[8];
+    m.drho = dg + p.dc.eps_mass;
+    m.rho = 1.0f + m.drho;
+    const float inv = 1.0f / m.rho;
+    const float jx = ((g[1] - g[3]) + (g[5] - g[7])) + (g[8] - g[6]);
+    const float jy = ((g[2] - g[4]) + (g[5] - g[7])) + (g[6] - g[8]);
+    const float d4 = (g[5] + g[6]) + (g[7] + g[8]);
+    const float sxx = (g[1] + g[3]) + d4;
+    const float syy = (g[2] + g[4]) + d4;
+    const float sxy = (g[5] - g[6]) + (g[7] - g[8]);
+    m.ux = jx * inv;
+    m.uy = jy * inv;
+    m.mxx = ((sxx - THIRD * dg) + p.dc.cxx) * inv;
+    m.myy = ((syy - THIRD * dg) + p.dc.cyy) * inv;
+    m.mxy = sxy * inv;
+    return m;
+}
+
+__device__ __forceinline__ float hxx_of(int k, float hm, float hp) { return ex(k) != 0 ? hp : hm; }
+__device__ __forceinline__ float hyy_of(int k, float hm, float hp) { return ey(k) != 0 ? hp : hm; }
+
+// Deviation sums over a fixed incoming mask: G = sum g, S_ab = sum g H_ab.
+template <int MASK>
+__device__ __forceinline__ void incoming(const float g[Q], float hm, float hp, float& G, float& Sxx, float& Syy,
+                                         float& Sxy) {
+    G = 0.f; Sxx = 0.f; Syy = 0.f; Sxy = 0.f;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        if (!((MASK >> k) & 1)) continue;
+        G += g[k];
+        Sxx += g[k] * hxx_of(k, hm, hp);
+        Syy += g[k] * hyy_of(k, hm, hp);
+        const int hxy = ex(k) * ey(k);
+        if (hxy > 0) Sxy += g[k];
+        if (hxy < 0) Sxy -= g[k];
+    }
+}
+
+constexpr int M_OUTLET = (1 << 0) | (1 << 1) | (1 << 2) | (1 << 4) | (1 << 5) | (1 << 8);
+constexpr int M_INLET = (1 << 0) | (1 << 2) | (1 << 3) | (1 << 4) | (1 << 6) | (1 << 7);
+constexpr int M_TOP = (1 << 0) | (1 << 1) | (1 << 2) | (1 << 3) | (1 << 5) | (1 << 6);
+constexpr int M_BOTTOM = (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | (1 << 8);
+
+// Edge nodes: Dirichlet values and the regularized edge closures of apply_bc /
+// apply_bc_incomp (2d_mrlbm.f90:249-272, 1237-1494) in deviation form.
+__device__ __noinline__ void edge_node(const P& p, int i, int j, const float g[Q], Mac& m) {
+    const int nx = p.L.nx, ny = p.L.ny;
+    const bool outlet = !p.xper && i == nx;
+    const bool inlet = !p.xper && i == 1;
+    const bool top = p.walls_ref && j == ny;
+    const bool bottom = p.walls_ref && j == 1;
+    const DevConsts& c = p.dc;
+    if (outlet) {                                   // rho, u copied from column nx-1
+        float gn[Q];
+        gather(p, nx - 1, j, gn);
+        const Mac mn = moments(p, gn);
+        m.drho = mn.drho; m.rho = mn.rho; m.ux = mn.ux; m.uy = mn.uy;
+    }
+    if (inlet) {
+        m.ux = p.u_in ? p.u_in[j - 1] : p.uinlet;
+        m.uy = p.vinlet;
+    }
+    if (top || bottom) { m.ux = 0.f; m.uy = 0.f; }
+    const float hm = p.hm, hp = p.hp, om = p.omega;
+    float G, Sxx, Syy, Sxy;
+    if (top || bottom) {
+        const int e = top ? 0 : 1;
+        if (top) incoming<M_TOP>(g, hm, hp, G, Sxx, Syy, Sxy);
+        else incoming<M_BOTTOM>(g, hm, hp, G, Sxx, Syy, Sxy);
+        if (!p.incomp_bc) {
+            m.drho = (c.k_w_rho[e] + 12.0f * G + 9.0f * (1.0f - om) * Syy) / (9.0f + om);
+            m.rho = 1.0f + m.drho;
+            m.mxx = 6.0f * (c.sw_w_xx[e] + Sxx) / (5.0f * m.rho);
+            m.myy = (c.k_w_myy[e] + m.drho + 9.0f * Syy) / (6.0f * m.rho);
+            m.mxy = 2.0f * Sxy / m.rho;
+        } else {
+            m.drho = (c.k_w_rho_inc[e] + 6.0f * G) / 5.0f;
+            m.rho = 1.0f + m.drho;
+            m.mxx = 0.f;
+            m.myy = 0.f;
+            m.mxy = 5.0f * (Sxy / (c.w_wall[e] + G)) / 3.0f;
+        }
+    } else if (inlet) {
+        incoming<M_INLET>(g, hm, hp, G, Sxx, Syy, Sxy);
+        const float u = m.ux;
+        if (!p.incomp_bc) {
+            m.drho = (c.k_in_rho + 4.0f * G + 3.0f * Sxx + 3.0f * u) / (3.0f - 3.0f * u);
+            m.rho = 1.0f + m.drho;
+            m.mxx = (c.k_in_mxx + m.drho + 9.0f * Sxx + 3.0f * m.rho * u) / (6.0f * m.rho);
+            m.myy = 6.0f * (c.sw_in_yy + Syy) / (5.0f * m.rho);
+            m.mxy = 2.0f * Sxy / m.rho;
+        } else {
+            m.drho = (c.k_in_rho_inc + 6.0f * G + 3.0f * u + 3.0f * (u * u)) / (5.0f - 3.0f * u - 3.0f * (u * u));
+            m.rho = 1.0f + m.drho;
+            m.mxx = u * u;
+            m.myy = 0.f;
+            m.mxy = 2.0f * Sxy / m.rho;
+        }
+    } else if (outlet) {
+        incoming<M_OUTLET>(g, hm, hp, G, Sxx, Syy, Sxy);
+        const float rp = m.rho;
+        if (!p.incomp_bc) {
+            m.mxx = (c.k_out_mxx + m.drho + 9.0f * Sxx - 3.0f * rp * m.ux) / (6.0f * rp);
+            m.myy = 6.0f * (c.sw_out_yy + Syy) / (5.0f * rp);
+        } else {
+            m.mxx = m.ux * m.ux;
+            m.myy = m.uy * m.uy;
+        }
+        m.mxy = (6.0f * Sxy - rp * m.uy) / (3.0f * rp);
+    }
+}
+
+// Moment-space collision and Hermite reconstruction (2d_mrlbm.f90:407-457) on deviations:
+// g_out_k = w_k (drho + rho a_k), a_k = 3 c_k.u + 4.5 m_xx H_xx,k + 4.5 m_yy H_yy,k + 9 m_xy H_xy,k.
+__device__ __forceinline__ void collide(const P& p, const Mac& m, float go[Q]) {
+    const float om = p.omega, om1 = p.omega1;
+    float mxx = om1 * m.mxx + om * m.ux * m.ux;
+    float myy = om1 * m.myy + om * m.uy * m.uy;
+    const float mxy = om1 * m.mxy + om * m.ux * m.uy;
+    if (p.incomp_bulk) {
+        const float t = 0.5f * (mxx + myy - m.ux * m.ux - m.uy * m.uy);
+        mxx -= t;
+        myy -= t;
+    }
+    const float A = 4.5f * mxx, B = 4.5f * myy, C = 9.0f * mxy;
+    const float hm = p.hm, hp = p.hp;
+    const float b0 = (A + B) * hm, bx = A * hp + B * hm, by = A * hm + B * hp, bd = (A + B) * hp;
+    const float tx = 3.0f * m.ux, ty = 3.0f * m.uy, tp = 3.0f * (m.ux + m.uy), tm = 3.0f * (m.ux - m.uy);
+    const float r = m.rho, d = m.drho;
+    go[0] = p.w[0] * (d + r * b0);
+    go[1] = p.w[1] * (d + r * (bx + tx));
+    go[2] = p.w[1] * (d + r * (by + ty));
+    go[3] = p.w[1] * (d + r * (bx - tx));
+    go[4] = p.w[1] * (d + r * (by - ty));
+    go[5] = p.w[5] * (d + r * ((bd + C) + tp));
+    go[6] = p.w[5] * (d + r * ((bd - C) - tm));
+    go[7] = p.w[5] * (d + r * ((bd + C) - tp));
+    go[8] = p.w[5] * (d + r * ((bd - C) + tm));
+}
+
+__device__ __forceinline__ float gf(const P& p, int field, int l) { return p.bgeo[field * p.nb + l]; }
+__device__ __forceinline__ int gi(const P& p, int field, int l) { return p.bint[field * p.nb + l]; }
+
+// Velocity and rotated moments at reference point r (2 or 3), bilinear over 4 stencil nodes.
+__device__ __noinline__ void ref_point(const P& p, int l, int r, float& uxr, float& uyr, float& mxxr, float& myyr) {
+    float uxv[4], uyv[4], mxv[4], myv[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int s = (r - 2) * 4 + c;
+        float g[Q];
+        gather(p, gi(p, I_SI + s, l), gi(p, I_SJ + s, l), g);
+        const Mac m = moments(p, g);
+        uxv[c] = m.ux;
+        uyv[c] = m.uy;
+        const float cc = gf(p, G_SCC + s, l), ss = gf(p, G_SSS + s, l), s2 = gf(p, G_SS2 + s, l);
+        mxv[c] = m.mxx * cc + m.myy * ss + m.mxy * s2;
+        myv[c] = m.mxx * ss + m.myy * cc - m.mxy * s2;
+    }
+    const float xd = gf(p, r == 2 ? G_XD2 : G_XD3, l), yd = gf(p, r == 2 ? G_YD2 : G_YD3, l);
+    auto bil = [&](const float v[4]) {
+        return (1.0f - yd) * ((1.0f - xd) * v[0] + xd * v[1]) + yd * ((1.0f - xd) * v[2] + xd * v[3]);
+    };
+    uxr = bil(uxv);
+    uyr = bil(uyv);
+    mxxr = bil(mxv);
+    myyr = bil(myv);
+}
+
+// numerical_boundary_cases_rotation (2d_mrlbm.f90:1635-1765) in deviation form.  With
+// W = sum_{Is} w = sum_{Os} w (equal for every handled label), the closure's O(1) parts
+// cancel exactly:  rho_I = W + G,  G' = W + (a1 + omega e2),  D_xy = SW_xy + d1, so
+//   R_xy = d1 - SG_xy - S_xy (a1 + omega e2 - G) / rho_I,
+//   den  = W + dden,  dden = a1 + (1-omega)(M'.B') + omega e2,  drho = (G - dden) / den.
+__device__ __noinline__ void closure_strong(const P& p, int l, const float g[Q], float uxp, float uyp, float Mxx,
+                                            float Myy, Mac& m) {
+    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const int label = gi(p, I_LABEL, l);
+    const float om = p.omega, om1 = p.omega1;
+    float a1 = 0.f, e2 = 0.f, B11 = 0.f, B22 = 0.f, B12 = 0.f;
+    float G = 0.f, SWxy = 0.f, SGxy = 0.f, d1 = 0.f, F11 = 0.f, F22 = 0.f, F12 = 0.f;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const float cxp = gf(p, G_CXP + k, l), cyp = gf(p, G_CYP + k, l);
+        const float hxx = gf(p, G_HXXP + k, l), hyy = gf(p, G_HYYP + k, l), hxy = gf(p, G_HXYP + k, l);
+        const float wk = p.w[k];
+        const float ak = 3.0f * wk * (uxp * cxp + uyp * cyp);
+        const float ek = 4.5f * wk * ((uxp * uxp) * hxx + (uyp * uyp) * hyy + 2.0f * (uxp * uyp) * hxy);
+        const float b11 = 4.5f * wk * hxx, b22 = 4.5f * wk * hyy, b12 = 4.5f * wk * hxy;
+        if ((Os >> k) & 1) { a1 += ak; e2 += ek; B11 += b11; B22 += b22; B12 += b12; }
+        if ((Is >> k) & 1) {
+            G += g[k];
+            SWxy += wk * hxy;
+            SGxy += g[k] * hxy;
+            d1 += ak * hxy;
+            F11 += b11 * hxy;
+            F22 += b22 * hxy;
+            F12 += b12 * hxy;
+        }
+    }
+    const float W = p.dc.lab_w[label];
+    const float rhoI = W + G;
+    const float Sxy = SWxy + SGxy;
+    const float mxyI = Sxy / rhoI;
+    const float L11 = om1 * B11 * mxyI - F11, L22 = om1 * B22 * mxyI - F22, L12 = 2.0f * (om1 * B12 * mxyI - F12);
+    const float R = d1 - SGxy - Sxy * ((a1 + om * e2) - G) / rhoI;
+    const float Mxy = (R - Mxx * L11 - Myy * L22) / L12;
+    const float dden = a1 + om1 * (Mxx * B11 + Myy * B22 + 2.0f * Mxy * B12) + om * e2;
+    m.drho = (G - dden) / (W + dden);
+    m.rho = 1.0f + m.drho;
+    const float cc = gf(p, G_CC, l), ss = gf(p, G_SS, l), s2 = gf(p, G_S2TH, l), c2 = gf(p, G_C2TH, l);
+    m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
+    m.myy = Mxx * ss + Myy * cc + Mxy * s2;
+    m.mxy = (Mxx - Myy) * 0.5f * s2 + Mxy * c2;
+}
+
+__device__ __noinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
+    const int i = gi(p, I_NODEI, l), j = gi(p, I_NODEJ, l);
+    float g[Q];
+    gather(p, i, j, g);
+    Mac m = moments(p, g);
+    float mxxp = 0.f, myyp = 0.f;
+    if (p.vel_interp || p.mom_interp) {
+        float ux2, uy2, mx2, my2, ux3, uy3, mx3, my3;
+        ref_point(p, l, 2, ux2, uy2, mx2, my2);
+        ref_point(p, l, 3, ux3, uy3, mx3, my3);
+        const float t2 = gf(p, G_T2, l), t3 = gf(p, G_T3, l);   // the wall value is 0
+        if (p.vel_interp) { m.ux = t2 * ux2 - t3 * ux3; m.uy = t2 * uy2 - t3 * uy3; }
+        if (p.mom_interp) { mxxp = t2 * mx2 - t3 * mx3; myyp = t2 * my2 - t3 * my3; }
+    }
+    if (p.closure == CLOSURE_STRONG) {
+        const float c = gf(p, G_CTH, l), s = gf(p, G_STH, l);
+        closure_strong(p, l, g, m.ux * c + m.uy * s, m.uy * c - m.ux * s, mxxp, myyp, m);
+    }
+    if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
+    if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    float go[Q];
+    collide(p, m, go);
+    store(p, i, j, go);
+    // momentum exchange (2d_mrlbm.f90:558-591) accumulated in FP64 from w_k + g_k
+    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    double fxo = 0.0, fyo = 0.0, fxi = 0.0, fyi = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double wk = (double)p.w[k];
+        if ((Os >> k) & 1) { const double v = wk + (double)go[k]; fxo += v * ex(k); fyo += v * ey(k); }
+        if ((Is >> k) & 1) { const double v = wk + (double)g[k]; fxi += v * ex(k); fyi += v * ey(k); }
+    }
+    Fx = fxi - fxo;
+    Fy = fyi - fyo;
+    if (p.node_force) { p.node_force[2 * l] = Fx; p.node_force[2 * l + 1] = Fy; }
+}
+
+__device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
+    const int cls = node_class(p, i, j);
+    if (cls >= 0) return;
+    float g[Q];
+    gather(p, i, j, g);
+    Mac m = moments(p, g);
+    if (i == 1 || i == p.L.nx || j == 1 || j == p.L.ny) edge_node(p, i, j, g, m);
+    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
+    if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
+    if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    float go[Q];
+    collide(p, m, go);
+    store(p, i, j, go);
+}
+
+struct Physics {
+    using P = StepParams<float>;
+    static __device__ __forceinline__ void bulk_node(const P& p, int i, int j) { fp32::bulk_node(p, i, j); }
+    static __device__ __forceinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
+        fp32::boundary_node(p, l, Fx, Fy);
+    }
+    static __device__ __forceinline__ double inlet_rho(const P& p, int j) {
+        float g[Q];
+        gather(p, 1, j, g);
+        Mac m = moments(p, g);
+        edge_node(p, 1, j, g, m);                // (1,j) is always an edge node
+        return 1.0 + (double)m.drho;
+    }
+};
+
+}  // namespace fp32
+}  // namespace mrlbm

@@ -18,7 +18,7 @@
 // node's result is bit-identical to the reference's FP64 arithmetic.
 #pragma once
 #include <cuda_runtime.h>
-#include "step_params.h"
+#include "step_common.cuh"
 
 namespace mrlbm {
 namespace fp64 {
@@ -26,23 +26,6 @@ namespace fp64 {
 using P = StepParams<double>;
 
 struct Mac { double rho, ux, uy, mxx, myy, mxy; };
-
-// f(i,j,:) of this step = fout of the previous step at the streaming sources.
-__device__ __forceinline__ void gather(const P& p, int i, int j, double f[Q]) {
-    const int nx = p.L.nx, ny = p.L.ny;
-    const int pitch = p.L.pitch, plane = (int)p.L.plane;
-    if (i > 1 && i < nx && j > 1 && j < ny) {
-        const double* s = p.src + ((int)(j * pitch + i + p.L.off));
-#pragma unroll
-        for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
-    } else {
-#pragma unroll
-        for (int k = 0; k < Q; ++k) {
-            SrcSlot sl = stream_source(nx, ny, i, j, k, p.xper, p.yper, p.freeslip);
-            f[k] = __ldg(p.src + p.L.at(sl.i, sl.j, sl.k));
-        }
-    }
-}
 
 // Macroscopic variables, 2d_mrlbm.f90:235-242.
 __device__ __forceinline__ Mac moments(const double f[Q], double hm, double hp) {
@@ -215,24 +198,6 @@ __device__ __forceinline__ void collide(const P& p, const Mac& m, double fo[Q]) 
     fo[6] = w5 * ((((1.0 - t8) + ap) + bp) - c);
     fo[7] = w5 * ((((1.0 - t5) + ap) + bp) + c);
     fo[8] = w5 * ((((1.0 + t8) + ap) + bp) - c);
-}
-
-__device__ __forceinline__ void store(const P& p, int i, int j, const double fo[Q]) {
-    double* d = p.dst + ((int)(j * p.L.pitch + i + p.L.off));
-    const int plane = (int)p.L.plane;
-#pragma unroll
-    for (int k = 0; k < Q; ++k) d[k * plane] = fo[k];
-}
-
-__device__ __forceinline__ void store_macro(const P& p, int i, int j, const Mac& m) {
-    const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1);
-    const int64_t N = (int64_t)p.L.nx * p.L.ny;
-    p.macro[n] = m.rho;
-    p.macro[N + n] = m.ux;
-    p.macro[2 * N + n] = m.uy;
-    p.macro[3 * N + n] = m.mxx;
-    p.macro[4 * N + n] = m.myy;
-    p.macro[5 * N + n] = m.mxy;
 }
 
 // Post-boundary-condition macroscopic values of a non-cylinder node.
@@ -426,7 +391,7 @@ __device__ __noinline__ void boundary_node(const P& p, int l, double& Fx, double
         closure_unrotated(p, l, f, m.ux, m.uy, m);
     }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, m);
+    if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
@@ -445,9 +410,7 @@ __device__ __noinline__ void boundary_node(const P& p, int l, double& Fx, double
 
 // Bulk node (fluid or solid, including edges).
 __device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
-    int cls = CLS_FLUID;
-    const unsigned bx = (unsigned)(i - p.box_x0), by = (unsigned)(j - p.box_y0);
-    if (bx < (unsigned)p.box_w && by < (unsigned)p.box_h) cls = __ldg(p.boxmap + by * p.box_w + bx);
+    const int cls = node_class(p, i, j);
     if (cls >= 0) return;                       // curved-wall node: owned by a boundary block
     double f[Q];
     gather(p, i, j, f);
@@ -455,84 +418,24 @@ __device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
     if (i == 1 || i == p.L.nx || j == 1 || j == p.L.ny) edge_node(p, i, j, f, m);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, m);
+    if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
 }
 
-// Block reduction of three doubles with warp shuffles; result valid in thread 0.
-__device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, double* sm) {
-    const unsigned full = 0xffffffffu;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(full, a, o);
-        b += __shfl_down_sync(full, b, o);
-        c += __shfl_down_sync(full, c, o);
+struct Physics {
+    using P = StepParams<double>;
+    static __device__ __forceinline__ void bulk_node(const P& p, int i, int j) { fp64::bulk_node(p, i, j); }
+    static __device__ __forceinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
+        fp64::boundary_node(p, l, Fx, Fy);
     }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane == 0) { sm[3 * wid] = a; sm[3 * wid + 1] = b; sm[3 * wid + 2] = c; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        a = sm[0]; b = sm[1]; c = sm[2];
-        for (int w = 1; w < nw; ++w) { a += sm[3 * w]; b += sm[3 * w + 1]; c += sm[3 * w + 2]; }
+    static __device__ __forceinline__ double inlet_rho(const P& p, int j) {
+        double f[Q];
+        gather(p, 1, j, f);
+        return node_macro(p, 1, j, f).rho;
     }
-}
-
-__device__ __forceinline__ void boundary_block(const P& p) {
-    __shared__ double sm[3 * 32];
-    __shared__ unsigned ticket;
-    const int nthr = blockDim.x;
-    const int l = blockIdx.x * nthr + threadIdx.x;
-    double Fx = 0.0, Fy = 0.0, rin = 0.0;
-    if (l < p.nb) boundary_node(p, l, Fx, Fy);
-    if (!p.do_stats) return;
-    if (!p.xper) {                              // sum(rho(1,:)) for the inlet mean (2d_mrlbm.f90:359)
-        for (int j = 1 + l; j <= p.L.ny; j += p.nbblk * nthr) {
-            double f[Q];
-            gather(p, 1, j, f);
-            Mac m = node_macro(p, 1, j, f);
-            rin += m.rho;
-        }
-    }
-    block_reduce3(Fx, Fy, rin, sm);
-    if (threadIdx.x == 0) {
-        p.partials[3 * blockIdx.x] = Fx;
-        p.partials[3 * blockIdx.x + 1] = Fy;
-        p.partials[3 * blockIdx.x + 2] = rin;
-        __threadfence();
-        ticket = atomicAdd(p.counter, 1u);
-        if (ticket == (unsigned)(p.nbblk - 1)) {
-            __threadfence();
-            double a = 0.0, b = 0.0, c = 0.0;
-            for (int q = 0; q < p.nbblk; ++q) {
-                a += __ldcg(p.partials + 3 * q);
-                b += __ldcg(p.partials + 3 * q + 1);
-                c += __ldcg(p.partials + 3 * q + 2);
-            }
-            if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = a; p.rec[2] = b; p.rec[3] = c; }
-            *p.counter = 0u;
-        }
-    }
-}
-
-template <int BX, int BY, int NJ>
-__global__ void __launch_bounds__(BX * BY, 1024 / (BX * BY)) step_kernel(const P p) {
-    if ((int)blockIdx.x < p.nbblk) {
-        boundary_block(p);
-        return;
-    }
-    const int t = blockIdx.x - p.nbblk;
-    const int tx = t % p.tiles_x, ty = t / p.tiles_x;
-    const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
-    const int i = 1 + tx * BX + lx;
-    if (i > p.L.nx) return;
-#pragma unroll
-    for (int r = 0; r < NJ; ++r) {
-        const int j = 1 + ty * BY * NJ + r * BY + ly;
-        if (j <= p.L.ny) bulk_node(p, i, j);
-    }
-}
+};
 
 }  // namespace fp64
 }  // namespace mrlbm

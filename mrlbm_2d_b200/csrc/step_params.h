@@ -9,17 +9,33 @@ namespace mrlbm {
 // sum(rho(1,:)) -- the values of 2d_mrlbm.f90:359 and 488-494.
 constexpr int REC_WORDS = 4;
 
-// Constants of the deviation (FP32) form, precomputed in FP64 on the host from the
-// reference's single-rounded weights so the FP32 kernel works only with small quantities.
+// Constants of the deviation (FP32) form, computed once in FP64 on the host from the
+// reference's single-rounded weights w_k and FP64 Hermite tables H_k.  Each is the rest-state
+// part of a closure that cancels in exact arithmetic; with single-rounded weights it is
+// O(1e-9) and is added back so the FP32 step keeps the FP64 step's arithmetic content.
+// SW_ab(e) = sum over edge e's incoming set of w_k H_ab,k; W(e) = sum of w_k over it.
 struct DevConsts {
-    float eps_mass;        // sum(w) - 1   (the reference's weights sum to 1 + 7.45e-9)
-    float cxx, cyy;        // sum_k w_k Hxx_k, sum_k w_k Hyy_k
-    // edge closures, per edge e in {outlet, inlet, top, bottom}:
-    float wI[4];           // sum_{Is} w
-    float swxx[4], swyy[4], swxy[4];   // sum_{Is} w H
-    // cylinder closure, per label (0..15):
-    float lab_wI[16];      // sum_{Is} w  ( == sum_{Os} w for every handled label)
+    float eps_mass;          // sum_k w_k - 1
+    float cxx, cyy;          // sum_k w_k H_xx,k, sum_k w_k H_yy,k
+    float k_out_mxx;         // outlet: 1 + 9 SW_xx
+    float sw_out_yy;         //         SW_yy
+    float k_in_rho;          // inlet:  4 W + 3 SW_xx - 3
+    float k_in_mxx;          //         1 + 9 SW_xx
+    float sw_in_yy;          //         SW_yy
+    float k_in_rho_inc;      //         6 W - 5                       (apply_bc_incomp)
+    float k_w_rho[2];        // walls (top, bottom): 12 W - 9 - omega + 9 (1 - omega) SW_yy
+    float sw_w_xx[2];        //         SW_xx
+    float k_w_myy[2];        //         1 + 9 SW_yy
+    float k_w_rho_inc[2];    //         6 W - 5                       (apply_bc_incomp)
+    float w_wall[2];         //         W
+    float lab_w[16];         // curved wall: sum of w_k over the label's Is (== over its Os)
 };
+
+// A population of the loaded state that the buffer cannot hold: with periodic wraps
+// (and free-slip with x-periodic) the reference copies one corner population to two
+// destinations (2d_mrlbm.f90:519-535), so after any step those two agree; a loaded state
+// may not.  Such destinations are served from this list on the first step after a load.
+struct OvrEntry { int i, j, k, pad; double v; };
 
 template <class T>
 struct StepParams {
@@ -32,6 +48,8 @@ struct StepParams {
     T omega, omega1;              // omega and (1 - omega)
     T uinlet, vinlet;
     const T* u_in;                // optional per-row inlet velocity (ny entries) or null
+    const OvrEntry* ovr;          // loaded-state overrides for this step, or null
+    int n_ovr;
     int xper, yper, freeslip, walls_ref, incomp_bc, incomp_bulk;
     int zero_solid_u;             // plot step: u = 0 at solid nodes (2d_mrlbm.f90:375-384)
     int do_stats;                 // stats step: forces + inlet density sum

@@ -14,6 +14,8 @@ from cases import CASES
 pytestmark = pytest.mark.gpu
 
 RTOL_SUM = 1e-12
+# absolute bound for a re-associated sum of ~1e3 per-node terms of magnitude <= 1e-1
+ATOL_FORCE = 1e-13
 
 
 def _assert_exact(a, b, what):
@@ -42,8 +44,8 @@ def _run(mrlbm, oracle_mod, cfg, chunks, inlet=None):
     it_g, fd_g, fl_g, rin_g = s.forces()
     assert np.array_equal(it_o, it_g)
     if cfg.channel_with_cylinder:
-        np.testing.assert_allclose(fd_g, fd_o, rtol=RTOL_SUM, atol=1e-15)
-        np.testing.assert_allclose(fl_g, fl_o, rtol=RTOL_SUM, atol=1e-15)
+        np.testing.assert_allclose(fd_g, fd_o, rtol=RTOL_SUM, atol=ATOL_FORCE)
+        np.testing.assert_allclose(fl_g, fl_o, rtol=RTOL_SUM, atol=ATOL_FORCE)
     np.testing.assert_allclose(rin_g, rin_o, rtol=RTOL_SUM)
     assert s.status() == 0
     s.close()
