@@ -157,7 +157,9 @@ int mrlbm_set_inlet_profile(mrlbm_handle* h, const double* u_in);
 #define MRLBM_STEP_MACRO   1
 int mrlbm_step(mrlbm_handle* h, int32_t nsteps, int32_t flags);
 
-/* Current iteration number (the reference's iter after the last step). */
+/* Current iteration number (the reference's iter after the last step).  A new handle is at
+ * iteration 1: the reference's restart_step starts at 1 (2d_mrlbm.f90:7), so its first step
+ * is iter 2 (2d_mrlbm.f90:229). */
 int mrlbm_get_iter(const mrlbm_handle* h, int32_t* iter);
 
 /* Macroscopic fields of the last step run with MRLBM_STEP_MACRO, after the Dirichlet and

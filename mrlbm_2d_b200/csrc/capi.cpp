@@ -404,7 +404,7 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
          ck(cudaMalloc((void**)&h->d_bint, nint * sizeof(int)), "cudaMalloc tables");
     const size_t nbox = std::max<size_t>(h->geo.boxmap.size(), 1);
     ok = ok && ck(cudaMalloc((void**)&h->d_boxmap, nbox * sizeof(int)), "cudaMalloc boxmap");
-    const int max_blk = nb / 64 + 2;
+    const int max_blk = nb / 16 + 2;
     ok = ok && ck(cudaMalloc((void**)&h->d_partials, (size_t)max_blk * 3 * sizeof(double)), "cudaMalloc partials") &&
          ck(cudaMalloc((void**)&h->d_counter, sizeof(unsigned)), "cudaMalloc counter") &&
          ck(cudaMalloc((void**)&h->d_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMalloc ring") &&
@@ -429,7 +429,9 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
     initial_state(h->cfg, h->lat, nx, ny, f0);
     int urc = upload_state(h, f0.data());
     if (urc != MRLBM_OK) { std::string m = h->err; return bail(urc, m); }
-    h->iter = 0;
+    // the main loop runs iter = restart_step+1, ... with restart_step initialised to 1
+    // (2d_mrlbm.f90:7, 229): a fresh run's first step is iter 2
+    h->iter = 1;
     *out = h;
     return MRLBM_OK;
 }

@@ -78,20 +78,84 @@ __device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, d
     }
 }
 
-// Boundary blocks: curved-wall nodes, then (stats steps) the momentum-exchange force and
-// the inlet density sum, reduced across blocks; the last block to arrive writes the record.
+// Boundary blocks own BNODES curved-wall nodes each, BLANES lanes per node.  The block first
+// stages its nodes' tables in shared memory with coalesced loads.  Lane c of a node then
+// pulls stencil node c (reference point 2 for c < 4, point 3 otherwise), computes its
+// velocity and rotated moments, and the bilinear interpolation is completed with shuffles
+// in the reference's operation order: (1-xd)*v1 + xd*v2 per row, then (1-yd)*a0 + yd*a1
+// (2d_mrlbm.f90:786-793, 869-876).  Lane 0 runs the closure, collision, store and force.
+constexpr int BNODES = 32;        // at most (256-thread blocks); blockDim.x / BLANES in general
+constexpr int BLANES = 8;
+constexpr int G_STAGED = G_SCC;   // GeoFields 0 .. G_SCC-1 live in shared memory
+
+template <class T>
+struct BTab {
+    const T* g;
+    const int* i;
+    int n;                            // nodes per block (row stride of the staged tables)
+    __device__ __forceinline__ T gf(int field, int li) const { return g[field * n + li]; }
+    __device__ __forceinline__ int gi(int field, int li) const { return i[field * n + li]; }
+};
+
 template <class Phys>
 __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
+    using T = typename Phys::T;
+    __shared__ T sg[G_STAGED * BNODES];
+    __shared__ int sgi[I_NFIELDS * BNODES];
     __shared__ double sm[3 * 32];
-    const int nthr = blockDim.x;
-    const int l = blockIdx.x * nthr + threadIdx.x;
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int bn = nthr / BLANES;
+    const int l0 = blockIdx.x * bn;
+    for (int idx = tid; idx < G_STAGED * bn; idx += nthr) {
+        const int f = idx / bn, n = idx - f * bn;
+        sg[idx] = (l0 + n < p.nb) ? p.bgeo[f * p.nb + l0 + n] : T(0);
+    }
+    for (int idx = tid; idx < I_NFIELDS * bn; idx += nthr) {
+        const int f = idx / bn, n = idx - f * bn;
+        sgi[idx] = (l0 + n < p.nb) ? p.bint[f * p.nb + l0 + n] : 0;
+    }
+    __syncthreads();
+    const BTab<T> tb{sg, sgi, bn};
+    const int li = tid / BLANES, lane = tid % BLANES;
+    const int l = l0 + li;
+    const bool active = l < p.nb;
+    const bool interp = p.closure == CLOSURE_UNROTATED || p.vel_interp || p.mom_interp;
+    T ux = T(0), uy = T(0), mx = T(0), my = T(0);
+    const int r = lane >> 2, c = lane & 3;        // reference point 2 + r, corner c
+    const T xd = active ? tb.gf(r == 0 ? G_XD2 : G_XD3, li) : T(0);
+    const T yd = active ? tb.gf(r == 0 ? G_YD2 : G_YD3, li) : T(0);
+    if (active && interp) {
+        const int s = 4 * r + c;
+        const T cc = p.bgeo[(G_SCC + s) * p.nb + l], ss = p.bgeo[(G_SSS + s) * p.nb + l];
+        const T s2 = p.bgeo[(G_SS2 + s) * p.nb + l];
+        Phys::stencil_node(p, tb.gi(I_SI + s, li), tb.gi(I_SJ + s, li), cc, ss, s2, ux, uy, mx, my);
+        const T wx = (c & 1) ? xd : (T(1) - xd);
+        ux = wx * ux; uy = wx * uy; mx = wx * mx; my = wx * my;
+    }
+    const unsigned full = 0xffffffffu;
+    // row sums (corner pairs 0+1, 2+3)
+    ux = ux + __shfl_down_sync(full, ux, 1, BLANES);
+    uy = uy + __shfl_down_sync(full, uy, 1, BLANES);
+    mx = mx + __shfl_down_sync(full, mx, 1, BLANES);
+    my = my + __shfl_down_sync(full, my, 1, BLANES);
+    // column combination (1-yd)*a0 + yd*a1 at corners 0 (ref 2, lane 0) and 4 (ref 3, lane 4)
+    {
+        const T ux1 = __shfl_down_sync(full, ux, 2, BLANES), uy1 = __shfl_down_sync(full, uy, 2, BLANES);
+        const T mx1 = __shfl_down_sync(full, mx, 2, BLANES), my1 = __shfl_down_sync(full, my, 2, BLANES);
+        ux = (T(1) - yd) * ux + yd * ux1;
+        uy = (T(1) - yd) * uy + yd * uy1;
+        mx = (T(1) - yd) * mx + yd * mx1;
+        my = (T(1) - yd) * my + yd * my1;
+    }
+    const T ux3 = __shfl_down_sync(full, ux, 4, BLANES), uy3 = __shfl_down_sync(full, uy, 4, BLANES);
+    const T mx3 = __shfl_down_sync(full, mx, 4, BLANES), my3 = __shfl_down_sync(full, my, 4, BLANES);
     double Fx = 0.0, Fy = 0.0, rin = 0.0;
-    if (l < p.nb) Phys::boundary_node(p, l, Fx, Fy);
+    if (active && lane == 0) Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
     if (!p.do_stats) return;
-    if (!p.xper)
-        for (int j = 1 + l; j <= p.L.ny; j += p.nbblk * nthr) rin += Phys::inlet_rho(p, j);
+    // sum(rho(1,:)) for the inlet running mean (2d_mrlbm.f90:359), whatever the x boundary
+    for (int j = 1 + blockIdx.x * nthr + tid; j <= p.L.ny; j += p.nbblk * nthr) rin += Phys::inlet_rho(p, j);
     block_reduce3(Fx, Fy, rin, sm);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         p.partials[3 * blockIdx.x] = Fx;
         p.partials[3 * blockIdx.x + 1] = Fy;
         p.partials[3 * blockIdx.x + 2] = rin;
@@ -99,13 +163,13 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
         const unsigned ticket = atomicAdd(p.counter, 1u);
         if (ticket == (unsigned)(p.nbblk - 1)) {
             __threadfence();
-            double a = 0.0, b = 0.0, c = 0.0;
+            double a = 0.0, b = 0.0, cc = 0.0;
             for (int q = 0; q < p.nbblk; ++q) {
                 a += __ldcg(p.partials + 3 * q);
                 b += __ldcg(p.partials + 3 * q + 1);
-                c += __ldcg(p.partials + 3 * q + 2);
+                cc += __ldcg(p.partials + 3 * q + 2);
             }
-            if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = a; p.rec[2] = b; p.rec[3] = c; }
+            if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = a; p.rec[2] = b; p.rec[3] = cc; }
             *p.counter = 0u;
         }
     }
@@ -134,7 +198,9 @@ __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const typename Phys
 template <class Phys, int BX, int BY, int NJ, int MINB>
 int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     const int nthr = BX * BY;
-    p.nbblk = p.nb > 0 ? (p.nb + nthr - 1) / nthr : 1;
+    static_assert(BX * BY % BLANES == 0 && BX * BY / BLANES <= BNODES, "boundary block size");
+    const int bn = nthr / BLANES;
+    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
     const long long nblocks = (long long)p.nbblk + (long long)p.tiles_x * tiles_y;

@@ -165,32 +165,16 @@ __device__ __forceinline__ void collide(const P& p, const Mac& m, float go[Q]) {
     go[8] = p.w[5] * (d + r * ((bd - C) + tm));
 }
 
-__device__ __forceinline__ float gf(const P& p, int field, int l) { return p.bgeo[field * p.nb + l]; }
-__device__ __forceinline__ int gi(const P& p, int field, int l) { return p.bint[field * p.nb + l]; }
-
-// Velocity and rotated moments at reference point r (2 or 3), bilinear over 4 stencil nodes.
-__device__ __noinline__ void ref_point(const P& p, int l, int r, float& uxr, float& uyr, float& mxxr, float& myyr) {
-    float uxv[4], uyv[4], mxv[4], myv[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int s = (r - 2) * 4 + c;
-        float g[Q];
-        gather(p, gi(p, I_SI + s, l), gi(p, I_SJ + s, l), g);
-        const Mac m = moments(p, g);
-        uxv[c] = m.ux;
-        uyv[c] = m.uy;
-        const float cc = gf(p, G_SCC + s, l), ss = gf(p, G_SSS + s, l), s2 = gf(p, G_SS2 + s, l);
-        mxv[c] = m.mxx * cc + m.myy * ss + m.mxy * s2;
-        myv[c] = m.mxx * ss + m.myy * cc - m.mxy * s2;
-    }
-    const float xd = gf(p, r == 2 ? G_XD2 : G_XD3, l), yd = gf(p, r == 2 ? G_YD2 : G_YD3, l);
-    auto bil = [&](const float v[4]) {
-        return (1.0f - yd) * ((1.0f - xd) * v[0] + xd * v[1]) + yd * ((1.0f - xd) * v[2] + xd * v[3]);
-    };
-    uxr = bil(uxv);
-    uyr = bil(uyv);
-    mxxr = bil(mxv);
-    myyr = bil(myv);
+// Velocity and rotated second moments of one bilinear stencil node (2d_mrlbm.f90:842-867).
+__device__ __forceinline__ void stencil_node(const P& p, int si, int sj, float cc, float ss, float s2, float& ux,
+                                             float& uy, float& mx, float& my) {
+    float g[Q];
+    gather(p, si, sj, g);
+    const Mac m = moments(p, g);
+    ux = m.ux;
+    uy = m.uy;
+    mx = m.mxx * cc + m.myy * ss + m.mxy * s2;
+    my = m.mxx * ss + m.myy * cc - m.mxy * s2;
 }
 
 // numerical_boundary_cases_rotation (2d_mrlbm.f90:1635-1765) in deviation form.  With
@@ -198,17 +182,17 @@ __device__ __noinline__ void ref_point(const P& p, int l, int r, float& uxr, flo
 // cancel exactly:  rho_I = W + G,  G' = W + (a1 + omega e2),  D_xy = SW_xy + d1, so
 //   R_xy = d1 - SG_xy - S_xy (a1 + omega e2 - G) / rho_I,
 //   den  = W + dden,  dden = a1 + (1-omega)(M'.B') + omega e2,  drho = (G - dden) / den.
-__device__ __noinline__ void closure_strong(const P& p, int l, const float g[Q], float uxp, float uyp, float Mxx,
-                                            float Myy, Mac& m) {
-    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
-    const int label = gi(p, I_LABEL, l);
+__device__ __noinline__ void closure_strong(const P& p, const BTab<float>& tb, int li, const float g[Q], float uxp,
+                                            float uyp, float Mxx, float Myy, Mac& m) {
+    const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
+    const int label = tb.gi(I_LABEL, li);
     const float om = p.omega, om1 = p.omega1;
     float a1 = 0.f, e2 = 0.f, B11 = 0.f, B22 = 0.f, B12 = 0.f;
     float G = 0.f, SWxy = 0.f, SGxy = 0.f, d1 = 0.f, F11 = 0.f, F22 = 0.f, F12 = 0.f;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-        const float cxp = gf(p, G_CXP + k, l), cyp = gf(p, G_CYP + k, l);
-        const float hxx = gf(p, G_HXXP + k, l), hyy = gf(p, G_HYYP + k, l), hxy = gf(p, G_HXYP + k, l);
+        const float cxp = tb.gf(G_CXP + k, li), cyp = tb.gf(G_CYP + k, li);
+        const float hxx = tb.gf(G_HXXP + k, li), hyy = tb.gf(G_HYYP + k, li), hxy = tb.gf(G_HXYP + k, li);
         const float wk = p.w[k];
         const float ak = 3.0f * wk * (uxp * cxp + uyp * cyp);
         const float ek = 4.5f * wk * ((uxp * uxp) * hxx + (uyp * uyp) * hyy + 2.0f * (uxp * uyp) * hxy);
@@ -234,37 +218,35 @@ __device__ __noinline__ void closure_strong(const P& p, int l, const float g[Q],
     const float dden = a1 + om1 * (Mxx * B11 + Myy * B22 + 2.0f * Mxy * B12) + om * e2;
     m.drho = (G - dden) / (W + dden);
     m.rho = 1.0f + m.drho;
-    const float cc = gf(p, G_CC, l), ss = gf(p, G_SS, l), s2 = gf(p, G_S2TH, l), c2 = gf(p, G_C2TH, l);
+    const float cc = tb.gf(G_CC, li), ss = tb.gf(G_SS, li), s2 = tb.gf(G_S2TH, li), c2 = tb.gf(G_C2TH, li);
     m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
     m.myy = Mxx * ss + Myy * cc + Mxy * s2;
     m.mxy = (Mxx - Myy) * 0.5f * s2 + Mxy * c2;
 }
 
-__device__ __noinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
-    const int i = gi(p, I_NODEI, l), j = gi(p, I_NODEJ, l);
+// Lane 0 of a boundary node: extrapolation (wall value 0), closure, collision, store and
+// the momentum-exchange force accumulated in FP64 from w_k + g_k (2d_mrlbm.f90:558-591).
+__device__ __noinline__ void boundary_close(const P& p, const BTab<float>& tb, int li, int l, float ux2, float uy2,
+                                            float mx2, float my2, float ux3, float uy3, float mx3, float my3,
+                                            double& Fx, double& Fy) {
+    const int i = tb.gi(I_NODEI, li), j = tb.gi(I_NODEJ, li);
     float g[Q];
     gather(p, i, j, g);
     Mac m = moments(p, g);
     float mxxp = 0.f, myyp = 0.f;
-    if (p.vel_interp || p.mom_interp) {
-        float ux2, uy2, mx2, my2, ux3, uy3, mx3, my3;
-        ref_point(p, l, 2, ux2, uy2, mx2, my2);
-        ref_point(p, l, 3, ux3, uy3, mx3, my3);
-        const float t2 = gf(p, G_T2, l), t3 = gf(p, G_T3, l);   // the wall value is 0
-        if (p.vel_interp) { m.ux = t2 * ux2 - t3 * ux3; m.uy = t2 * uy2 - t3 * uy3; }
-        if (p.mom_interp) { mxxp = t2 * mx2 - t3 * mx3; myyp = t2 * my2 - t3 * my3; }
-    }
+    const float t2 = tb.gf(G_T2, li), t3 = tb.gf(G_T3, li);
+    if (p.vel_interp) { m.ux = t2 * ux2 - t3 * ux3; m.uy = t2 * uy2 - t3 * uy3; }
+    if (p.mom_interp) { mxxp = t2 * mx2 - t3 * mx3; myyp = t2 * my2 - t3 * my3; }
     if (p.closure == CLOSURE_STRONG) {
-        const float c = gf(p, G_CTH, l), s = gf(p, G_STH, l);
-        closure_strong(p, l, g, m.ux * c + m.uy * s, m.uy * c - m.ux * s, mxxp, myyp, m);
+        const float c = tb.gf(G_CTH, li), s = tb.gf(G_STH, li);
+        closure_strong(p, tb, li, g, m.ux * c + m.uy * s, m.uy * c - m.ux * s, mxxp, myyp, m);
     }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     float go[Q];
     collide(p, m, go);
     store(p, i, j, go);
-    // momentum exchange (2d_mrlbm.f90:558-591) accumulated in FP64 from w_k + g_k
-    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     double fxo = 0.0, fyo = 0.0, fxi = 0.0, fyi = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
@@ -294,9 +276,16 @@ __device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
 
 struct Physics {
     using P = StepParams<float>;
+    using T = float;
     static __device__ __forceinline__ void bulk_node(const P& p, int i, int j) { fp32::bulk_node(p, i, j); }
-    static __device__ __forceinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
-        fp32::boundary_node(p, l, Fx, Fy);
+    static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
+                                                        T& mx, T& my) {
+        fp32::stencil_node(p, si, sj, cc, ss, s2, ux, uy, mx, my);
+    }
+    static __device__ __forceinline__ void boundary_close(const P& p, const BTab<T>& tb, int li, int l, T ux2, T uy2,
+                                                          T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
+                                                          double& Fy) {
+        fp32::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
     static __device__ __forceinline__ double inlet_rho(const P& p, int j) {
         float g[Q];

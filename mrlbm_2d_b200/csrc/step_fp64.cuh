@@ -209,54 +209,31 @@ __device__ __forceinline__ Mac node_macro(const P& p, int i, int j, const double
 
 // ---------------------------------------------------------------------------------------
 // Curved-wall boundary node (2d_mrlbm.f90:294-311 and the routines they call).
-__device__ __forceinline__ double gf(const P& p, int field, int l) { return p.bgeo[field * p.nb + l]; }
-__device__ __forceinline__ int gi(const P& p, int field, int l) { return p.bint[field * p.nb + l]; }
 
-// Bilinear value at reference point r (2 or 3) of boundary node l of velocity and rotated
-// moments (velocity_interpolation_boundary_nodes 2d_mrlbm.f90:782-806 and
-// moments_interpolation_boundary_nodes 2d_mrlbm.f90:837-916).
-__device__ __noinline__ void ref_point(const P& p, int l, int r, double& uxr, double& uyr, double& mxxr, double& myyr) {
-    double uxv[4], uyv[4], mxv[4], myv[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int s = (r - 2) * 4 + c;
-        const int si = gi(p, I_SI + s, l), sj = gi(p, I_SJ + s, l);
-        double f[Q];
-        gather(p, si, sj, f);
-        Mac m = moments(f, p.hm, p.hp);
-        uxv[c] = m.ux;
-        uyv[c] = m.uy;
-        const double cc = gf(p, G_SCC + s, l), ss = gf(p, G_SSS + s, l), s2 = gf(p, G_SS2 + s, l);
-        mxv[c] = m.mxx * cc + m.myy * ss + m.mxy * s2;
-        myv[c] = m.mxx * ss + m.myy * cc - m.mxy * s2;
-    }
-    const double xd = gf(p, r == 2 ? G_XD2 : G_XD3, l), yd = gf(p, r == 2 ? G_YD2 : G_YD3, l);
-    double a0 = (1.0 - xd) * uxv[0] + xd * uxv[1];
-    double a1 = (1.0 - xd) * uxv[2] + xd * uxv[3];
-    uxr = (1.0 - yd) * a0 + yd * a1;
-    a0 = (1.0 - xd) * uyv[0] + xd * uyv[1];
-    a1 = (1.0 - xd) * uyv[2] + xd * uyv[3];
-    uyr = (1.0 - yd) * a0 + yd * a1;
-    a0 = (1.0 - xd) * mxv[0] + xd * mxv[1];
-    a1 = (1.0 - xd) * mxv[2] + xd * mxv[3];
-    mxxr = (1.0 - yd) * a0 + yd * a1;
-    a0 = (1.0 - xd) * myv[0] + xd * myv[1];
-    a1 = (1.0 - xd) * myv[2] + xd * myv[3];
-    myyr = (1.0 - yd) * a0 + yd * a1;
+// Velocity and rotated second moments (2d_mrlbm.f90:842-867) of one bilinear stencil node.
+__device__ __forceinline__ void stencil_node(const P& p, int si, int sj, double cc, double ss, double s2, double& ux,
+                                             double& uy, double& mx, double& my) {
+    double f[Q];
+    gather(p, si, sj, f);
+    const Mac m = moments(f, p.hm, p.hp);
+    ux = m.ux;
+    uy = m.uy;
+    mx = m.mxx * cc + m.myy * ss + m.mxy * s2;
+    my = m.mxx * ss + m.myy * cc - m.mxy * s2;
 }
 
 // Rotated closures, 2d_mrlbm.f90:1635-1765 (strong), 1873-1972 (rhoeq), 1767-1871 (weak).
-__device__ __noinline__ void closure_rotated(const P& p, int l, const double f[Q], double uxp, double uyp,
+__device__ __noinline__ void closure_rotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp, double uyp,
                                              double Mxx, double Myy, Mac& m) {
-    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     const double omega = p.omega;
     const int variant = p.closure;
     double rhoI = 0, mxxI = 0, myyI = 0, mxyI = 0, A_p = 0, E_p = 0;
     double B11 = 0, B22 = 0, B12 = 0, D_xy = 0, F11_xy = 0, F22_xy = 0, F12_xy = 0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-        const double cxp = gf(p, G_CXP + k, l), cyp = gf(p, G_CYP + k, l);
-        const double hxx = gf(p, G_HXXP + k, l), hyy = gf(p, G_HYYP + k, l), hxy = gf(p, G_HXYP + k, l);
+        const double cxp = tb.gf(G_CXP + k, li), cyp = tb.gf(G_CYP + k, li);
+        const double hxx = tb.gf(G_HXXP + k, li), hyy = tb.gf(G_HYYP + k, li), hxy = tb.gf(G_HXYP + k, li);
         const double wk = p.w[k];
         const double A_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp);
         const double E_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp + 4.50 * (uxp * uxp) * hxx +
@@ -304,7 +281,7 @@ __device__ __noinline__ void closure_rotated(const P& p, int l, const double f[Q
         Mxy = (R - Mxx * L11 - Myy * L22) / L12;
         rhop = rhoI / E_p;
     }
-    const double cc = gf(p, G_CC, l), ss = gf(p, G_SS, l), s2 = gf(p, G_S2TH, l), c2 = gf(p, G_C2TH, l);
+    const double cc = tb.gf(G_CC, li), ss = tb.gf(G_SS, li), s2 = tb.gf(G_S2TH, li), c2 = tb.gf(G_C2TH, li);
     m.rho = rhop;
     m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
     m.myy = Mxx * ss + Myy * cc + Mxy * s2;
@@ -312,8 +289,9 @@ __device__ __noinline__ void closure_rotated(const P& p, int l, const double f[Q
 }
 
 // Unrotated closure with Cramer's rule, 2d_mrlbm.f90:1496-1633 and 1974-2003.
-__device__ __noinline__ void closure_unrotated(const P& p, int l, const double f[Q], double uxp, double uyp, Mac& m) {
-    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+__device__ __noinline__ void closure_unrotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp,
+                                               double uyp, Mac& m) {
+    const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     const double omega = p.omega, hm = p.hm, hp = p.hp;
     double rhoI = 0, mxxI = 0, myyI = 0, mxyI = 0, A_p = 0, E_p = 0, B11 = 0, B22 = 0, B12 = 0;
     double D_xx = 0, D_yy = 0, D_xy = 0, F11_xx = 0, F12_xx = 0, F22_xx = 0, F11_yy = 0, F12_yy = 0, F22_yy = 0;
@@ -359,44 +337,43 @@ __device__ __noinline__ void closure_unrotated(const P& p, int l, const double f
     m.mxy = Mxy;
 }
 
-__device__ __noinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
-    const int i = gi(p, I_NODEI, l), j = gi(p, I_NODEJ, l);
+// Lane 0 of a boundary node: extrapolated velocity / rotated moments from the reference
+// points (the wall value is 0; 2d_mrlbm.f90:809-814, 919-924), closure, collision, store,
+// momentum-exchange force (evaluate_forces, 2d_mrlbm.f90:558-591).
+__device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, int li, int l, double ux2, double uy2,
+                                            double mx2, double my2, double ux3, double uy3, double mx3, double my3,
+                                            double& Fx, double& Fy) {
+    const int i = tb.gi(I_NODEI, li), j = tb.gi(I_NODEJ, li);
     double f[Q];
     gather(p, i, j, f);
     Mac m = moments(f, p.hm, p.hp);
     const bool rotated = p.closure != CLOSURE_UNROTATED;
     double mxxp = 0.0, myyp = 0.0;
-    if (!rotated || p.vel_interp || p.mom_interp) {
-        double ux2, uy2, mx2, my2, ux3, uy3, mx3, my3;
-        ref_point(p, l, 2, ux2, uy2, mx2, my2);
-        ref_point(p, l, 3, ux3, uy3, mx3, my3);
-        const double t1 = gf(p, G_T1, l), t2 = gf(p, G_T2, l), t3 = gf(p, G_T3, l);
-        if (!rotated || p.vel_interp) {             // 2d_mrlbm.f90:813-814
-            m.ux = t1 * 0.0 + t2 * ux2 - t3 * ux3;
-            m.uy = t1 * 0.0 + t2 * uy2 - t3 * uy3;
-        }
-        if (rotated && p.mom_interp) {              // 2d_mrlbm.f90:923-924
-            mxxp = t1 * 0.0 + t2 * mx2 - t3 * mx3;
-            myyp = t1 * 0.0 + t2 * my2 - t3 * my3;
-        }
+    const double t1 = tb.gf(G_T1, li), t2 = tb.gf(G_T2, li), t3 = tb.gf(G_T3, li);
+    if (!rotated || p.vel_interp) {
+        m.ux = t1 * 0.0 + t2 * ux2 - t3 * ux3;
+        m.uy = t1 * 0.0 + t2 * uy2 - t3 * uy3;
+    }
+    if (rotated && p.mom_interp) {
+        mxxp = t1 * 0.0 + t2 * mx2 - t3 * mx3;
+        myyp = t1 * 0.0 + t2 * my2 - t3 * my3;
     }
     if (rotated) {
         if (p.closure != CLOSURE_NONE) {
-            const double c = gf(p, G_CTH, l), s = gf(p, G_STH, l);
+            const double c = tb.gf(G_CTH, li), s = tb.gf(G_STH, li);
             const double uxp = m.ux * c + m.uy * s;    // 2d_mrlbm.f90:304-305
             const double uyp = m.uy * c - m.ux * s;
-            closure_rotated(p, l, f, uxp, uyp, mxxp, myyp, m);
+            closure_rotated(p, tb, li, f, uxp, uyp, mxxp, myyp, m);
         }
     } else {
-        closure_unrotated(p, l, f, m.ux, m.uy, m);
+        closure_unrotated(p, tb, li, f, m.ux, m.uy, m);
     }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
-    // evaluate_forces, 2d_mrlbm.f90:558-591
-    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     double fxo = 0.0, fyo = 0.0, fxi = 0.0, fyi = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
@@ -426,9 +403,16 @@ __device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
 
 struct Physics {
     using P = StepParams<double>;
+    using T = double;
     static __device__ __forceinline__ void bulk_node(const P& p, int i, int j) { fp64::bulk_node(p, i, j); }
-    static __device__ __forceinline__ void boundary_node(const P& p, int l, double& Fx, double& Fy) {
-        fp64::boundary_node(p, l, Fx, Fy);
+    static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
+                                                        T& mx, T& my) {
+        fp64::stencil_node(p, si, sj, cc, ss, s2, ux, uy, mx, my);
+    }
+    static __device__ __forceinline__ void boundary_close(const P& p, const BTab<T>& tb, int li, int l, T ux2, T uy2,
+                                                          T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
+                                                          double& Fy) {
+        fp64::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
     static __device__ __forceinline__ double inlet_rho(const P& p, int j) {
         double f[Q];

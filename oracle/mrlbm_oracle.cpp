@@ -209,7 +209,8 @@ bool Oracle::setup(const mrlbm_config& c) {
             }
         }
     }
-    iter = c.irestart ? 0 : 0;
+    // restart_step is initialised to 1 (2d_mrlbm.f90:7): a fresh run's first step is iter 2
+    iter = 1;
     return true;
 }
 

@@ -1,0 +1,104 @@
+"""Parity against outputs of the reference's own source.
+
+tests/golden/*.npz were produced by tests/golden/make_golden.py, which executes
+2d_mrlbm.f90 (unmodified) with the Fortran-subset interpreter in tests/golden/ on small inputs
+the reference can express.  Each fixture holds the input.dat used, an optional restart state
+(read through the reference's irestart path), the populations/fields it wrote to
+restart/restart.dat, its forces_time.dat records, its PLOT3D function files and theta.dat.
+
+CPU tests pin the oracle to those fixtures (bit for bit); the GPU tests pin the FP64 CUDA
+step to them directly through the C ABI.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+NAMES = [os.path.basename(f)[:-4] for f in FIXTURES]
+ATOL_FORCE = 1e-13
+
+
+def _load(name):
+    return dict(np.load(os.path.join(HERE, "golden", name + ".npz")))
+
+
+def _config(mrlbm, d, tmp_path):
+    p = tmp_path / "input.dat"
+    p.write_text(str(d["input_dat"]))
+    c = mrlbm.config_from_namelist(str(p))
+    return c.replace(num_threads=2)
+
+
+def _snapshots(d):
+    return sorted(int(k[2:]) for k in d if k.startswith("f_") and k[2:].isdigit())
+
+
+def _plot_steps(d):
+    return sorted(int(k[7:]) for k in d if k.startswith("plot3d_"))
+
+
+def test_fixtures_present():
+    assert len(FIXTURES) >= 9
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_matches_reference_execution(mrlbm, oracle_mod, tmp_path, name):
+    d = _load(name)
+    cfg = _config(mrlbm, d, tmp_path)
+    o = oracle_mod.Oracle(cfg)
+    nx, ny = int(d["nx"]), int(d["ny"])
+    assert (o.nx, o.ny) == (nx, ny)
+    assert np.array_equal(o.get("thetas_cy"), d["theta"])
+    if "restart_in_f" in d:
+        o.set_state(np.ascontiguousarray(d["restart_in_f"].transpose(2, 1, 0)).ravel())
+        o.set_iter(int(d["restart_in_iter"]))
+    it = int(o.scalars()["iter"])
+    events = [t for t in sorted(set(_snapshots(d)) | set(_plot_steps(d))) if t > it]
+    for t in events:
+        o.step(t - it)
+        it = t
+        if f"f_{t}" in d:
+            assert np.array_equal(o.field("f"), d[f"f_{t}"]), f"populations at iter {t}"
+            for n in ("rho", "ux", "uy"):
+                assert np.array_equal(o.field(n), d[f"{n}_{t}"]), f"{n} at iter {t}"
+        if f"plot3d_{t}" in d:
+            p3 = d[f"plot3d_{t}"]                    # float32 (3, ny, nx): rho, ux, uy
+            for q, n in enumerate(("rho", "ux", "uy")):
+                assert np.array_equal(o.field(n).astype(np.float32).T, p3[q]), f"PLOT3D {n} at iter {t}"
+    its, fd, fl, _ = o.forces()
+    ref = d["forces"]
+    assert np.array_equal(its, ref[:, 0].astype(int))
+    assert np.array_equal(fd, ref[:, 1]) and np.array_equal(fl, ref[:, 2])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_fp64_gpu_matches_reference_execution(mrlbm, tmp_path, name):
+    d = _load(name)
+    cfg = _config(mrlbm, d, tmp_path)
+    s = mrlbm.Simulation(cfg, precision=mrlbm.FP64)
+    if "restart_in_f" in d:
+        s.load_state(d["restart_in_f"], iter=int(d["restart_in_iter"]))
+    it = s.iter
+    events = [t for t in sorted(set(_snapshots(d)) | set(_plot_steps(d))) if t > it]
+    for t in events:
+        s.step(t - it, macro=True)
+        it = t
+        mac = s.macro()
+        if f"f_{t}" in d:
+            assert np.array_equal(s.get_state(), d[f"f_{t}"]), f"populations at iter {t}"
+            for n in ("rho", "ux", "uy"):
+                assert np.array_equal(mac[n], d[f"{n}_{t}"]), f"{n} at iter {t}"
+        if f"plot3d_{t}" in d:
+            p3 = d[f"plot3d_{t}"]
+            for q, n in enumerate(("rho", "ux", "uy")):
+                assert np.array_equal(mac[n].astype(np.float32).T, p3[q]), f"PLOT3D {n} at iter {t}"
+    its, fd, fl, _ = s.forces()
+    ref = d["forces"]
+    assert np.array_equal(its, ref[:, 0].astype(int))
+    np.testing.assert_allclose(fd, ref[:, 1], rtol=1e-12, atol=ATOL_FORCE)
+    np.testing.assert_allclose(fl, ref[:, 2], rtol=1e-12, atol=ATOL_FORCE)
+    s.close()

@@ -96,9 +96,9 @@ def test_forces_per_step_ring_drains_in_order(mrlbm):
     s = mrlbm.Simulation(cfg)
     s.step(100)
     it, fd, fl, rin = s.forces()
-    assert np.array_equal(it, np.arange(1, 101))
+    assert np.array_equal(it, np.arange(2, 102))
     assert np.all(np.isfinite(fd)) and np.all(np.isfinite(fl))
     s.step(5)
     it2, *_ = s.forces()
-    assert np.array_equal(it2, np.arange(101, 106))
+    assert np.array_equal(it2, np.arange(102, 107))
     assert s.launch_count() == 105
