@@ -175,6 +175,24 @@ int mrlbm_get_macro(mrlbm_handle* h, double* rho, double* ux, double* uy,
 int mrlbm_get_forces(mrlbm_handle* h, int32_t* iter, double* f_drag, double* f_lift,
                      double* rho_inlet_sum, int32_t cap, int32_t* n);
 
+/* Strouhal number, mean drag coefficient and rms lift coefficient of a force history, as
+ * 2d_statistics.f90 computes them: period = distance of the first two strict local maxima of
+ * the lift (find_peaks, 2d_statistics.f90:183-214), averages over the n_cycle whole cycles
+ * after the first peak (2d_statistics.f90:90-131), forces normalised by
+ * 0.5 rho_infty uo^2 (2 r_cy) (2d_statistics.f90:28-32).  Host-only; returns MRLBM_ESTATE
+ * where the reference stops with "Could not detect two peaks". */
+int mrlbm_force_statistics(const double* f_drag, const double* f_lift, int32_t nstep,
+                           double r_cy, double uo, double rho_infty,
+                           double* St, double* Cd_mean, double* Cl_rms,
+                           int32_t* cycle_start, int32_t* period, int32_t* n_cycle);
+
+/* Cycle-averaged surface pressure coefficient Cp(k), k = 1..nbct (2d_statistics.f90:114-122);
+ * p_surface is the step-major history (nstep x nbct) of the surface pressure records
+ * (data_mean/p_surface_time.dat, 2d_mrlbm.f90:609-612). Host-only. */
+int mrlbm_cp_statistics(const double* p_surface, int32_t nstep, int32_t nbct,
+                        int32_t cycle_start, int32_t period, int32_t n_cycle,
+                        double rho_infty, double uo, double* cp);
+
 /* Number of kernel launches issued by this handle so far (all kinds). */
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n);
 

@@ -29,6 +29,7 @@ EXPORTED = [
     "mrlbm_get_geometry_info", "mrlbm_get_boundary_nodes", "mrlbm_get_node_classes",
     "mrlbm_load_state", "mrlbm_get_state", "mrlbm_set_inlet_profile", "mrlbm_step",
     "mrlbm_get_iter", "mrlbm_get_macro", "mrlbm_get_forces", "mrlbm_get_launch_count",
+    "mrlbm_force_statistics", "mrlbm_cp_statistics",
 ]
 
 
@@ -78,12 +79,13 @@ def load_library(path=None):
         "mrlbm_get_macro": [vp] * 7,
         "mrlbm_get_forces": [vp, vp, vp, vp, vp, i32, vp],
         "mrlbm_get_launch_count": [vp, vp],
+        "mrlbm_force_statistics": [vp, vp, i32, dbl, dbl, dbl, vp, vp, vp, vp, vp, vp],
+        "mrlbm_cp_statistics": [vp, i32, i32, i32, i32, i32, dbl, dbl, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = ctypes.c_int
-    del dbl
     if path is None:
         _lib = L
     return L
@@ -91,6 +93,47 @@ def load_library(path=None):
 
 def _ptr(a):
     return None if a is None else a.ctypes.data
+
+
+def force_statistics(f_drag, f_lift, r_cy, uo, rho_infty):
+    """St, Cd, Cl_rms and the cycle window of a force history (2d_statistics.f90:90-131)."""
+    L = load_library()
+    fd = np.ascontiguousarray(f_drag, dtype=np.float64)
+    fl = np.ascontiguousarray(f_lift, dtype=np.float64)
+    st, cd, cl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    cs, per, nc = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    rc = L.mrlbm_force_statistics(_ptr(fd), _ptr(fl), fd.size, float(r_cy), float(uo), float(rho_infty),
+                                  ctypes.byref(st), ctypes.byref(cd), ctypes.byref(cl), ctypes.byref(cs),
+                                  ctypes.byref(per), ctypes.byref(nc))
+    if rc != 0:
+        raise MrlbmError(rc, "could not detect two lift peaks" if rc == 5 else "bad arguments")
+    return {"St": st.value, "Cd": cd.value, "Cl_rms": cl.value, "cycle_start": cs.value, "period": per.value,
+            "n_cycle": nc.value}
+
+
+def cp_statistics(p_surface, cycle_start, period, n_cycle, rho_infty, uo):
+    """Cycle-averaged Cp per wall node (2d_statistics.f90:114-122)."""
+    L = load_library()
+    ps = np.ascontiguousarray(p_surface, dtype=np.float64)
+    nstep, nbct = ps.shape
+    cp = np.empty(nbct)
+    rc = L.mrlbm_cp_statistics(_ptr(ps), nstep, nbct, int(cycle_start), int(period), int(n_cycle),
+                               float(rho_infty), float(uo), _ptr(cp))
+    if rc != 0:
+        raise MrlbmError(rc, "bad arguments")
+    return cp
+
+
+def rho_inlet_running_mean(iters, rho_inlet_sum, ny, statsbegin):
+    """rho_inf_mean as the reference updates it each stats step (2d_mrlbm.f90:357-360)."""
+    m = 0.0
+    out = np.empty(len(iters))
+    for n, (it, s) in enumerate(zip(iters, rho_inlet_sum)):
+        c = float(np.float32(it - statsbegin))          # real(iter - statsbegin): default REAL
+        rho_infty = s / ny
+        m = ((c * m) + rho_infty) / (c + 1.0)
+        out[n] = m
+    return out
 
 
 def config_from_namelist(path):

@@ -25,7 +25,7 @@ CU_UNITS = {
     "step_f64.cu": ["-fmad=false"],
     "step_f32.cu": [],
 }
-CPP_UNITS = ["geometry.cpp", "capi.cpp"]
+CPP_UNITS = ["geometry.cpp", "capi.cpp", "statistics.cpp"]
 
 
 def _nvcc():

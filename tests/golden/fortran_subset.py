@@ -616,6 +616,7 @@ class Interpreter:
         self.compiled = {}
         self.stdout = []
         self.history = {}                                # name -> every record written
+        self.text_records = {}                           # name -> records of a formatted input file
 
     # -- declarations ------------------------------------------------------------------
     def _new_scalar(self, ftype):
@@ -1267,7 +1268,8 @@ class Interpreter:
             name = str(fexp(fr)).rstrip()
             self.units_open[uexp(fr)] = (name, form, [0])
             append = position == "append" or access == "append"
-            if name in self.text_inputs:
+            if name in self.text_inputs or name in self.text_records or name in self.unformatted_inputs and \
+                    status == "old":
                 return
             if not append or status == "replace":
                 self.files[name] = []
@@ -1289,8 +1291,12 @@ class Interpreter:
             if ustr.strip() == "*":
                 return lambda fr: None
             # internal write to a character variable with a numbered FORMAT
-            if fmt is not None and fmt.strip().isdigit() and self._scope(ustr.strip().lower(), unit):
-                fspec = (unit.formats.get(int(fmt)) or self.main.formats.get(int(fmt)))
+            if fmt is not None and self._scope(ustr.strip().lower(), unit) and (
+                    fmt.strip().isdigit() or fmt.strip()[:1] in "'\""):
+                if fmt.strip().isdigit():
+                    fspec = (unit.formats.get(int(fmt)) or self.main.formats.get(int(fmt)))
+                else:
+                    fspec = fmt.strip()[1:-1].strip()[1:-1]
                 setv = self._setter(ustr.strip().lower(), unit)
 
                 def f(fr):
@@ -1323,17 +1329,46 @@ class Interpreter:
                     setters[k](fr, v)
             return f
         targets = [self._compile_read_target(x, unit) for x in items]
+        kw = dict(self._kw(spec)[1])
+        iostat = self._setter(kw["iostat"].strip().lower(), unit) if "iostat" in kw else None
+        as_line = fmt is not None and fmt.strip().replace(" ", "").lower() in ("'(a)'", '"(a)"')
 
         def f(fr):
             name, form, cursor = self.units_open[uexp(fr)]
-            recs = self.unformatted_inputs[name]
+            recs = self.unformatted_inputs.get(name)
+            if recs is None:
+                recs = self.text_records.get(name, [])
+            if cursor[0] >= len(recs):                 # end of file
+                if iostat is None:
+                    raise FortranStop(f"end of file on {name}")
+                iostat(fr, -1)
+                return
             rec = list(recs[cursor[0]])
             cursor[0] += 1
+            if as_line:
+                rec = [" ".join(str(x) for x in rec)]
             for t in targets:
                 t(fr, rec)
+            if iostat is not None:
+                iostat(fr, 0)
         return f
 
     def _compile_read_target(self, x, unit):
+        x = x.strip()
+        if x.startswith("(") and match_paren(x, 0) == len(x) - 1:      # implied-do target list
+            parts = split_top(x[1:-1])
+            var, lo = parts[-2].split("=", 1)
+            lo_e = self.compile_expr(parse_expr(lo), unit)
+            hi_e = self.compile_expr(parse_expr(parts[-1]), unit)
+            subs = [self._compile_read_target(q, unit) for q in parts[:-2]]
+            setv = self._setter(var.strip().lower(), unit)
+
+            def t_do(fr, rec):
+                for v in range(int(lo_e(fr)), int(hi_e(fr)) + 1):
+                    setv(fr, v)
+                    for sb in subs:
+                        sb(fr, rec)
+            return t_do
         e = parse_expr(x)
         if e[0] == "name":
             get = self._getter(e[1], unit)
@@ -1346,6 +1381,12 @@ class Interpreter:
                 else:
                     setv(fr, rec.pop(0))
             return t
+        if e[0] == "call":
+            setter = self._actual_setter(e, unit)
+
+            def t2(fr, rec):
+                setter(fr, rec.pop(0))
+            return t2
         raise SyntaxError(x)
 
     def _compile_io_item(self, x, unit):
@@ -1416,6 +1457,8 @@ def _format(spec, values):
     for d in split_top(spec):
         d = d.strip()
         m = re.match(r"^([aAiI])(\d*)$", d)
+        if m and m.group(2) == "0":
+            m = re.match(r"^([aAiI])()$", d[0])
         if not m:
             continue
         v = values[vi]

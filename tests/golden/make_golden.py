@@ -169,6 +169,7 @@ def run_case(name, over):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default=None)
+    ap.add_argument("--stats", action="store_true")
     a = ap.parse_args()
     for name, over in CASES.items():
         if a.only and name != a.only:
@@ -179,5 +180,58 @@ def main():
         print(f"{name}: {out['elapsed_s']:.1f} s, {len(out['forces'])} force records -> {path}", flush=True)
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and "--stats" not in sys.argv:
     main()
+
+
+# ---------------------------------------------------------------------------------------
+# 2d_statistics.f90 on synthetic force / surface-pressure histories
+STAT_CASES = {
+    # name: (nstep, period, lift amplitude, mean drag, nbct, r_cy, uo, rho_infty)
+    "stats_sine": (400, 37.3, 0.02, 0.09, 24, 10.5, 0.05, 1.01),
+    "stats_short_cycles": (260, 61.7, 0.015, 0.07, 16, 5.3851648071345, 0.04, 0.998),
+}
+
+
+def run_stats_case(name, prm):
+    nstep, period, amp, fd0, nbct, r_cy, uo, rho_inf = prm
+    rng = np.random.default_rng(len(name) * 7919)
+    t = np.arange(1, nstep + 1)
+    phase = rng.uniform(0, 2 * np.pi)
+    fl = amp * np.sin(2 * np.pi * t / period + phase) + 1e-5 * rng.standard_normal(nstep)
+    fd = fd0 + 0.1 * amp * np.sin(4 * np.pi * t / period + 2 * phase) + 1e-5 * rng.standard_normal(nstep)
+    theta = np.sort(rng.uniform(0, 2 * np.pi, nbct))
+    ps = (1.0 / 3.0) * (1 + 1e-3 * rng.standard_normal((nstep, nbct)))
+    psf = ps + 1e-5 * rng.standard_normal((nstep, nbct))
+    src = open(os.path.join(REF, "2d_statistics.f90")).read()
+    text = (f"&parameters\n\tnbct = {nbct}\n\tr_cy = {r_cy!r}\n\tuo = {uo!r}\n\trho_infty = {rho_inf!r}\n/\n")
+    it = Interpreter(src, inputs={"input_stat.dat": text})
+    it.text_records["data_mean/forces_time.dat"] = [[int(a), float(b), float(c)] for a, b, c in zip(t, fd, fl)]
+    it.text_records["data_mean/theta.dat"] = [[float(x)] for x in theta]
+    it.unformatted_inputs["data_mean/p_surface_time.dat"] = [[int(a)] + [float(x) for x in row] for a, row in zip(t, ps)]
+    it.unformatted_inputs["data_mean/p_surface_smooth_time.dat"] = [[int(a)] + [float(x) for x in row]
+                                                                   for a, row in zip(t, psf)]
+    it.run()
+    f = it.files
+    dl = f["plots/drag_lift.dat"]
+    out = {"nstep": nstep, "nbct": nbct, "r_cy": r_cy, "uo": uo, "rho_infty": rho_inf, "iter": t, "f_drag": fd,
+           "f_lift": fl, "theta": theta, "p_surface": ps, "p_surface_smooth": psf,
+           "St": float(dl[0][-1]), "Cd": float(dl[1][-1]), "Cl_rms": float(dl[2][-1]),
+           "cp": np.array([[float(x) for x in r] for r in f["plots/cp.dat"]]),
+           "cp_fit": np.array([[float(x) for x in r] for r in f["plots/cp_fit.dat"]]),
+           "cd_time": np.array([[float(x) for x in r] for r in f["plots/cd_time.dat"]]),
+           "cl_time": np.array([[float(x) for x in r] for r in f["plots/cl_time.dat"]])}
+    return out
+
+
+def main_stats(only=None):
+    for name, prm in STAT_CASES.items():
+        if only and name != only:
+            continue
+        out = run_stats_case(name, prm)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(f"{name}: St={out['St']:.6f} Cd={out['Cd']:.6f} Cl_rms={out['Cl_rms']:.6f}", flush=True)
+
+
+if __name__ == "__main__" and "--stats" in sys.argv:
+    main_stats()
