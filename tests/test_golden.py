@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_*.npz")))
 NAMES = [os.path.basename(f)[:-4] for f in FIXTURES]
 ATOL_FORCE = 1e-13
 
