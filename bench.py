@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--case", choices=["mid", "large", "small"], default="mid")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only run warmup + steps of the case (for ncu); prints nothing else")
     return ap.parse_args()
 
 
@@ -183,10 +185,26 @@ def run_reference(args):
     return 0
 
 
+def run_profile(args):
+    """Minimal launch sequence for profilers: create the case, warmup + steps, nothing else."""
+    from mrlbm_2d_b200 import build
+    build.build()
+    import mrlbm_2d_b200 as m
+    cfg = make_case(args.case, 1234)
+    sim = m.Simulation(cfg, precision=args.precision or 32)
+    sim.step(args.warmup)
+    sim.step(args.steps)
+    st = sim.status()
+    sim.close()
+    return 0 if st == 0 else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
 
     import numpy as np
     import torch

@@ -1,0 +1,84 @@
+"""FP32 (deviation storage) against FP64 on the same case: force statistics and fields.
+
+    python -m mrlbm_2d_b200.precision_study --case small --steps 20000 [--stats-from 8000]
+
+Runs the case twice on one GPU (FP64 reference-order step, FP32 deviation step) from the
+same seeded initial state, records the per-step drag and lift, and reports
+  * St, Cd (mean), Cl_rms of each run over whole shedding cycles (2d_statistics.f90:90-131,
+    normalised by 0.5 rho_infty U^2 D with rho_infty = 1 and D = 2 r_c),
+  * |dCd|/Cd, |dSt|, |dCl_rms|/Cl_rms of FP32 against FP64,
+  * the relative L2 error of the final velocity field, max |du|/U,
+and the wall-clock MLUPS of each run.  One JSON line on stdout.
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import api
+from .config import case_adjoint, case_large, case_mid, case_small
+
+CASES = {"small": case_small, "mid": case_mid, "adjoint": case_adjoint, "large": case_large}
+
+
+def run(cfg, precision, steps, chunk=5000):
+    sim = api.Simulation(cfg, precision=precision)
+    fd, fl = [], []
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        n = min(chunk, steps - done)
+        sim.step(n, macro=(done + n == steps))
+        _, d, l, _ = sim.forces()
+        fd.append(d)
+        fl.append(l)
+        done += n
+    mac = sim.macro()
+    el = time.perf_counter() - t0
+    st = sim.status()
+    sim.close()
+    if st != 0:
+        raise RuntimeError(f"device error flag in fp{precision} run")
+    return np.concatenate(fd), np.concatenate(fl), mac, cfg.nx * cfg.ny * steps / el / 1e6
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="small", choices=sorted(CASES))
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--stats-from", type=int, default=None, help="first step of the statistics window")
+    a = ap.parse_args(argv)
+    cfg = CASES[a.case]()
+    start = a.stats_from if a.stats_from is not None else a.steps // 2
+    cfg = cfg.replace(statsbegin=start, statsend=a.steps + 10)
+    out = {"case": a.case, "nx": cfg.nx, "ny": cfg.ny, "steps": a.steps, "stats_from": start,
+           "D": 2 * cfg.r_c, "U": cfg.uo, "Re": cfg.Re}
+    res = {}
+    for prec in (64, 32):
+        fd, fl, mac, mlups = run(cfg, prec, a.steps)
+        r = {"mlups_wall": mlups}
+        try:
+            s = api.force_statistics(fd, fl, cfg.r_c, cfg.uo, 1.0)
+            r.update(s)
+        except api.MrlbmError as e:
+            r["error"] = str(e)
+        res[prec] = (r, fd, fl, mac)
+        out[f"fp{prec}"] = r
+    r64, fd64, fl64, m64 = res[64]
+    r32, fd32, fl32, m32 = res[32]
+    if "Cd" in r64 and "Cd" in r32:
+        out["rel_err_Cd"] = abs(r32["Cd"] - r64["Cd"]) / abs(r64["Cd"])
+        out["abs_err_St"] = abs(r32["St"] - r64["St"])
+        out["rel_err_Cl_rms"] = abs(r32["Cl_rms"] - r64["Cl_rms"]) / abs(r64["Cl_rms"])
+    du = np.sqrt((m32["ux"] - m64["ux"]) ** 2 + (m32["uy"] - m64["uy"]) ** 2)
+    u64 = np.sqrt(m64["ux"] ** 2 + m64["uy"] ** 2)
+    out["velocity_rel_l2"] = float(np.sqrt((du ** 2).sum() / (u64 ** 2).sum()))
+    out["velocity_max_abs_over_U"] = float(du.max() / cfg.uo)
+    out["drag_history_rel_l2"] = float(np.linalg.norm(fd32 - fd64) / np.linalg.norm(fd64))
+    print(json.dumps(out), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    main()
