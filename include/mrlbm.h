@@ -85,6 +85,11 @@ typedef struct mrlbm_geometry_info {
     int32_t n_label15;               /* boundary nodes whose quadrant label is 15 */
     double  x_c, y_c, r_c, r_cyl;    /* r_cyl = max boundary-node radius (2d_mrlbm.f90:1038-1050) */
     double  nu, omega;               /* 2d_mrlbm.f90:133-135 */
+    /* padded population layout of one time level: population k of node (i,j), with i in
+     * 0..nx+1 and j in 0..ny+1 (ghost ring included), is element k*plane + j*pitch + i + off */
+    int32_t pitch, off;
+    int64_t plane;
+    int64_t state_bytes;             /* bytes of the two time levels mrlbm_step_noalloc needs */
 } mrlbm_geometry_info;
 
 typedef struct mrlbm_handle mrlbm_handle;
@@ -143,7 +148,7 @@ int mrlbm_get_node_classes(const mrlbm_handle* h, int32_t* isfluid, int32_t* iss
 int mrlbm_load_state(mrlbm_handle* h, const double* f, int32_t iter);
 
 /* Post-streaming populations after the last step (the f of write_restart_file,
- * 2d_mrlbm.f90:2186-2202). */
+ * 2d_mrlbm.f90:2186-2202).  On a host-only handle: the configured initial populations. */
 int mrlbm_get_state(mrlbm_handle* h, double* f);
 
 /* Per-row inlet velocity u_in(1..ny) replacing the uniform uinlet of 2d_mrlbm.f90:258
@@ -192,6 +197,33 @@ int mrlbm_force_statistics(const double* f_drag, const double* f_lift, int32_t n
 int mrlbm_cp_statistics(const double* p_surface, int32_t nstep, int32_t nbct,
                         int32_t cycle_start, int32_t period, int32_t n_cycle,
                         double rho_infty, double uo, double* cp);
+
+/* Step without any device allocation by this library (no counterpart in the reference).
+ *
+ * For hosts that own all device memory themselves and cannot let a library call cudaMalloc:
+ * a Fortran host whose device arrays come from its CUDA Fortran or OpenACC runtime, a
+ * framework whose caching allocator or arena holds the GPU, a service that freezes
+ * allocation after start-up.  `h` is a host-only handle (mrlbm_create with device -1, which
+ * allocates no device memory); the caller passes
+ *   d_state  device buffer of info.state_bytes bytes (both time levels, the padded layout of
+ *            mrlbm_geometry_info; FP64 values, or FP32 deviations f_k - w_k),
+ *   d_f0     device array f(nx,ny,0:8) (Fortran order, FP64) to start from, or NULL to
+ *            continue from the state left in d_state by the previous call,
+ *   records  host array of nsteps * 4 doubles receiving (iter, F_drag_net, F_lift_net,
+ *            sum(rho(1,:))) for each stats step; *n_records receives the count.
+ * The handle's mrlbm_get_state returns the configured initial populations to seed d_f0.
+ * Everything else the step kernel uses (its force-reduction partials and arrival counter,
+ * the per-step records, the curved-wall tables) lives in fixed-size file-scope device arrays
+ * of about 2 MB that every GPU loading this library holds until the process exits.  Limits:
+ * at most 1024 curved-wall nodes and a cylinder bounding box of at most 512 x 512 cells;
+ * larger cases are rejected with MRLBM_EINVAL.  The first call on a device looks up the
+ * arrays' device addresses (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls share the arrays and re-upload the case tables
+ * and clear the counters each time, so calls that overlap on the GPU (other streams or
+ * devices' threads using the same device) race; serialise them.  Allocates nothing: no
+ * cudaMalloc, cudaFree or allocating library routine on any path. */
+int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32_t nsteps,
+                       double* records, int32_t* n_records, void* cuda_stream);
 
 /* Number of kernel launches issued by this handle so far (all kinds). */
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n);

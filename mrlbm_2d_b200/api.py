@@ -29,7 +29,7 @@ EXPORTED = [
     "mrlbm_get_geometry_info", "mrlbm_get_boundary_nodes", "mrlbm_get_node_classes",
     "mrlbm_load_state", "mrlbm_get_state", "mrlbm_set_inlet_profile", "mrlbm_step",
     "mrlbm_get_iter", "mrlbm_get_macro", "mrlbm_get_forces", "mrlbm_get_launch_count",
-    "mrlbm_force_statistics", "mrlbm_cp_statistics",
+    "mrlbm_force_statistics", "mrlbm_cp_statistics", "mrlbm_step_noalloc",
 ]
 
 
@@ -43,7 +43,8 @@ class GeometryInfo(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nbct", ctypes.c_int32),
                 ("n_label15", ctypes.c_int32), ("x_c", ctypes.c_double), ("y_c", ctypes.c_double),
                 ("r_c", ctypes.c_double), ("r_cyl", ctypes.c_double), ("nu", ctypes.c_double),
-                ("omega", ctypes.c_double)]
+                ("omega", ctypes.c_double), ("pitch", ctypes.c_int32), ("off", ctypes.c_int32),
+                ("plane", ctypes.c_int64), ("state_bytes", ctypes.c_int64)]
 
 
 _lib = None
@@ -81,6 +82,7 @@ def load_library(path=None):
         "mrlbm_get_launch_count": [vp, vp],
         "mrlbm_force_statistics": [vp, vp, i32, dbl, dbl, dbl, vp, vp, vp, vp, vp, vp],
         "mrlbm_cp_statistics": [vp, i32, i32, i32, i32, i32, dbl, dbl, vp],
+        "mrlbm_step_noalloc": [vp, vp, vp, i32, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -214,6 +216,17 @@ class Simulation:
         n = ctypes.c_int64()
         self._check(self._L.mrlbm_get_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+    def step_noalloc(self, d_state_ptr, nsteps, d_f0_ptr=None, stream_ptr=None):
+        """Step a host-only handle in caller-owned device memory (see mrlbm_step_noalloc).
+        Returns the (n, 4) records (iter, F_drag_net, F_lift_net, sum(rho(1,:)))."""
+        rec = np.empty((max(int(nsteps), 1), 4))
+        n = ctypes.c_int32()
+        self._check(self._L.mrlbm_step_noalloc(self._h, ctypes.c_void_p(d_state_ptr),
+                                               ctypes.c_void_p(d_f0_ptr) if d_f0_ptr else None, int(nsteps),
+                                               _ptr(rec), ctypes.byref(n),
+                                               ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+        return rec[:n.value].copy()
 
     # -- state and outputs -----------------------------------------------------------
     def get_state(self):

@@ -12,6 +12,7 @@
 
 #include "../../include/mrlbm.h"
 #include "geometry.h"
+#include "noalloc.h"
 #include "step_params.h"
 
 using namespace mrlbm;
@@ -54,6 +55,7 @@ struct mrlbm_handle {
     std::string err;
     DevConsts dc{};
     bool host_only = false;
+    std::vector<float> geo32;                 // FP32 tables of a host-only FP32 handle
     std::vector<OvrEntry> ovr;                // loaded-state overrides (see OvrEntry)
     bool ovr_live = false;                    // true until the first step after a load
     OvrEntry* d_ovr = nullptr;
@@ -376,13 +378,15 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
         return bail(MRLBM_EUNSUPPORTED, "FP32 closure needs equal Is/Os weight sums for every label");
     if (precision == MRLBM_FP32 && c.channel_with_cylinder && h->closure != CLOSURE_STRONG && h->closure != CLOSURE_NONE)
         return bail(MRLBM_EUNSUPPORTED, "the FP32 step implements only the default rotated strong-mass closure");
+
     h->L = make_layout(nx, ny, precision == MRLBM_FP64 ? 16 : 32);
     if (h->L.total() >= (int64_t)1 << 31) return bail(MRLBM_EINVAL, "grid too large for one handle (2^31 populations)");
     const char* tc = std::getenv("MRLBM_TILE_CFG");
     if (tc) h->tile_cfg = std::max(0, std::min(N_TILE_CFGS - 1, std::atoi(tc)));
-
     if (device == -1) {            // host-only handle: configuration and geometry, no device state
         h->host_only = true;
+        h->iter = 1;
+        if (precision == MRLBM_FP32) h->geo32.assign(h->geo.tgeo.begin(), h->geo.tgeo.end());
         *out = h;
         return MRLBM_OK;
     }
@@ -475,6 +479,8 @@ int mrlbm_get_geometry_info(const mrlbm_handle* h, mrlbm_geometry_info* info) {
     info->nx = h->L.nx; info->ny = h->L.ny; info->nbct = h->geo.nb; info->n_label15 = h->geo.n_label15;
     info->x_c = h->geo.x_c; info->y_c = h->geo.y_c; info->r_c = h->geo.r_c; info->r_cyl = h->geo.r_cyl;
     info->nu = h->nu; info->omega = h->omega;
+    info->pitch = h->L.pitch; info->off = h->L.off; info->plane = h->L.plane;
+    info->state_bytes = 2 * h->L.total() * (int64_t)h->elem;
     return MRLBM_OK;
 }
 
@@ -517,7 +523,12 @@ int mrlbm_load_state(mrlbm_handle* h, const double* f, int32_t iter) {
 
 int mrlbm_get_state(mrlbm_handle* h, double* f) {
     if (!h || !f) return MRLBM_EINVAL;
-    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    if (h->host_only) {                 // the configured initial populations
+        std::vector<double> f0;
+        initial_state(h->cfg, h->lat, h->L.nx, h->L.ny, f0);
+        std::copy(f0.begin(), f0.end(), f);
+        return MRLBM_OK;
+    }
     CK(cudaSetDevice(h->device));
     const int nx = h->L.nx, ny = h->L.ny;
     const size_t N = (size_t)nx * ny;
@@ -619,6 +630,56 @@ int mrlbm_get_forces(mrlbm_handle* h, int32_t* iter, double* fd, double* fl, dou
     h->hist.erase(h->hist.begin(), h->hist.begin() + (size_t)m * REC_WORDS);
     *n = m;
     return MRLBM_OK;
+}
+
+int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32_t nsteps, double* records,
+                       int32_t* n_records, void* stream) {
+    if (!h || nsteps < 0) return MRLBM_EINVAL;
+    if (!h->host_only) return fail(h, MRLBM_EINVAL, "mrlbm_step_noalloc takes a host-only handle (device -1)");
+    const mrlbm_config& c = h->cfg;
+    NaCase nc;
+    nc.geo = &h->geo;
+    nc.geo32 = &h->geo32;
+    nc.precision = h->precision;
+    nc.L = h->L;
+    for (int k = 0; k < Q; ++k) nc.w[k] = h->lat.w[k];
+    nc.xper = c.x_periodic != 0;
+    nc.yper = c.y_periodic != 0;
+    nc.freeslip = c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic;
+    nc.post_process = c.post_process;
+    nc.statsbegin = c.statsbegin;
+    nc.statsend = c.statsend;
+    nc.iplot = c.iplot;
+    nc.plot_enabled = c.post_process && (c.channel_with_cylinder || c.channel_with_square);
+    StepParams<double> p64{};
+    StepParams<float> p32{};
+    if (h->precision == MRLBM_FP64) { fill_common(h, p64); nc.p64 = &p64; }
+    else { fill_common(h, p32); nc.p32 = &p32; }
+    if (d_f0) {
+        // destinations whose streaming slot another destination also uses (corner wraps)
+        std::vector<std::pair<int64_t, OvrEntry>> cand;
+        const int ci[2] = {1, h->L.nx}, cj[2] = {1, h->L.ny};
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int k = 0; k < Q; ++k) cand.push_back({slot_of(h, ci[a], cj[b], k), OvrEntry{ci[a], cj[b], k, 0, 0.0}});
+        for (size_t x = 0; x < cand.size(); ++x) {
+            bool shared = false;
+            for (size_t y = 0; y < cand.size(); ++y)
+                if (x != y && cand[x].first == cand[y].first) shared = true;
+            if (shared) nc.conflicts.push_back(cand[x].second);
+        }
+    }
+    nc.tile_cfg = h->tile_cfg;
+    nc.iter = h->iter;
+    nc.cur = h->cur;
+    nc.launches = h->launches;
+    std::string err;
+    const int rc = noalloc_step(nc, d_state, d_f0, nsteps, records, n_records, stream, err);
+    h->iter = nc.iter;
+    h->cur = nc.cur;
+    h->launches = nc.launches;
+    if (rc != MRLBM_OK) h->err = err;
+    return rc;
 }
 
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n) {
