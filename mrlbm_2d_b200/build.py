@@ -15,6 +15,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libmrlbm.so")
+DRIVER = os.path.join(PKG, "mrlbm_run")
 BUILD = os.path.join(PKG, "_build")
 ROOT = os.path.dirname(PKG)
 
@@ -46,7 +47,7 @@ def _sources():
 
 
 def up_to_date():
-    if not os.path.exists(OUT):
+    if not os.path.exists(OUT) or not os.path.exists(DRIVER):
         return False
     t = os.path.getmtime(OUT)
     return all(os.path.getmtime(s) <= t for s in _sources())
@@ -75,6 +76,11 @@ def build(force=False, verbose=False):
     tmp = OUT + ".tmp"
     subprocess.run([nvcc] + ARCH + ["-shared", "-o", tmp] + objs, check=True)
     os.replace(tmp, OUT)
+    # the input.dat-driven host driver (mrlbm_run) over the public C ABI
+    drv_obj = os.path.join(BUILD, "driver_main.cpp.o")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-c", os.path.join(CSRC, "driver_main.cpp"), "-o", drv_obj],
+                   check=True)
+    subprocess.run(["g++", "-o", DRIVER, drv_obj, "-L" + PKG, "-lmrlbm", "-Wl,-rpath,$ORIGIN"], check=True)
     return OUT
 
 
