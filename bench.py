@@ -41,6 +41,10 @@ def parse():
     ap.add_argument("--case", choices=["mid", "large", "small"], default="mid")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile", type=int, default=None,
+                    help="bulk tile shape (default: chosen by the autotuner before timing)")
+    ap.add_argument("--large-steps", type=int, default=30,
+                    help="timed steps of the 16384 x 4096 roofline case at N=1 (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps of the case (for ncu); prints nothing else")
     return ap.parse_args()
@@ -168,18 +172,26 @@ def run_reference(args):
     n = os.cpu_count() or 1
     oracle.set_threads(n)
     o = oracle.Oracle(cfg.replace(num_threads=n), threads=n)
-    o.step(args.warmup)
+    o.step(min(args.warmup, 3))
+    # bounded sample: the timed steps stop after ~90 s of host work whatever --steps asks
     t0 = time.perf_counter()
-    o.step(args.steps)
+    done = 0
+    while done < args.steps:
+        o.step(1)
+        done += 1
+        if time.perf_counter() - t0 > 90.0:
+            break
     el = time.perf_counter() - t0
     nodes = cfg.nx * cfg.ny
-    v = nodes * args.steps / el / 1e6
+    v = nodes * done / el / 1e6
     line = {"metric": "D2Q9 MLUPS", "value": v, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": el / done * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": case_desc(args.case, cfg), "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": n, "kind": "port",
-                             "sample": f"{args.steps} timed steps after {args.warmup} warm-up, full grid"},
+                             "sample": f"{done} timed steps of the full grid after {min(args.warmup, 3)} "
+                                       f"warm-up (FP64 C++ restatement of 2d_mrlbm.f90, OpenMP loops, "
+                                       f"serial streaming)"},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -192,6 +204,8 @@ def run_profile(args):
     import mrlbm_2d_b200 as m
     cfg = make_case(args.case, 1234)
     sim = m.Simulation(cfg, precision=args.precision or 32)
+    if args.tile is not None:
+        sim.tile_config = args.tile
     sim.step(args.warmup)
     sim.step(args.steps)
     st = sim.status()
@@ -246,14 +260,24 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def time_device(precision, K, W, sampler=None):
-        sim = m.Simulation(cfg, precision=precision, device=dev)
+    def pick_tile(sim):
+        if args.tile is not None:
+            sim.tile_config = args.tile
+            return args.tile
+        best, _ = sim.autotune(trial_steps=10)
+        return best
+
+    def time_device(precision, K, W, case_cfg=None, soak_s=1.0):
+        c = case_cfg or cfg
+        sim = m.Simulation(c, precision=precision, device=dev)
         sim.set_stream(stream.cuda_stream)
         sim.step(W)
+        tile = pick_tile(sim)
         # untimed soak so clock samples see the steady state
-        t_soak = time.time()
-        while time.time() - t_soak < 1.0:
+        t_soak, n_soak = time.time(), 0
+        while time.time() - t_soak < soak_s and n_soak < 20000:
             sim.step(50)
+            n_soak += 50
             torch.cuda.synchronize()
         sim.forces()
         launches0 = sim.launch_count()
@@ -283,12 +307,13 @@ def main():
         sim.close()
         assert st == 0, "device error flag set"
         assert np.all(np.isfinite(fd)), "non-finite forces"
-        return total_ms, launches, per, noflush_ms, (t_wall0, t_wall1)
+        return total_ms, launches, per, noflush_ms, (t_wall0, t_wall1), tile
 
-    def time_e2e(precision, K):
+    def time_e2e(precision, K, tile):
         """Public-API run with host buffers: load state, K steps, force drains, fields back."""
         sim = m.Simulation(cfg, precision=precision, device=dev)
         sim.set_stream(stream.cuda_stream)
+        sim.tile_config = tile               # the autotuner's choice for this case (untimed setup)
         f0 = sim.get_state()                 # host copy of the seeded initial populations
         sim.step(3)
         sim.forces()
@@ -322,15 +347,25 @@ def main():
         time.sleep(0.3)
     results = {}
     for prec in precisions:
-        total_ms, launches, per, noflush_ms, win = time_device(prec, args.steps, args.warmup)
+        total_ms, launches, per, noflush_ms, win, tile = time_device(prec, args.steps, args.warmup)
         total_ms = max_over_ranks(total_ms)
-        results[prec] = (total_ms, launches, per, noflush_ms, win)
+        results[prec] = (total_ms, launches, per, noflush_ms, win, tile)
+    large = {}
+    if world == 1 and args.large_steps > 0 and args.case != "large":
+        lcfg = make_case("large", 1234)
+        lnodes = lcfg.nx * lcfg.ny
+        for prec in precisions:
+            t, _, _, nf, lwin, ltile = time_device(prec, args.large_steps, 3, case_cfg=lcfg, soak_s=0.5)
+            ms = t / args.large_steps
+            large[prec] = {"ms_per_step": ms, "mlups": lnodes / (ms * 1e-3) / 1e6, "tile_shape": ltile,
+                           "hbm_gbs_alg": BYTES_PER_LU[prec] * lnodes / (ms * 1e-3) / 1e9,
+                           "ms_per_step_unflushed": nf, "window": lwin}
     if sampler:
         time.sleep(0.3)
         sampler.stop()
-    e2e = time_e2e(head, args.steps)
+    e2e = time_e2e(head, args.steps, results[head][5])
 
-    total_ms, launches, per, noflush_ms, win = results[head]
+    total_ms, launches, per, noflush_ms, win, tile = results[head]
     ms_step = total_ms / args.steps
     value = world * nodes * args.steps / (total_ms * 1e-3) / 1e6
     peak, peak_kind = hbm_peak()
@@ -342,7 +377,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if head == 32 else "f64", "data": "synthetic (seeded noise init)",
         "config": dict(case_desc(args.case, cfg), precision=f"fp{head}", l2="flushed before every timed step",
-                       parallelism=f"replicas{world}"),
+                       parallelism=f"replicas{world}", tile_shape=tile),
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
@@ -352,15 +387,30 @@ def main():
         "e2e": e2e,
     }
     for prec in precisions:
-        t, _, _, nf, _ = results[prec]
+        t, _, _, nf, _, tl = results[prec]
         line[f"fp{prec}"] = {"mlups": world * nodes * args.steps / (t * 1e-3) / 1e6, "ms_per_step": t / args.steps,
+                             "tile_shape": tl,
                              "ms_per_step_unflushed": nf,
                              "hbm_gbs_alg": BYTES_PER_LU[prec] * nodes / (t / args.steps * 1e-3) / 1e9}
     if 32 in results and 64 in results:
         line["fp32_over_fp64"] = results[64][0] / results[32][0]
+    if large:
+        lcfg = make_case("large", 1234)
+        rl = {"workload": case_desc("large", lcfg)["workload"], "steps": args.large_steps,
+              "l2": "flushed before every timed step (working set 4.8 GB FP32 / 9.7 GB FP64)", "peak": peak,
+              "peak_kind": peak_kind, "unit": "GB/s", "bound": "hbm"}
+        for prec, v in large.items():
+            v = dict(v)
+            v.pop("window")
+            v["frac"] = v["hbm_gbs_alg"] / peak
+            rl[f"fp{prec}"] = v
+        if 32 in large and 64 in large:
+            rl["fp32_over_fp64"] = large[64]["ms_per_step"] / large[32]["ms_per_step"]
+        line["roofline_large"] = rl
     if sampler:
-        t0 = min(r[4][0] for r in results.values()) - 1.2
-        t1 = max(r[4][1] for r in results.values())
+        wins = [r[4] for r in results.values()] + [v["window"] for v in large.values()]
+        t0 = min(w[0] for w in wins) - 1.2
+        t1 = max(w[1] for w in wins)
         line["clocks"] = sampler.summary(t0, t1)
     if world > 1:
         dist.barrier()

@@ -39,6 +39,7 @@ extern "C" {
 #define MRLBM_ECUDA          -1   /* CUDA runtime error                                  */
 #define MRLBM_EDEVICE_NAN    -2   /* device flag: NaN or non-positive density           */
 #define MRLBM_ENODEVICE      -3   /* no CUDA device / kernels not loadable              */
+#define MRLBM_EDEVICE_TIMEOUT -4  /* device flag: a bounded wait in a kernel gave up      */
 
 /* ---- precision of a handle ----------------------------------------------------- */
 #define MRLBM_FP64  64            /* populations and arithmetic in FP64 (reference form) */
@@ -121,7 +122,7 @@ int mrlbm_destroy(mrlbm_handle* h);
 /* Last error text of a handle (or of the last failed mrlbm_create when h == NULL). */
 int mrlbm_last_error(const mrlbm_handle* h, char* buf, size_t len);
 
-/* Sticky device status: MRLBM_OK or MRLBM_EDEVICE_NAN.  Synchronises. */
+/* Sticky device status: MRLBM_OK, MRLBM_EDEVICE_NAN or MRLBM_EDEVICE_TIMEOUT.  Synchronises. */
 int mrlbm_status(mrlbm_handle* h);
 
 /* Run subsequent work on a caller-owned cudaStream_t (NULL = the legacy default stream).
@@ -215,8 +216,8 @@ int mrlbm_cp_statistics(const double* p_surface, int32_t nstep, int32_t nbct,
  * Everything else the step kernel uses (its force-reduction partials and arrival counter,
  * the per-step records, the curved-wall tables) lives in fixed-size file-scope device arrays
  * of about 2 MB that every GPU loading this library holds until the process exits.  Limits:
- * at most 1024 curved-wall nodes and a cylinder bounding box of at most 512 x 512 cells;
- * larger cases are rejected with MRLBM_EINVAL.  The first call on a device looks up the
+ * at most 1024 curved-wall nodes, 8192 rows and a cylinder bounding box of at most 512 x 512
+ * cells; larger cases are rejected with MRLBM_EINVAL.  The first call on a device looks up the
  * arrays' device addresses (cudaGetSymbolAddress) with that device current; make that first
  * call before any stream capture.  All calls share the arrays and re-upload the case tables
  * and clear the counters each time, so calls that overlap on the GPU (other streams or
@@ -224,6 +225,23 @@ int mrlbm_cp_statistics(const double* p_surface, int32_t nstep, int32_t nbct,
  * cudaMalloc, cudaFree or allocating library routine on any path. */
 int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32_t nsteps,
                        double* records, int32_t* n_records, void* cuda_stream);
+
+/* Bulk tile shape of the step kernel.  Shapes 0..9 are one-tile-per-block grids (threads per
+ * block, rows per thread, register budget; TILE_CFGS in mrlbm_2d_b200/csrc/step_params.h);
+ * shapes 10..15 are persistent blocks fed by tensor copies (TMA) with several tiles in flight
+ * (TMA_CFGS there).  Every shape computes the same bits.  The default is 1; MRLBM_TILE_CFG in
+ * the environment overrides it at creation.  A shape that does not fit the handle's precision
+ * makes the next mrlbm_step return MRLBM_EUNSUPPORTED.  mrlbm_step_noalloc runs shape 1 when a
+ * TMA shape is selected (its counters live in the handle). */
+#define MRLBM_N_TILE_CONFIGS 16
+int mrlbm_set_tile_config(mrlbm_handle* h, int32_t cfg);
+int mrlbm_get_tile_config(const mrlbm_handle* h, int32_t* cfg);
+
+/* Autotuner: time every tile shape for trial_steps steps on this handle's own case (after one
+ * warm-up step each), keep the fastest, and restore the populations, the iteration counter
+ * and the force history, so a simulation is unaffected.  Returns the chosen shape and its
+ * time per step in milliseconds. */
+int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, double* best_ms);
 
 /* Number of kernel launches issued by this handle so far (all kinds). */
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n);

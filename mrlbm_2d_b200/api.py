@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmrlbm.so")
 
 FP64, FP32 = 64, 32
+N_TILE_CONFIGS = 16   # MRLBM_N_TILE_CONFIGS: shapes 0..9 one tile per block, 10..15 TMA-fed persistent
 STEP_MACRO = 1
 
 EXPORTED = [
@@ -30,6 +31,7 @@ EXPORTED = [
     "mrlbm_load_state", "mrlbm_get_state", "mrlbm_set_inlet_profile", "mrlbm_step",
     "mrlbm_get_iter", "mrlbm_get_macro", "mrlbm_get_forces", "mrlbm_get_launch_count",
     "mrlbm_force_statistics", "mrlbm_cp_statistics", "mrlbm_step_noalloc",
+    "mrlbm_set_tile_config", "mrlbm_get_tile_config", "mrlbm_autotune",
 ]
 
 
@@ -83,6 +85,9 @@ def load_library(path=None):
         "mrlbm_force_statistics": [vp, vp, i32, dbl, dbl, dbl, vp, vp, vp, vp, vp, vp],
         "mrlbm_cp_statistics": [vp, i32, i32, i32, i32, i32, dbl, dbl, vp],
         "mrlbm_step_noalloc": [vp, vp, vp, i32, vp, vp, vp],
+        "mrlbm_set_tile_config": [vp, i32],
+        "mrlbm_get_tile_config": [vp, vp],
+        "mrlbm_autotune": [vp, i32, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -199,6 +204,22 @@ class Simulation:
     # -- stepping --------------------------------------------------------------------
     def step(self, n=1, macro=False):
         self._check(self._L.mrlbm_step(self._h, int(n), STEP_MACRO if macro else 0))
+
+    def autotune(self, trial_steps=20):
+        """Pick the fastest bulk tile shape for this case (state and history are restored)."""
+        best, ms = ctypes.c_int32(), ctypes.c_double()
+        self._check(self._L.mrlbm_autotune(self._h, int(trial_steps), ctypes.byref(best), ctypes.byref(ms)))
+        return best.value, ms.value
+
+    @property
+    def tile_config(self):
+        c = ctypes.c_int32()
+        self._check(self._L.mrlbm_get_tile_config(self._h, ctypes.byref(c)))
+        return c.value
+
+    @tile_config.setter
+    def tile_config(self, cfg):
+        self._check(self._L.mrlbm_set_tile_config(self._h, int(cfg)))
 
     def set_stream(self, stream_ptr):
         self._check(self._L.mrlbm_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))

@@ -26,6 +26,7 @@ CU_UNITS = {
     "step_f64.cu": ["-fmad=false"],
     "step_f32.cu": [],
     "noalloc.cu": [],
+    "state_io.cu": [],
 }
 CPP_UNITS = ["geometry.cpp", "capi.cpp", "statistics.cpp"]
 

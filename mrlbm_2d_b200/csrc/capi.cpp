@@ -1,5 +1,7 @@
 // capi.cpp -- the extern "C" surface of include/mrlbm.h: handle lifetime, device memory,
 // state transfer, the time-step loop and the force history ring.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,6 +15,7 @@
 #include "../../include/mrlbm.h"
 #include "geometry.h"
 #include "noalloc.h"
+#include "state_io.h"
 #include "step_params.h"
 
 using namespace mrlbm;
@@ -59,6 +62,14 @@ struct mrlbm_handle {
     std::vector<OvrEntry> ovr;                // loaded-state overrides (see OvrEntry)
     bool ovr_live = false;                    // true until the first step after a load
     OvrEntry* d_ovr = nullptr;
+    double* d_fstage = nullptr;               // f(nx,ny,0:8) staging for state transfers
+    // TMA shapes: tensor maps of both time levels, tile-claim counter, persistent CTAs
+    unsigned long long* d_tile_ctr = nullptr;
+    unsigned long long tile_base = 0;
+    int tmap_cfg = -1;
+    CUtensorMap tmap[2];
+    int workers = 0;
+    int num_sms = 0;
 };
 
 #define CK(call)                                                                           \
@@ -135,65 +146,46 @@ bool make_dev_consts(mrlbm_handle* h) {
     return ok;
 }
 
-int upload_state(mrlbm_handle* h, const double* f) {
-    const int nx = h->L.nx, ny = h->L.ny;
-    const size_t N = (size_t)nx * ny;
-    const int64_t total = h->L.total();
-    if (h->precision == MRLBM_FP64) {
-        std::vector<double> b((size_t)total, 0.0);
-        for (int k = 0; k < Q; ++k)
-            for (int j = 1; j <= ny; ++j)
-                for (int i = 1; i <= nx; ++i)
-                    b[(size_t)slot_of(h, i, j, k)] = f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k];
-        CK(cudaMemcpyAsync(h->buf[0], b.data(), (size_t)total * 8, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(h->buf[1], b.data(), (size_t)total * 8, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-    } else {
-        std::vector<float> b((size_t)total, 0.0f);
-        for (int k = 0; k < Q; ++k)
-            for (int j = 1; j <= ny; ++j)
-                for (int i = 1; i <= nx; ++i)
-                    b[(size_t)slot_of(h, i, j, k)] =
-                        (float)(f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k] - h->lat.w[k]);
-        CK(cudaMemcpyAsync(h->buf[0], b.data(), (size_t)total * 4, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(h->buf[1], b.data(), (size_t)total * 4, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-    }
-    h->cur = 0;
-    // destinations whose streaming source slot another destination also uses keep their
-    // own value for the first step (and for get_state until then)
-    h->ovr.clear();
-    auto check = [&](int i, int j) {
-        for (int k = 0; k < Q; ++k) {
-            const size_t src = (size_t)(i - 1) + (size_t)nx * (j - 1) + N * k;
-            const int64_t sl = slot_of(h, i, j, k);
-            double stored;
-            if (h->precision == MRLBM_FP64) {
-                CK(cudaMemcpy(&stored, (const double*)h->buf[0] + sl, 8, cudaMemcpyDeviceToHost));
-            } else {
-                float g;
-                CK(cudaMemcpy(&g, (const float*)h->buf[0] + sl, 4, cudaMemcpyDeviceToHost));
-                stored = h->lat.w[k] + (double)g;
-            }
-            const double want = h->precision == MRLBM_FP64 ? f[src] : h->lat.w[k] + (double)(float)(f[src] - h->lat.w[k]);
-            if (!(stored == want)) {
-                OvrEntry e{i, j, k, 0, h->precision == MRLBM_FP64 ? f[src] : (double)(float)(f[src] - h->lat.w[k])};
-                h->ovr.push_back(e);
-            }
-        }
-        return MRLBM_OK;
-    };
-    const int ci[2] = {1, nx}, cj[2] = {1, ny};
+// Destinations whose streaming slot another destination also uses (the corner populations
+// both periodic wraps touch): they keep their own loaded value for the first step.
+std::vector<OvrEntry> slot_conflicts(const mrlbm_handle* h) {
+    std::vector<std::pair<int64_t, OvrEntry>> cand;
+    const int ci[2] = {1, h->L.nx}, cj[2] = {1, h->L.ny};
     for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b) {
-            int rc = check(ci[a], cj[b]);
-            if (rc != MRLBM_OK) return rc;
-        }
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < Q; ++k) cand.push_back({slot_of(h, ci[a], cj[b], k), OvrEntry{ci[a], cj[b], k, 0, 0.0}});
+    std::vector<OvrEntry> out;
+    for (size_t x = 0; x < cand.size(); ++x)
+        for (size_t y = 0; y < cand.size(); ++y)
+            if (x != y && cand[x].first == cand[y].first) { out.push_back(cand[x].second); break; }
+    return out;
+}
+
+// f(nx,ny,0:8) on the host -> both padded time levels: one host->device copy and a scatter
+// kernel (state_io.cu).
+int upload_state(mrlbm_handle* h, const double* f) {
+    const size_t n = (size_t)h->L.nx * h->L.ny * Q;
+    if (!h->d_fstage) CK(cudaMalloc((void**)&h->d_fstage, n * sizeof(double)));
+    CK(cudaMemcpyAsync(h->d_fstage, f, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const mrlbm_config& c = h->cfg;
+    CK(launch_scatter_state(h->precision, h->d_fstage, h->buf[0], h->buf[1], h->L, c.x_periodic != 0,
+                            c.y_periodic != 0, c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic, h->lat.w,
+                            h->stream));
+    ++h->launches;
+    h->cur = 0;
+    h->ovr = slot_conflicts(h);
+    const size_t N = (size_t)h->L.nx * h->L.ny;
+    for (OvrEntry& e : h->ovr) {
+        const double v = f[(size_t)(e.i - 1) + (size_t)h->L.nx * (e.j - 1) + N * e.k];
+        e.v = h->precision == MRLBM_FP64 ? v : (double)(float)(v - h->lat.w[e.k]);
+    }
     if (!h->ovr.empty()) {
         if (h->d_ovr) cudaFree(h->d_ovr);
         CK(cudaMalloc((void**)&h->d_ovr, h->ovr.size() * sizeof(OvrEntry)));
-        CK(cudaMemcpy(h->d_ovr, h->ovr.data(), h->ovr.size() * sizeof(OvrEntry), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(h->d_ovr, h->ovr.data(), h->ovr.size() * sizeof(OvrEntry), cudaMemcpyHostToDevice,
+                           h->stream));
     }
+    CK(cudaStreamSynchronize(h->stream));
     h->ovr_live = !h->ovr.empty();
     return MRLBM_OK;
 }
@@ -245,8 +237,66 @@ void fill_common(mrlbm_handle* h, StepParams<T>& p) {
     p.dc = h->dc;
 }
 
+// Claims one TMA step makes on the tile counter (see step_tma.cuh): every tile once plus
+// STAGES failing claims per persistent CTA.
+unsigned long long tma_claims_host(int nx, int ny, int bx, int by, int stages, int workers) {
+    return (unsigned long long)(((nx + bx - 1) / bx) * ((ny + by - 1) / by)) +
+           (unsigned long long)workers * (unsigned long long)stages;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* ptr = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)ptr;
+    }
+    return fn;
+}
+
+// Tensor maps (one per time level) and persistent CTA count for a TMA shape.  The map views a
+// level as a 2-D array of pitch columns and 9*(ny+2) rows (the nine direction planes stacked).
+int prepare_tma(mrlbm_handle* h, int cfg) {
+    if (h->tmap_cfg == cfg) return MRLBM_OK;
+    auto enc = tensor_map_encoder();
+    if (!enc) return fail(h, MRLBM_EUNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+    int bw, bh, st;
+    tma_box(h->precision, cfg, &bw, &bh, &st);
+    const int per_sm = tma_ctas_per_sm(h->precision, cfg);
+    if (per_sm < 0) {
+        cudaGetLastError();
+        return fail(h, MRLBM_ECUDA, std::string("TMA occupancy query: ") + cudaGetErrorString((cudaError_t)-per_sm));
+    }
+    if (per_sm == 0) return fail(h, MRLBM_EUNSUPPORTED, "TMA shape does not fit this precision");
+    if (!h->d_tile_ctr) {
+        CK(cudaMalloc((void**)&h->d_tile_ctr, sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(h->d_tile_ctr, 0, sizeof(unsigned long long), h->stream));
+        h->tile_base = 0;
+    }
+    for (int b = 0; b < 2; ++b) {
+        cuuint64_t dims[2] = {(cuuint64_t)h->L.pitch, (cuuint64_t)Q * (h->L.ny + 2)};
+        cuuint64_t strides[1] = {(cuuint64_t)h->L.pitch * h->elem};
+        cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+        cuuint32_t estr[2] = {1, 1};
+        CUresult r = enc(&h->tmap[b], h->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, h->buf[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(h, MRLBM_EUNSUPPORTED, "tensor map encoding failed");
+    }
+    h->workers = h->num_sms * per_sm;
+    h->tmap_cfg = cfg;
+    return MRLBM_OK;
+}
+
 int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     const int tc = h->tile_cfg;
+    const bool tma = tc >= TMA_CFG0;
+    if (tma) {
+        int prc = prepare_tma(h, tc);
+        if (prc != MRLBM_OK) return prc;
+    }
     int rc;
     if (h->precision == MRLBM_FP64) {
         StepParams<double> p{};
@@ -261,7 +311,12 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
         p.iter = h->iter;
         p.macro = macro ? h->d_macro : nullptr;
-        rc = launch_step_f64(p, tc, h->stream);
+        if (tma) {
+            p.tmap = h->tmap[h->cur];
+            p.tile_ctr = h->d_tile_ctr;
+            p.tile_base = h->tile_base;
+        }
+        rc = launch_step_f64(p, tc, h->stream, h->workers);
     } else {
         StepParams<float> p{};
         fill_common(h, p);
@@ -275,12 +330,26 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
         p.iter = h->iter;
         p.macro = macro ? h->d_macro : nullptr;
-        rc = launch_step_f32(p, tc, h->stream);
+        if (tma) {
+            p.tmap = h->tmap[h->cur];
+            p.tile_ctr = h->d_tile_ctr;
+            p.tile_base = h->tile_base;
+        }
+        rc = launch_step_f32(p, tc, h->stream, h->workers);
     }
     ++h->launches;
+    if (rc == -2) {
+        --h->launches;
+        return fail(h, MRLBM_EUNSUPPORTED, "tile shape does not fit this precision");
+    }
     if (rc != 0) {
         h->err = std::string("kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
         return MRLBM_ECUDA;
+    }
+    if (tma) {
+        int bw, bh, st;
+        tma_box(h->precision, tc, &bw, &bh, &st);
+        h->tile_base += tma_claims_host(h->L.nx, h->L.ny, TMA_CFGS[tc - TMA_CFG0].bx, bh, st, h->workers);
     }
     h->cur ^= 1;
     h->ovr_live = false;
@@ -292,7 +361,8 @@ void free_all(mrlbm_handle* h) {
     if (h->host_only) return;
     cudaSetDevice(h->device);
     for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
-                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, (void*)h->d_ovr})
+                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, (void*)h->d_ovr, (void*)h->d_fstage,
+                    (void*)h->d_tile_ctr})
         if (p) cudaFree(p);
     if (h->h_ring) cudaFreeHost(h->h_ring);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -382,7 +452,7 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
     h->L = make_layout(nx, ny, precision == MRLBM_FP64 ? 16 : 32);
     if (h->L.total() >= (int64_t)1 << 31) return bail(MRLBM_EINVAL, "grid too large for one handle (2^31 populations)");
     const char* tc = std::getenv("MRLBM_TILE_CFG");
-    if (tc) h->tile_cfg = std::max(0, std::min(N_TILE_CFGS - 1, std::atoi(tc)));
+    if (tc) h->tile_cfg = std::max(0, std::min(N_ALL_CFGS - 1, std::atoi(tc)));
     if (device == -1) {            // host-only handle: configuration and geometry, no device state
         h->host_only = true;
         h->iter = 1;
@@ -398,6 +468,7 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
         return true;
     };
     bool ok = ck(cudaSetDevice(device), "cudaSetDevice") &&
+              ck(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count") &&
               ck(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     h->stream = h->own_stream;
     const size_t bytes = (size_t)h->L.total() * h->elem;
@@ -408,8 +479,8 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
          ck(cudaMalloc((void**)&h->d_bint, nint * sizeof(int)), "cudaMalloc tables");
     const size_t nbox = std::max<size_t>(h->geo.boxmap.size(), 1);
     ok = ok && ck(cudaMalloc((void**)&h->d_boxmap, nbox * sizeof(int)), "cudaMalloc boxmap");
-    const int max_blk = nb / 16 + 2;
-    ok = ok && ck(cudaMalloc((void**)&h->d_partials, (size_t)max_blk * 3 * sizeof(double)), "cudaMalloc partials") &&
+    const size_t nscratch = 2 * (size_t)nb + (size_t)ny + 8;
+    ok = ok && ck(cudaMalloc((void**)&h->d_partials, nscratch * sizeof(double)), "cudaMalloc partials") &&
          ck(cudaMalloc((void**)&h->d_counter, sizeof(unsigned)), "cudaMalloc counter") &&
          ck(cudaMalloc((void**)&h->d_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMalloc ring") &&
          ck(cudaMalloc((void**)&h->d_err, sizeof(int)), "cudaMalloc err") &&
@@ -461,6 +532,7 @@ int mrlbm_status(mrlbm_handle* h) {
     int e = 0;
     CK(cudaMemcpyAsync(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    if (e & 4) return fail(h, MRLBM_EDEVICE_TIMEOUT, "device flag: tensor-copy wait timed out");
     if (e) return fail(h, MRLBM_EDEVICE_NAN, "device flag: NaN or non-positive density");
     return MRLBM_OK;
 }
@@ -532,19 +604,13 @@ int mrlbm_get_state(mrlbm_handle* h, double* f) {
     CK(cudaSetDevice(h->device));
     const int nx = h->L.nx, ny = h->L.ny;
     const size_t N = (size_t)nx * ny;
-    const int64_t total = h->L.total();
-    std::vector<unsigned char> b((size_t)total * h->elem);
-    CK(cudaMemcpyAsync(b.data(), h->buf[h->cur], b.size(), cudaMemcpyDeviceToHost, h->stream));
+    if (!h->d_fstage) CK(cudaMalloc((void**)&h->d_fstage, N * Q * sizeof(double)));
+    const mrlbm_config& c = h->cfg;
+    CK(launch_gather_state(h->precision, h->buf[h->cur], h->d_fstage, h->L, c.x_periodic != 0, c.y_periodic != 0,
+                           c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic, h->lat.w, h->stream));
+    ++h->launches;
+    CK(cudaMemcpyAsync(f, h->d_fstage, N * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    for (int k = 0; k < Q; ++k)
-        for (int j = 1; j <= ny; ++j)
-            for (int i = 1; i <= nx; ++i) {
-                const int64_t s = slot_of(h, i, j, k);
-                double v;
-                if (h->precision == MRLBM_FP64) v = ((const double*)b.data())[s];
-                else v = h->lat.w[k] + (double)((const float*)b.data())[s];
-                f[(size_t)(i - 1) + (size_t)nx * (j - 1) + N * k] = v;
-            }
     if (h->ovr_live)
         for (const OvrEntry& e : h->ovr)
             f[(size_t)(e.i - 1) + (size_t)nx * (e.j - 1) + N * e.k] =
@@ -655,21 +721,8 @@ int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32
     StepParams<float> p32{};
     if (h->precision == MRLBM_FP64) { fill_common(h, p64); nc.p64 = &p64; }
     else { fill_common(h, p32); nc.p32 = &p32; }
-    if (d_f0) {
-        // destinations whose streaming slot another destination also uses (corner wraps)
-        std::vector<std::pair<int64_t, OvrEntry>> cand;
-        const int ci[2] = {1, h->L.nx}, cj[2] = {1, h->L.ny};
-        for (int a = 0; a < 2; ++a)
-            for (int b = 0; b < 2; ++b)
-                for (int k = 0; k < Q; ++k) cand.push_back({slot_of(h, ci[a], cj[b], k), OvrEntry{ci[a], cj[b], k, 0, 0.0}});
-        for (size_t x = 0; x < cand.size(); ++x) {
-            bool shared = false;
-            for (size_t y = 0; y < cand.size(); ++y)
-                if (x != y && cand[x].first == cand[y].first) shared = true;
-            if (shared) nc.conflicts.push_back(cand[x].second);
-        }
-    }
-    nc.tile_cfg = h->tile_cfg;
+    if (d_f0) nc.conflicts = slot_conflicts(h);
+    nc.tile_cfg = h->tile_cfg < TMA_CFG0 ? h->tile_cfg : 1;   // TMA shapes need handle-owned counters
     nc.iter = h->iter;
     nc.cur = h->cur;
     nc.launches = h->launches;
@@ -680,6 +733,84 @@ int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32
     h->launches = nc.launches;
     if (rc != MRLBM_OK) h->err = err;
     return rc;
+}
+
+int mrlbm_set_tile_config(mrlbm_handle* h, int32_t cfg) {
+    if (!h || cfg < 0 || cfg >= N_ALL_CFGS) return MRLBM_EINVAL;
+    h->tile_cfg = cfg;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_tile_config(const mrlbm_handle* h, int32_t* cfg) {
+    if (!h || !cfg) return MRLBM_EINVAL;
+    *cfg = h->tile_cfg;
+    return MRLBM_OK;
+}
+
+int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, double* best_ms) {
+    if (!h || trial_steps < 1) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    int drc = drain_ring(h);                            // pending records go to the history first
+    if (drc != MRLBM_OK) return drc;
+    // everything a trial changes is saved and put back: both time levels, iteration, ring
+    const size_t bytes = (size_t)h->L.total() * h->elem;
+    void* save[2] = {nullptr, nullptr};
+    CK(cudaMalloc(&save[0], bytes));
+    if (cudaMalloc(&save[1], bytes) != cudaSuccess) {
+        cudaFree(save[0]);
+        return fail(h, MRLBM_ECUDA, "cudaMalloc autotune save");
+    }
+    auto cleanup = [&]() { cudaFree(save[0]); cudaFree(save[1]); };
+    const int iter0 = h->iter, cur0 = h->cur, ring0 = h->ring_n;
+    const bool ovr0 = h->ovr_live;
+    const size_t hist0 = h->hist.size();
+    for (int b = 0; b < 2; ++b)
+        if (cudaMemcpyAsync(save[b], h->buf[b], bytes, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess) {
+            cleanup();
+            return fail(h, MRLBM_ECUDA, "autotune save copy");
+        }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int cfg0 = h->tile_cfg;
+    int best = cfg0;
+    float best_t = 1e30f;
+    int rc = MRLBM_OK;
+    for (int c = 0; c < N_ALL_CFGS && rc == MRLBM_OK; ++c) {
+        h->tile_cfg = c;
+        rc = mrlbm_step(h, 1, 0);                       // warm-up (and instruction cache)
+        if (rc == MRLBM_EUNSUPPORTED) { rc = MRLBM_OK; continue; }   // shape does not fit
+        if (rc != MRLBM_OK) break;
+        cudaEventRecord(e0, h->stream);
+        rc = mrlbm_step(h, trial_steps, 0);
+        cudaEventRecord(e1, h->stream);
+        if (rc != MRLBM_OK || cudaEventSynchronize(e1) != cudaSuccess) { rc = rc ? rc : MRLBM_ECUDA; break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_t) { best_t = ms; best = c; }
+        // restore before the next trial so every shape starts from the same state
+        for (int b = 0; b < 2; ++b)
+            if (cudaMemcpyAsync(h->buf[b], save[b], bytes, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+                rc = MRLBM_ECUDA;
+        h->iter = iter0;
+        h->cur = cur0;
+        h->ring_n = ring0;
+        h->ovr_live = ovr0;
+        h->hist.resize(hist0);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(h->stream);
+    cleanup();
+    if (rc != MRLBM_OK) {
+        h->tile_cfg = cfg0;
+        return rc;
+    }
+    h->tile_cfg = best;
+    if (best_cfg) *best_cfg = best;
+    if (best_ms) *best_ms = best_t / trial_steps;
+    return MRLBM_OK;
 }
 
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n) {

@@ -19,6 +19,7 @@
 #include "../../include/mrlbm.h"
 #include "geometry.h"
 #include "noalloc.h"
+#include "state_io.h"
 #include "step_params.h"
 
 namespace mrlbm {
@@ -26,21 +27,21 @@ namespace mrlbm {
 // ---- fixed device storage (the scratch of the step kernel and the case tables) ---------
 constexpr int NA_MAX_NB = 1024;                      // curved-wall nodes
 constexpr int NA_MAX_BOX = 512 * 512;                // cells of the cylinder bounding box
-constexpr int NA_MAX_BLOCKS = NA_MAX_NB / 16 + 2;    // boundary blocks (16-node blocks at most)
+constexpr int NA_MAX_NY = 8192;                      // rows (the inlet column sum is per row)
 constexpr int NA_RING = 4096;                        // stats records buffered per drain
 constexpr int NA_MAX_OVR = 64;                       // loaded-state corner overrides
 
 static __device__ __align__(256) double na_geo[G_NFIELDS * NA_MAX_NB];        // FP64 or FP32 tables
 static __device__ __align__(256) int na_int[I_NFIELDS * NA_MAX_NB];
 static __device__ __align__(256) int na_box[NA_MAX_BOX];
-static __device__ __align__(256) double na_partials[3 * NA_MAX_BLOCKS];
+static __device__ __align__(256) double na_partials[2 * NA_MAX_NB + NA_MAX_NY];
 static __device__ __align__(256) unsigned na_counter[1];
 static __device__ __align__(256) int na_err[1];
 static __device__ __align__(256) double na_ring[REC_WORDS * NA_RING];
 static __device__ __align__(256) OvrEntry na_ovr[NA_MAX_OVR];
 
 constexpr size_t NA_STATIC_BYTES = sizeof(double) * G_NFIELDS * NA_MAX_NB + sizeof(int) * I_NFIELDS * NA_MAX_NB +
-                                   sizeof(int) * NA_MAX_BOX + sizeof(double) * 3 * NA_MAX_BLOCKS +
+                                   sizeof(int) * NA_MAX_BOX + sizeof(double) * (2 * NA_MAX_NB + NA_MAX_NY) +
                                    sizeof(double) * REC_WORDS * NA_RING + sizeof(OvrEntry) * NA_MAX_OVR + 16;
 
 struct NaSymbols {
@@ -80,37 +81,6 @@ static cudaError_t na_symbols(int dev, NaSymbols** out) {
     return cudaSuccess;
 }
 
-// Scatter f(nx,ny,0:8) (Fortran order, FP64, caller's device memory) into both padded
-// buffers: population (i,j,k) goes to the slot its next-step gather reads (stream_source).
-template <class T>
-__global__ void scatter_state(const double* __restrict__ f0, T* a, T* b, Layout L, int xper, int yper, int freeslip,
-                              double w0, double w1, double w5, int deviation) {
-    const int64_t N = (int64_t)L.nx * L.ny;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N * Q) return;
-    const int k = (int)(t / N);
-    const int64_t n = t - (int64_t)k * N;
-    const int i = (int)(n % L.nx) + 1, j = (int)(n / L.nx) + 1;
-    const SrcSlot s = stream_source(L.nx, L.ny, i, j, k, xper != 0, yper != 0, freeslip != 0);
-    const int64_t slot = L.at(s.i, s.j, s.k);
-    const double wk = k == 0 ? w0 : (k < 5 ? w1 : w5);
-    const T v = deviation ? (T)(f0[t] - wk) : (T)f0[t];
-    a[slot] = v;
-    b[slot] = v;
-}
-
-// Values of the override entries (destinations whose slot another destination shares).
-template <class T>
-__global__ void fill_overrides(const double* __restrict__ f0, OvrEntry* ovr, int n, int nx, int ny, double w0,
-                               double w1, double w5, int deviation) {
-    const int q = threadIdx.x;
-    if (q >= n) return;
-    const OvrEntry e = ovr[q];
-    const double v = f0[(int64_t)(e.i - 1) + (int64_t)nx * (e.j - 1) + (int64_t)nx * ny * e.k];
-    const double wk = e.k == 0 ? w0 : (e.k < 5 ? w1 : w5);
-    ovr[q].v = deviation ? (double)(T)(v - wk) : v;
-}
-
 int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, double* records, int32_t* n_records,
                  void* stream, std::string& err) {
     if (n_records) *n_records = 0;
@@ -122,6 +92,10 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
     }
     if ((int64_t)g.boxmap.size() > NA_MAX_BOX) {
         err = "mrlbm_step_noalloc supports a cylinder bounding box of at most " + std::to_string(NA_MAX_BOX) + " cells";
+        return MRLBM_EINVAL;
+    }
+    if (c.L.ny > NA_MAX_NY) {
+        err = "mrlbm_step_noalloc supports at most " + std::to_string(NA_MAX_NY) + " rows";
         return MRLBM_EINVAL;
     }
     if (!d_state) { err = "d_state is NULL"; return MRLBM_EINVAL; }
@@ -153,24 +127,15 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
     bool ovr_live = false;
     int n_ovr = 0;
     if (d_f0) {
-        const int64_t total = (int64_t)c.L.nx * c.L.ny * Q;
-        const unsigned blocks = (unsigned)((total + 255) / 256);
-        const int dev32 = c.precision == MRLBM_FP32;
-        if (c.precision == MRLBM_FP64)
-            scatter_state<double><<<blocks, 256, 0, st>>>(d_f0, (double*)half[0], (double*)half[1], c.L, c.xper, c.yper,
-                                                          c.freeslip, c.w[0], c.w[1], c.w[5], 0);
-        else
-            scatter_state<float><<<blocks, 256, 0, st>>>(d_f0, (float*)half[0], (float*)half[1], c.L, c.xper, c.yper,
-                                                         c.freeslip, c.w[0], c.w[1], c.w[5], 1);
+        e = launch_scatter_state(c.precision, d_f0, half[0], half[1], c.L, c.xper, c.yper, c.freeslip, c.w, st);
+        if (e != cudaSuccess) { err = cudaGetErrorString(e); return MRLBM_ECUDA; }
         n_ovr = (int)c.conflicts.size();
         if (n_ovr > NA_MAX_OVR) { err = "too many loaded-state overrides"; return MRLBM_EINVAL; }
         if (n_ovr > 0) {
             e = cudaMemcpyAsync(S->ovr, c.conflicts.data(), (size_t)n_ovr * sizeof(OvrEntry), cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) { err = cudaGetErrorString(e); return MRLBM_ECUDA; }
-            if (c.precision == MRLBM_FP64)
-                fill_overrides<double><<<1, 64, 0, st>>>(d_f0, S->ovr, n_ovr, c.L.nx, c.L.ny, c.w[0], c.w[1], c.w[5], 0);
-            else
-                fill_overrides<float><<<1, 64, 0, st>>>(d_f0, S->ovr, n_ovr, c.L.nx, c.L.ny, c.w[0], c.w[1], c.w[5], dev32);
+            e = launch_fill_overrides(c.precision, d_f0, S->ovr, n_ovr, c.L.nx, c.L.ny, c.w, st);
+            if (e != cudaSuccess) { err = cudaGetErrorString(e); return MRLBM_ECUDA; }
             ovr_live = true;
         }
         c.cur = 0;
@@ -213,7 +178,7 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
             p.u_in = nullptr;
             p.ovr = ovr_live ? S->ovr : nullptr;
             p.n_ovr = ovr_live ? n_ovr : 0;
-            rc = launch_step_f64(p, c.tile_cfg, st);
+            rc = launch_step_f64(p, c.tile_cfg, st, 0);
         } else {
             StepParams<float> p = *c.p32;
             p.src = (const float*)half[c.cur];
@@ -232,7 +197,7 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
             p.u_in = nullptr;
             p.ovr = ovr_live ? S->ovr : nullptr;
             p.n_ovr = ovr_live ? n_ovr : 0;
-            rc = launch_step_f32(p, c.tile_cfg, st);
+            rc = launch_step_f32(p, c.tile_cfg, st, 0);
         }
         ++c.launches;
         if (rc != 0) { err = std::string("kernel launch failed: ") + cudaGetErrorString(cudaGetLastError()); return MRLBM_ECUDA; }

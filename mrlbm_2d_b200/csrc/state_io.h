@@ -1,0 +1,21 @@
+// state_io.h -- conversion between the reference's f(nx,ny,0:8) and the padded pull layout.
+#pragma once
+#include <cuda_runtime.h>
+#include "step_params.h"
+
+namespace mrlbm {
+
+// f0 (Fortran order, FP64, device) -> both padded time levels a and b (FP64 values, or FP32
+// deviations f - w_k when precision == 32).  Population (i,j,k) goes to the slot its
+// next-step gather reads (stream_source).
+cudaError_t launch_scatter_state(int precision, const double* f0, void* a, void* b, const Layout& L, int xper,
+                                 int yper, int freeslip, const double* w, cudaStream_t s);
+// padded time level src -> f (Fortran order, FP64, device): the populations the next
+// step's gather reads, i.e. the reference's post-streaming f.
+cudaError_t launch_gather_state(int precision, const void* src, double* f, const Layout& L, int xper, int yper,
+                                int freeslip, const double* w, cudaStream_t s);
+// override entries (destinations sharing a streaming slot) take their values from f0.
+cudaError_t launch_fill_overrides(int precision, const double* f0, OvrEntry* ovr, int n, int nx, int ny,
+                                  const double* w, cudaStream_t s);
+
+}  // namespace mrlbm

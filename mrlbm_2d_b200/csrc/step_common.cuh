@@ -60,24 +60,6 @@ __device__ __forceinline__ int node_class(const StepParams<T>& p, int i, int j) 
     return CLS_FLUID;
 }
 
-// Block reduction of three doubles with warp shuffles; result valid in thread 0.
-__device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, double* sm) {
-    const unsigned full = 0xffffffffu;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(full, a, o);
-        b += __shfl_down_sync(full, b, o);
-        c += __shfl_down_sync(full, c, o);
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane == 0) { sm[3 * wid] = a; sm[3 * wid + 1] = b; sm[3 * wid + 2] = c; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        a = sm[0]; b = sm[1]; c = sm[2];
-        for (int w = 1; w < nw; ++w) { a += sm[3 * w]; b += sm[3 * w + 1]; c += sm[3 * w + 2]; }
-    }
-}
-
 // Boundary blocks own BNODES curved-wall nodes each, BLANES lanes per node.  The block first
 // stages its nodes' tables in shared memory with coalesced loads.  Lane c of a node then
 // pulls stencil node c (reference point 2 for c < 4, point 3 otherwise), computes its
@@ -149,36 +131,56 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
     }
     const T ux3 = __shfl_down_sync(full, ux, 4, BLANES), uy3 = __shfl_down_sync(full, uy, 4, BLANES);
     const T mx3 = __shfl_down_sync(full, mx, 4, BLANES), my3 = __shfl_down_sync(full, my, 4, BLANES);
-    double Fx = 0.0, Fy = 0.0, rin = 0.0;
-    if (active && lane == 0) Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
+    double Fx = 0.0, Fy = 0.0;
+    if (active && lane == 0) {
+        Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
+        if (p.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
+    }
     if (!p.do_stats) return;
-    // sum(rho(1,:)) for the inlet running mean (2d_mrlbm.f90:359), whatever the x boundary
-    for (int j = 1 + blockIdx.x * nthr + tid; j <= p.L.ny; j += p.nbblk * nthr) rin += Phys::inlet_rho(p, j);
-    block_reduce3(Fx, Fy, rin, sm);
+    // rho(1,j) after the closures, for the inlet running mean (2d_mrlbm.f90:359)
+    for (int j = 1 + blockIdx.x * nthr + tid; j <= p.L.ny; j += p.nbblk * nthr)
+        p.partials[2 * p.nb + j - 1] = Phys::inlet_rho(p, j);
+    // The last block to arrive sums the per-node forces and the inlet column in index order,
+    // as the reference's sum() does (2d_mrlbm.f90:359, 488-489): the result does not depend on
+    // the launch shape and equals the reference's sums bit for bit.
+    __shared__ unsigned ticket;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) ticket = atomicAdd(p.counter, 1u);
+    __syncthreads();
+    if (ticket != (unsigned)(p.nbblk - 1)) return;
+    __threadfence();
+    const int w = tid >> 5;
+    if ((tid & 31) == 0 && w < 3) {
+        const int n = w < 2 ? p.nb : p.L.ny;
+        const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
+        double acc = 0.0;
+        for (int q = 0; q < n; ++q) acc = acc + __ldcg(v + q);
+        sm[w] = acc;
+    }
+    __syncthreads();
     if (tid == 0) {
-        p.partials[3 * blockIdx.x] = Fx;
-        p.partials[3 * blockIdx.x + 1] = Fy;
-        p.partials[3 * blockIdx.x + 2] = rin;
-        __threadfence();
-        const unsigned ticket = atomicAdd(p.counter, 1u);
-        if (ticket == (unsigned)(p.nbblk - 1)) {
-            __threadfence();
-            double a = 0.0, b = 0.0, cc = 0.0;
-            for (int q = 0; q < p.nbblk; ++q) {
-                a += __ldcg(p.partials + 3 * q);
-                b += __ldcg(p.partials + 3 * q + 1);
-                cc += __ldcg(p.partials + 3 * q + 2);
-            }
-            if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = a; p.rec[2] = b; p.rec[3] = cc; }
-            *p.counter = 0u;
-        }
+        if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = sm[0]; p.rec[2] = sm[1]; p.rec[3] = sm[2]; }
+        *p.counter = 0u;
     }
 }
 
+// Interior populations (no wraps, no ghosts): the branch-free half of `gather`.
+template <class T>
+__device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, int j, T f[Q]) {
+    const int pitch = p.L.pitch, plane = (int)p.L.plane;
+    const T* s = p.src + ((int)(j * pitch + i + p.L.off));
+#pragma unroll
+    for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
+}
+
 // One time step.  Blocks [0, nbblk) are boundary blocks; the rest are bulk tiles of
-// BX x (BY*NJ) nodes, one thread per column and NJ rows.
+// BX x (BY*NJ) nodes, one thread per column and NJ rows.  A thread first issues the loads of
+// all its interior rows, then finishes them (collide and store) one by one, so up to 9*NJ
+// loads per thread are in flight; edge rows and columns take the out-of-line edge path.
 template <class Phys, int BX, int BY, int NJ, int MINB>
-__global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const typename Phys::P p) {
+__global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
+    using T = typename Phys::T;
     if ((int)blockIdx.x < p.nbblk) {
         boundary_block<Phys>(p);
         return;
@@ -187,11 +189,28 @@ __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const typename Phys
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
     const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
     const int i = 1 + tx * BX + lx;
-    if (i > p.L.nx) return;
+    const int nx = p.L.nx, ny = p.L.ny;
+    if (i > nx) return;
+    T f[NJ][Q];
+    int cls[NJ];
+    unsigned interior = 0u;
 #pragma unroll
     for (int r = 0; r < NJ; ++r) {
         const int j = 1 + ty * BY * NJ + r * BY + ly;
-        if (j <= p.L.ny) Phys::bulk_node(p, i, j);
+        cls[r] = CLS_FLUID;
+        if (j <= ny) {
+            cls[r] = node_class(p, i, j);
+            if (cls[r] < 0 && i > 1 && i < nx && j > 1 && j < ny) {
+                gather_interior(p, i, j, f[r]);
+                interior |= 1u << r;
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NJ; ++r) {
+        const int j = 1 + ty * BY * NJ + r * BY + ly;
+        if ((interior >> r) & 1u) Phys::finish(p, i, j, cls[r], f[r]);
+        else if (j <= ny && cls[r] < 0) Phys::edge_bulk_node(p, i, j, cls[r]);
     }
 }
 

@@ -1,18 +1,47 @@
 // step_f32.cu -- FP32 deviation-form fused step instantiations (contraction allowed).
 #include "step_fp32.cuh"
+#include "step_tma.cuh"
 
 namespace mrlbm {
 
-int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream) {
+int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers) {
     cudaStream_t s = (cudaStream_t)stream;
     using Ph = fp32::Physics;
     switch (tile_cfg) {
-    case 0: return launch_step_tiles<Ph, 32, 8, 1, 4>(p, s);
-    case 1: return launch_step_tiles<Ph, 32, 8, 2, 4>(p, s);
-    case 2: return launch_step_tiles<Ph, 32, 4, 4, 8>(p, s);
-    case 3: return launch_step_tiles<Ph, 64, 4, 2, 4>(p, s);
+#define MRLBM_TILE_CASE(id, bx, by, nj, mb) \
+    case id: return launch_step_tiles<Ph, bx, by, nj, mb>(p, s);
+        MRLBM_TILE_LIST(MRLBM_TILE_CASE)
+#undef MRLBM_TILE_CASE
+#define MRLBM_TMA_CASE(id, bx, by, st) \
+    case id: return launch_step_tma<Ph, bx, by, st>(p, s, workers);
+        MRLBM_TMA_LIST(MRLBM_TMA_CASE)
+#undef MRLBM_TMA_CASE
     default: return -1;
     }
+}
+
+int tma_ctas_per_sm_f32(int tile_cfg) {
+    int n = 0;
+    switch (tile_cfg) {
+#define MRLBM_TMA_OCC(id, bx, by, st) \
+    case id: n = tma_occupancy(step_kernel_tma<fp32::Physics, bx, by, st>, bx, st * TmaGeom<float, bx, by>::STAGE_BYTES + 128); break;
+        MRLBM_TMA_LIST(MRLBM_TMA_OCC)
+#undef MRLBM_TMA_OCC
+    default: n = 0;
+    }
+    return n;
+}
+
+int tma_ctas_per_sm(int precision, int tile_cfg) {
+    return precision == 64 ? tma_ctas_per_sm_f64(tile_cfg) : tma_ctas_per_sm_f32(tile_cfg);
+}
+
+void tma_box(int precision, int tile_cfg, int* box_w, int* box_h, int* stages) {
+    const TmaCfg c = TMA_CFGS[tile_cfg - TMA_CFG0];
+    const int m = 16 / (precision == 64 ? 8 : 4);
+    *box_w = c.bx + 2 * m;
+    *box_h = c.by;
+    *stages = c.stages;
 }
 
 }  // namespace mrlbm

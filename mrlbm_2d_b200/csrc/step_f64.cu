@@ -1,19 +1,36 @@
 // step_f64.cu -- FP64 fused step instantiations.  Built with -fmad=false so every product
 // and sum rounds separately, as in the reference's x86-64 FP64 arithmetic.
 #include "step_fp64.cuh"
+#include "step_tma.cuh"
 
 namespace mrlbm {
 
-int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream) {
+int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers) {
     cudaStream_t s = (cudaStream_t)stream;
     using Ph = fp64::Physics;
-    switch (tile_cfg) {   // minimum resident blocks sized for a 64-register budget
-    case 0: return launch_step_tiles<Ph, 32, 8, 1, 4>(p, s);
-    case 1: return launch_step_tiles<Ph, 32, 8, 2, 4>(p, s);
-    case 2: return launch_step_tiles<Ph, 32, 4, 4, 8>(p, s);
-    case 3: return launch_step_tiles<Ph, 64, 4, 2, 4>(p, s);
+    switch (tile_cfg) {
+#define MRLBM_TILE_CASE(id, bx, by, nj, mb) \
+    case id: return launch_step_tiles<Ph, bx, by, nj, mb>(p, s);
+        MRLBM_TILE_LIST(MRLBM_TILE_CASE)
+#undef MRLBM_TILE_CASE
+#define MRLBM_TMA_CASE(id, bx, by, st) \
+    case id: return launch_step_tma<Ph, bx, by, st>(p, s, workers);
+        MRLBM_TMA_LIST(MRLBM_TMA_CASE)
+#undef MRLBM_TMA_CASE
     default: return -1;
     }
+}
+
+int tma_ctas_per_sm_f64(int tile_cfg) {
+    int n = 0;
+    switch (tile_cfg) {
+#define MRLBM_TMA_OCC(id, bx, by, st) \
+    case id: n = tma_occupancy(step_kernel_tma<fp64::Physics, bx, by, st>, bx, st * TmaGeom<double, bx, by>::STAGE_BYTES + 128); break;
+        MRLBM_TMA_LIST(MRLBM_TMA_OCC)
+#undef MRLBM_TMA_OCC
+    default: n = 0;
+    }
+    return n;
 }
 
 }  // namespace mrlbm

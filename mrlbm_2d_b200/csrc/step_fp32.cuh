@@ -259,13 +259,23 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<float>& tb, i
     if (p.node_force) { p.node_force[2 * l] = Fx; p.node_force[2 * l + 1] = Fy; }
 }
 
-__device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
-    const int cls = node_class(p, i, j);
-    if (cls >= 0) return;
+// Edge nodes: own gather, Dirichlet values and closures (out of line, see the FP64 step).
+__device__ __noinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
     float g[Q];
     gather(p, i, j, g);
     Mac m = moments(p, g);
-    if (i == 1 || i == p.L.nx || j == 1 || j == p.L.ny) edge_node(p, i, j, g, m);
+    edge_node(p, i, j, g, m);
+    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
+    if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
+    if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    float go[Q];
+    collide(p, m, go);
+    store(p, i, j, go);
+}
+
+// Interior fluid or solid node: populations already gathered.
+__device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const float g[Q]) {
+    Mac m = moments(p, g);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
@@ -277,7 +287,12 @@ __device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
 struct Physics {
     using P = StepParams<float>;
     using T = float;
-    static __device__ __forceinline__ void bulk_node(const P& p, int i, int j) { fp32::bulk_node(p, i, j); }
+    static __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const T g[Q]) {
+        fp32::finish(p, i, j, cls, g);
+    }
+    static __device__ __forceinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
+        fp32::edge_bulk_node(p, i, j, cls);
+    }
     static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
                                                         T& mx, T& my) {
         fp32::stencil_node(p, si, sj, cc, ss, s2, ux, uy, mx, my);
@@ -287,7 +302,7 @@ struct Physics {
                                                           double& Fy) {
         fp32::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
-    static __device__ __forceinline__ double inlet_rho(const P& p, int j) {
+    static __device__ __noinline__ double inlet_rho(const P& p, int j) {
         float g[Q];
         gather(p, 1, j, g);
         Mac m = moments(p, g);

@@ -385,14 +385,25 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
     if (p.node_force) { p.node_force[2 * l] = Fx; p.node_force[2 * l + 1] = Fy; }
 }
 
-// Bulk node (fluid or solid, including edges).
-__device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
-    const int cls = node_class(p, i, j);
-    if (cls >= 0) return;                       // curved-wall node: owned by a boundary block
+// Edge nodes (first/last row or column): own gather, Dirichlet values and closures.  Out
+// of line so the interior path keeps its populations in registers.
+__device__ __noinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
     double f[Q];
     gather(p, i, j, f);
     Mac m = moments(f, p.hm, p.hp);
-    if (i == 1 || i == p.L.nx || j == 1 || j == p.L.ny) edge_node(p, i, j, f, m);
+    edge_node(p, i, j, f, m);
+    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
+    if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
+    if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    double fo[Q];
+    collide(p, m, fo);
+    store(p, i, j, fo);
+}
+
+// Bulk node (fluid or solid).
+// Interior fluid or solid node: populations already gathered.
+__device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const double f[Q]) {
+    Mac m = moments(f, p.hm, p.hp);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
@@ -404,7 +415,12 @@ __device__ __forceinline__ void bulk_node(const P& p, int i, int j) {
 struct Physics {
     using P = StepParams<double>;
     using T = double;
-    static __device__ __forceinline__ void bulk_node(const P& p, int i, int j) { fp64::bulk_node(p, i, j); }
+    static __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const T f[Q]) {
+        fp64::finish(p, i, j, cls, f);
+    }
+    static __device__ __forceinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
+        fp64::edge_bulk_node(p, i, j, cls);
+    }
     static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
                                                         T& mx, T& my) {
         fp64::stencil_node(p, si, sj, cc, ss, s2, ux, uy, mx, my);
@@ -414,7 +430,7 @@ struct Physics {
                                                           double& Fy) {
         fp64::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
-    static __device__ __forceinline__ double inlet_rho(const P& p, int j) {
+    static __device__ __noinline__ double inlet_rho(const P& p, int j) {
         double f[Q];
         gather(p, 1, j, f);
         return node_macro(p, 1, j, f).rho;

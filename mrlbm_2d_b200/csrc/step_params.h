@@ -1,5 +1,6 @@
 // step_params.h -- parameter block of one fused time-step launch (host <-> device contract).
 #pragma once
+#include <cuda.h>
 #include <cstdint>
 #include "lattice.h"
 
@@ -38,7 +39,10 @@ struct DevConsts {
 struct OvrEntry { int i, j, k, pad; double v; };
 
 template <class T>
-struct StepParams {
+struct alignas(64) StepParams {
+    CUtensorMap tmap;             // 2-D map of src (rows = 9 planes x (ny+2)), TMA shapes only
+    unsigned long long* tile_ctr; // tile claim counter of the TMA shapes
+    unsigned long long tile_base; // counter value at the start of this step
     const T* __restrict__ src;    // fout of the previous step (+ ghost ring)
     T* __restrict__ dst;          // fout of this step
     Layout L;
@@ -62,7 +66,7 @@ struct StepParams {
     const int* __restrict__ boxmap;
     int label15_allnine;
     // reduction scratch and output
-    double* partials;             // [nbblk * 3]
+    double* partials;             // per-step scratch: Fx[nb], Fy[nb], rho(1,j)[ny]
     unsigned* counter;            // arrival counter of boundary blocks (reset by the last)
     double* rec;                  // REC_WORDS doubles for this step, or null
     double* node_force;           // optional per-boundary-node (Fx, Fy) [2 * nb], or null
@@ -74,13 +78,51 @@ struct StepParams {
     DevConsts dc;                 // deviation-form constants (FP32 only)
 };
 
-// Host-side launch entry points (defined in step_f64.cu / step_f32.cu).
-int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream);
-int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream);
+// Bulk tile shapes of step_kernel (threads BX x BY, NJ rows per thread, MINB resident blocks
+// per SM, which sets the register budget 65536 / (BX*BY*MINB)).  The autotuner picks one.
+struct TileCfg { int bx, by, nj, minb; };
+#define MRLBM_TILE_LIST(X) \
+    X(0, 32, 8, 1, 4)      \
+    X(1, 32, 8, 2, 4)      \
+    X(2, 32, 8, 2, 3)      \
+    X(3, 32, 4, 4, 4)      \
+    X(4, 32, 4, 4, 6)      \
+    X(5, 32, 8, 4, 3)      \
+    X(6, 64, 4, 2, 4)      \
+    X(7, 32, 4, 8, 4)      \
+    X(8, 32, 8, 4, 2)      \
+    X(9, 32, 4, 2, 8)
+constexpr int N_TILE_CFGS = 10;
+#define MRLBM_TILE_ENTRY(id, bx, by, nj, mb) {bx, by, nj, mb},
+constexpr TileCfg TILE_CFGS[N_TILE_CFGS] = {MRLBM_TILE_LIST(MRLBM_TILE_ENTRY)};
+#undef MRLBM_TILE_ENTRY
 
-// Tile configurations (bulk threads: 32 x BY, each thread NJ nodes along y).
-struct TileCfg { int bx, by, nj; };
-constexpr int N_TILE_CFGS = 4;
-constexpr TileCfg TILE_CFGS[N_TILE_CFGS] = {{32, 8, 1}, {32, 8, 2}, {32, 4, 4}, {64, 4, 2}};
+// TMA-fed persistent shapes of step_kernel_tma (BX threads = columns per tile, BY rows per
+// tile, STAGES tiles in flight per CTA).  Shape ids continue after the step_kernel ones.
+// The copy box is BX + 32 bytes wide, which must stay within the 256-element box limit.
+struct TmaCfg { int bx, by, stages; };
+#define MRLBM_TMA_LIST(X) \
+    X(10, 128, 4, 4)      \
+    X(11, 128, 2, 6)      \
+    X(12, 224, 2, 4)      \
+    X(13, 128, 8, 3)      \
+    X(14, 64, 4, 6)       \
+    X(15, 224, 4, 3)
+constexpr int N_TMA_CFGS = 6;
+constexpr int TMA_CFG0 = N_TILE_CFGS;
+constexpr int N_ALL_CFGS = N_TILE_CFGS + N_TMA_CFGS;
+#define MRLBM_TMA_ENTRY(id, bx, by, st) {bx, by, st},
+constexpr TmaCfg TMA_CFGS[N_TMA_CFGS] = {MRLBM_TMA_LIST(MRLBM_TMA_ENTRY)};
+#undef MRLBM_TMA_ENTRY
+
+// Host-side launch entry points (step_f64.cu / step_f32.cu).  `workers` is the persistent
+// CTA count for TMA shapes (ignored otherwise).  Return 0, -1 on a launch error, -2 when the
+// shape does not fit this precision.
+int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers);
+int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers);
+// Persistent CTAs one SM holds for a TMA shape (0 when the shape does not fit).
+int tma_ctas_per_sm(int precision, int tile_cfg);
+// Bytes of one tensor-map box row and rows per box for a TMA shape.
+void tma_box(int precision, int tile_cfg, int* box_w, int* box_h, int* stages);
 
 }  // namespace mrlbm

@@ -4,8 +4,8 @@ memory (their device memory comes from their own runtime, pool or arena).
 The case comes from a host-only handle (no device allocation); the caller -- here the test,
 through torch -- owns the two population time levels and the initial populations.  The
 result must equal the ordinary entry point's (mrlbm_step on a device handle) within the
-tolerances of the parity tests: populations exactly, per-step force and inlet-density sums
-to 1e-12 relative, over two calls in a row.  The file is collected last on purpose.
+tolerances of the parity tests -- exact equality for the populations and for the per-step
+force and inlet-density sums -- over two calls in a row.  The file is collected last on purpose.
 """
 import numpy as np
 import pytest
@@ -85,9 +85,8 @@ def test_step_noalloc_matches_step(mrlbm, name):
     assert np.array_equal(f2, f_b)
     for rec, it, fd, fl, rin in ((rec1, it_a, fd_a, fl_a, rin_a), (rec2, it_b, fd_b, fl_b, rin_b)):
         assert np.array_equal(rec[:, 0].astype(int), it)
-        np.testing.assert_allclose(rec[:, 1], fd, rtol=1e-12, atol=1e-13)
-        np.testing.assert_allclose(rec[:, 2], fl, rtol=1e-12, atol=1e-13)
-        np.testing.assert_allclose(rec[:, 3], rin, rtol=1e-12)
+        assert np.array_equal(rec[:, 1], fd) and np.array_equal(rec[:, 2], fl)
+        assert np.array_equal(rec[:, 3], rin)
     assert host.iter == ref_iter(n1 + n2)
     host.close()
 
