@@ -292,7 +292,7 @@ int prepare_tma(mrlbm_handle* h, int cfg) {
 
 int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     const int tc = h->tile_cfg;
-    const bool tma = tc >= TMA_CFG0;
+    const bool tma = is_tma_cfg(tc);
     if (tma) {
         int prc = prepare_tma(h, tc);
         if (prc != MRLBM_OK) return prc;
@@ -722,7 +722,7 @@ int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32
     if (h->precision == MRLBM_FP64) { fill_common(h, p64); nc.p64 = &p64; }
     else { fill_common(h, p32); nc.p32 = &p32; }
     if (d_f0) nc.conflicts = slot_conflicts(h);
-    nc.tile_cfg = h->tile_cfg < TMA_CFG0 ? h->tile_cfg : 1;   // TMA shapes need handle-owned counters
+    nc.tile_cfg = is_tma_cfg(h->tile_cfg) ? 1 : h->tile_cfg;   // TMA shapes need handle-owned counters
     nc.iter = h->iter;
     nc.cur = h->cur;
     nc.launches = h->launches;

@@ -29,7 +29,7 @@ MRLBM_HD constexpr int mirror_y(int k) {
 // (they keep their initial value, 2d_mrlbm.f90:509-517); kernels never write them.
 struct Layout {
     int nx, ny;
-    int pitch;        // elements per row (>= nx + 2 + off)
+    int pitch;        // elements per row (>= off + nx + 4: ghost column plus 128-bit read slack)
     int off;          // element offset of column 0
     int64_t plane;    // elements per direction plane = pitch * (ny + 2)
     MRLBM_HD int64_t at(int i, int j, int k) const { return (int64_t)k * plane + (int64_t)j * pitch + i + off; }
@@ -41,7 +41,7 @@ inline Layout make_layout(int nx, int ny, int align_elems) {
     L.nx = nx;
     L.ny = ny;
     L.off = align_elems - 1;                                   // column 1 at index align_elems
-    int need = L.off + nx + 2;
+    int need = L.off + nx + 4;                                 // 16-byte reads starting at i <= nx stay in the row
     L.pitch = ((need + align_elems - 1) / align_elems) * align_elems;
     L.plane = (int64_t)L.pitch * (ny + 2);
     return L;

@@ -1,9 +1,11 @@
 // step_common.cuh -- launch skeleton shared by the FP64 and FP32 fused steps: pull-stream
-// gather, coalesced store, tile mapping, boundary blocks and the per-step force reduction.
-// The arithmetic of a node lives in a "physics" policy (step_fp64.cuh, step_fp32.cuh) with
-//   static void bulk_node(const P&, int i, int j);
-//   static void boundary_node(const P&, int l, double& Fx, double& Fy);
-//   static double inlet_rho(const P&, int j);   // post-closure density of node (1,j)
+// gather, coalesced store, tile mapping, boundary and edge blocks and the per-step force
+// reduction.  The arithmetic of a node lives in a "physics" policy (step_fp64.cuh,
+// step_fp32.cuh) with
+//   static void compute(const P&, int i, int j, int cls, const T f[Q], T fo[Q]);  // bulk node
+//   static void finish(const P&, int i, int j, int cls, const T f[Q]);            // compute + store
+//   static double edge_bulk_node(const P&, int i, int j, int cls);  // edge node; returns rho
+//   static void stencil_node(...), boundary_close(...);               // curved-wall nodes
 #pragma once
 #include <cuda_runtime.h>
 #include "step_params.h"
@@ -79,12 +81,58 @@ struct BTab {
     __device__ __forceinline__ int gi(int field, int li) const { return i[field * n + li]; }
 };
 
+// The last boundary or edge block to finish sums the per-node forces and the inlet column in
+// index order, as the reference's sum() does (2d_mrlbm.f90:359, 488-489): the result does not
+// depend on the launch shape and equals the reference's sums bit for bit.
+template <class Phys>
+__device__ __forceinline__ void aux_tail(const typename Phys::P& p) {
+    if (!p.do_stats) return;
+    __shared__ unsigned ticket;
+    __shared__ double sm[3];
+    const int tid = threadIdx.x;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) ticket = atomicAdd(p.counter, 1u);
+    __syncthreads();
+    if (ticket != (unsigned)(p.nbblk + p.neblk - 1)) return;
+    __threadfence();
+    // Three sequential sums (Fx over nodes, Fy over nodes, rho over the inlet column), one per
+    // warp: the warp loads up to 512 terms at once and every lane accumulates them in index
+    // order from shuffles, so only the adds are serial.
+    const int w = tid >> 5, lane = tid & 31;
+    if (w < 3) {
+        const int n = w < 2 ? p.nb : p.L.ny;
+        const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
+        double acc = 0.0;
+        constexpr int R = 16;
+        for (int q0 = 0; q0 < n; q0 += 32 * R) {
+            double x[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int q = q0 + r * 32 + lane;
+                x[r] = q < n ? __ldcg(v + q) : 0.0;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int m = min(32, n - (q0 + r * 32));
+#pragma unroll 8
+                for (int q = 0; q < m; ++q) acc = acc + __shfl_sync(0xffffffffu, x[r], q);
+            }
+        }
+        if (lane == 0) sm[w] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = sm[0]; p.rec[2] = sm[1]; p.rec[3] = sm[2]; }
+        *p.counter = 0u;
+    }
+}
+
 template <class Phys>
 __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
     using T = typename Phys::T;
     __shared__ T sg[G_STAGED * BNODES];
     __shared__ int sgi[I_NFIELDS * BNODES];
-    __shared__ double sm[3 * 32];
     const int nthr = blockDim.x, tid = threadIdx.x;
     const int bn = nthr / BLANES;
     const int l0 = blockIdx.x * bn;
@@ -136,34 +184,47 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
         Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
         if (p.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
     }
-    if (!p.do_stats) return;
-    // rho(1,j) after the closures, for the inlet running mean (2d_mrlbm.f90:359)
-    for (int j = 1 + blockIdx.x * nthr + tid; j <= p.L.ny; j += p.nbblk * nthr)
-        p.partials[2 * p.nb + j - 1] = Phys::inlet_rho(p, j);
-    // The last block to arrive sums the per-node forces and the inlet column in index order,
-    // as the reference's sum() does (2d_mrlbm.f90:359, 488-489): the result does not depend on
-    // the launch shape and equals the reference's sums bit for bit.
-    __shared__ unsigned ticket;
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) ticket = atomicAdd(p.counter, 1u);
-    __syncthreads();
-    if (ticket != (unsigned)(p.nbblk - 1)) return;
-    __threadfence();
-    const int w = tid >> 5;
-    if ((tid & 31) == 0 && w < 3) {
-        const int n = w < 2 ? p.nb : p.L.ny;
-        const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
-        double acc = 0.0;
-        for (int q = 0; q < n; ++q) acc = acc + __ldcg(v + q);
-        sm[w] = acc;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = sm[0]; p.rec[2] = sm[1]; p.rec[3] = sm[2]; }
-        *p.counter = 0u;
-    }
+    aux_tail<Phys>(p);
 }
+
+// Edge blocks: one thread per domain-edge node (rows 1 and ny, then columns 1 and nx without
+// the corners), so the edge closures (outlet neighbour gather, inlet/outlet/wall closures,
+// 2d_mrlbm.f90:249-272, 313-351) run side by side instead of serially inside bulk tiles.  The
+// thread of node (1,j) also records rho(1,j) after the closures for the inlet running mean
+// (2d_mrlbm.f90:359).
+template <class Phys>
+__device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb) {
+    const int nx = p.L.nx, ny = p.L.ny;
+    const int e = eb * (int)blockDim.x + (int)threadIdx.x;
+    if (e < 2 * nx + 2 * (ny - 2)) {
+        int i, j;
+        if (e < nx) { i = e + 1; j = 1; }
+        else if (e < 2 * nx) { i = e - nx + 1; j = ny; }
+        else if (e < 2 * nx + ny - 2) { i = 1; j = e - 2 * nx + 2; }
+        else { i = nx; j = e - 2 * nx - (ny - 2) + 2; }
+        const double rho = Phys::edge_bulk_node(p, i, j, CLS_FLUID);
+        if (p.do_stats && i == 1) p.partials[2 * p.nb + j - 1] = rho;
+    }
+    aux_tail<Phys>(p);
+}
+
+// Boundary and edge blocks sit at the start of the grid.  True when this block is one of them
+// (and has done its work); bulk tile t is then blockIdx.x - nbblk - neblk.
+template <class Phys>
+__device__ __forceinline__ bool run_aux_block(const typename Phys::P& p) {
+    const int b = (int)blockIdx.x;
+    if (b < p.nbblk) {
+        boundary_block<Phys>(p);
+        return true;
+    }
+    if (b < p.nbblk + p.neblk) {
+        edge_block<Phys>(p, b - p.nbblk);
+        return true;
+    }
+    return false;
+}
+
+inline int edge_blocks(int nx, int ny, int nthr) { return (2 * nx + 2 * (ny - 2) + nthr - 1) / nthr; }
 
 // Interior populations (no wraps, no ghosts): the branch-free half of `gather`.
 template <class T>
@@ -174,18 +235,15 @@ __device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, i
     for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
 }
 
-// One time step.  Blocks [0, nbblk) are boundary blocks; the rest are bulk tiles of
+// One time step.  Blocks [0, nbblk) are boundary blocks, the next neblk edge blocks; the rest are bulk tiles of
 // BX x (BY*NJ) nodes, one thread per column and NJ rows.  A thread first issues the loads of
 // all its interior rows, then finishes them (collide and store) one by one, so up to 9*NJ
-// loads per thread are in flight; edge rows and columns take the out-of-line edge path.
+// loads per thread are in flight.
 template <class Phys, int BX, int BY, int NJ, int MINB>
 __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
-    if ((int)blockIdx.x < p.nbblk) {
-        boundary_block<Phys>(p);
-        return;
-    }
-    const int t = blockIdx.x - p.nbblk;
+    if (run_aux_block<Phys>(p)) return;
+    const int t = blockIdx.x - p.nbblk - p.neblk;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
     const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
     const int i = 1 + tx * BX + lx;
@@ -209,9 +267,127 @@ __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_consta
 #pragma unroll
     for (int r = 0; r < NJ; ++r) {
         const int j = 1 + ty * BY * NJ + r * BY + ly;
-        if ((interior >> r) & 1u) Phys::finish(p, i, j, cls[r], f[r]);
-        else if (j <= ny && cls[r] < 0) Phys::edge_bulk_node(p, i, j, cls[r]);
+        if ((interior >> r) & 1u) Phys::finish(p, i, j, cls[r], f[r]);    // edge nodes: edge blocks
     }
+}
+
+// ---- 128-bit vector bulk path -------------------------------------------------------------
+// Each lane owns VW consecutive nodes of a row (VW = 16 bytes / element: four FP32 or two FP64
+// nodes) and reads every direction plane with one aligned 16-byte load per plane.  A pull
+// source one column left (planes with e_kx = +1) or right (e_kx = -1) of the lane's group comes
+// from the neighbouring lane by a warp shuffle; the warp's two outermost lanes fetch that
+// column with one scalar load.  A group whose nodes are all interior bulk nodes is written
+// back with one 16-byte store per plane; groups touching an edge or the cylinder box fall back
+// to per-node handling (edge nodes belong to the edge blocks, wall nodes to the boundary
+// blocks).  Columns read: i0-1 .. i0+VW of rows j-1 .. j+1, which the layout's row slack
+// (pitch >= off + nx + 4) keeps inside the row for every group with i0 <= nx.
+template <class T> struct Vec16;
+template <> struct Vec16<float> {
+    static constexpr int N = 4;
+    static __device__ __forceinline__ void load(const float* a, float (&v)[4]) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(a));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+    static __device__ __forceinline__ void store(float* a, const float (&v)[4]) {
+        *reinterpret_cast<float4*>(a) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+template <> struct Vec16<double> {
+    static constexpr int N = 2;
+    static __device__ __forceinline__ void load(const double* a, double (&v)[2]) {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(a));
+        v[0] = t.x; v[1] = t.y;
+    }
+    static __device__ __forceinline__ void store(double* a, const double (&v)[2]) {
+        *reinterpret_cast<double2*>(a) = make_double2(v[0], v[1]);
+    }
+};
+
+template <class Phys, int WARPS, int NJ, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
+    using T = typename Phys::T;
+    using VT = Vec16<T>;
+    constexpr int VW = VT::N;
+    if (run_aux_block<Phys>(p)) return;
+    const int t = blockIdx.x - p.nbblk - p.neblk;
+    const int tx = t % p.tiles_x, ty = t / p.tiles_x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nx = p.L.nx, ny = p.L.ny;
+    const int i0 = 1 + (tx * 32 + lane) * VW;
+    const bool act = i0 <= nx;
+    const int pitch = p.L.pitch, plane = (int)p.L.plane;
+    // cylinder-box overlap of this lane's columns (rows checked per row)
+    const bool box_cols = (i0 + VW - 1 >= p.box_x0) && (i0 < p.box_x0 + p.box_w);
+#pragma unroll 1
+    for (int r = 0; r < NJ; ++r) {
+        const int j = 1 + (ty * WARPS + warp) * NJ + r;
+        if (j > ny) break;                                    // uniform across the warp
+        T v[Q][VW];
+        T side[Q];                                            // column i0-1 (e_kx=+1) or i0+VW (e_kx=-1)
+        const int rowbase = j * pitch + i0 + p.L.off;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const T* a = p.src + (rowbase + k * plane - ey(k) * pitch);
+            if (act) VT::load(a, v[k]);
+            else {
+#pragma unroll
+                for (int n = 0; n < VW; ++n) v[k][n] = T(0);
+            }
+            if (ex(k) > 0) {
+                side[k] = __shfl_up_sync(0xffffffffu, v[k][VW - 1], 1);
+                if (lane == 0 && act) side[k] = __ldg(a - 1);
+            } else if (ex(k) < 0) {
+                side[k] = __shfl_down_sync(0xffffffffu, v[k][0], 1);
+                if (lane == 31 && i0 + VW <= nx) side[k] = __ldg(a + VW);
+            }
+        }
+        if (!act) continue;
+        const bool row_int = j > 1 && j < ny;
+        const bool in_box_row = box_cols && (unsigned)(j - p.box_y0) < (unsigned)p.box_h;
+        const bool all_int = row_int && i0 > 1 && i0 + VW - 1 < nx && !in_box_row;
+        T out[Q][VW];
+#pragma unroll
+        for (int n = 0; n < VW; ++n) {
+            const int i = i0 + n;
+            T f[Q];
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                if (ex(k) == 0) f[k] = v[k][n];
+                else if (ex(k) > 0) f[k] = n == 0 ? side[k] : v[k][n - 1];
+                else f[k] = n == VW - 1 ? side[k] : v[k][n + 1];
+            }
+            if (all_int) {
+                T fo[Q];
+                Phys::compute(p, i, j, CLS_FLUID, f, fo);
+#pragma unroll
+                for (int k = 0; k < Q; ++k) out[k][n] = fo[k];
+            } else if (row_int && i > 1 && i < nx) {          // edge nodes: edge blocks
+                const int cls = in_box_row ? node_class(p, i, j) : CLS_FLUID;
+                if (cls < 0) Phys::finish(p, i, j, cls, f);   // cls >= 0: curved-wall node
+            }
+        }
+        if (all_int) {
+            T* d = p.dst + rowbase;
+#pragma unroll
+            for (int k = 0; k < Q; ++k) VT::store(d + k * plane, out[k]);
+        }
+    }
+}
+
+template <class Phys, int WARPS, int NJ, int MINB>
+int launch_step_vec(typename Phys::P p, cudaStream_t s) {
+    using T = typename Phys::T;
+    constexpr int VW = Vec16<T>::N;
+    const int nthr = WARPS * 32;
+    static_assert(WARPS * 32 % BLANES == 0 && WARPS * 32 / BLANES <= BNODES, "boundary block size");
+    const int bn = nthr / BLANES;
+    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
+    p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
+    p.tiles_x = (p.L.nx + 32 * VW - 1) / (32 * VW);
+    const int tiles_y = (p.L.ny + WARPS * NJ - 1) / (WARPS * NJ);
+    const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
+    step_kernel_vec<Phys, WARPS, NJ, MINB><<<(unsigned)nblocks, nthr, 0, s>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 template <class Phys, int BX, int BY, int NJ, int MINB>
@@ -220,9 +396,10 @@ int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     static_assert(BX * BY % BLANES == 0 && BX * BY / BLANES <= BNODES, "boundary block size");
     const int bn = nthr / BLANES;
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
+    p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
-    const long long nblocks = (long long)p.nbblk + (long long)p.tiles_x * tiles_y;
+    const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
     step_kernel<Phys, BX, BY, NJ, MINB><<<(unsigned)nblocks, nthr, 0, s>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -17,6 +17,10 @@ int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int
     case id: return launch_step_tma<Ph, bx, by, st>(p, s, workers);
         MRLBM_TMA_LIST(MRLBM_TMA_CASE)
 #undef MRLBM_TMA_CASE
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return launch_step_vec<Ph, w, nj, mb>(p, s);
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
     default: return -1;
     }
 }

@@ -260,7 +260,7 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<float>& tb, i
 }
 
 // Edge nodes: own gather, Dirichlet values and closures (out of line, see the FP64 step).
-__device__ __noinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
+__device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
     float g[Q];
     gather(p, i, j, g);
     Mac m = moments(p, g);
@@ -271,27 +271,35 @@ __device__ __noinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
     float go[Q];
     collide(p, m, go);
     store(p, i, j, go);
+    return 1.0 + (double)m.drho;
 }
 
 // Interior fluid or solid node: populations already gathered.
-__device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const float g[Q]) {
+__device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const float g[Q], float go[Q]) {
     Mac m = moments(p, g);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    float go[Q];
     collide(p, m, go);
+}
+
+__device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const float g[Q]) {
+    float go[Q];
+    compute(p, i, j, cls, g, go);
     store(p, i, j, go);
 }
 
 struct Physics {
     using P = StepParams<float>;
     using T = float;
+    static __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const T f[Q], T fo[Q]) {
+        fp32::compute(p, i, j, cls, f, fo);
+    }
     static __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const T g[Q]) {
         fp32::finish(p, i, j, cls, g);
     }
-    static __device__ __forceinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
-        fp32::edge_bulk_node(p, i, j, cls);
+    static __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
+        return fp32::edge_bulk_node(p, i, j, cls);
     }
     static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
                                                         T& mx, T& my) {
@@ -301,13 +309,6 @@ struct Physics {
                                                           T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
                                                           double& Fy) {
         fp32::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
-    }
-    static __device__ __noinline__ double inlet_rho(const P& p, int j) {
-        float g[Q];
-        gather(p, 1, j, g);
-        Mac m = moments(p, g);
-        edge_node(p, 1, j, g, m);                // (1,j) is always an edge node
-        return 1.0 + (double)m.drho;
     }
 };
 

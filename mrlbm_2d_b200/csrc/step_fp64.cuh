@@ -387,7 +387,7 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
 
 // Edge nodes (first/last row or column): own gather, Dirichlet values and closures.  Out
 // of line so the interior path keeps its populations in registers.
-__device__ __noinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
+__device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
     double f[Q];
     gather(p, i, j, f);
     Mac m = moments(f, p.hm, p.hp);
@@ -398,28 +398,36 @@ __device__ __noinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
+    return m.rho;
 }
 
 // Bulk node (fluid or solid).
 // Interior fluid or solid node: populations already gathered.
-__device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const double f[Q]) {
+__device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const double f[Q], double fo[Q]) {
     Mac m = moments(f, p.hm, p.hp);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    double fo[Q];
     collide(p, m, fo);
+}
+
+__device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const double f[Q]) {
+    double fo[Q];
+    compute(p, i, j, cls, f, fo);
     store(p, i, j, fo);
 }
 
 struct Physics {
     using P = StepParams<double>;
     using T = double;
+    static __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const T f[Q], T fo[Q]) {
+        fp64::compute(p, i, j, cls, f, fo);
+    }
     static __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const T f[Q]) {
         fp64::finish(p, i, j, cls, f);
     }
-    static __device__ __forceinline__ void edge_bulk_node(const P& p, int i, int j, int cls) {
-        fp64::edge_bulk_node(p, i, j, cls);
+    static __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
+        return fp64::edge_bulk_node(p, i, j, cls);
     }
     static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
                                                         T& mx, T& my) {
@@ -429,11 +437,6 @@ struct Physics {
                                                           T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
                                                           double& Fy) {
         fp64::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
-    }
-    static __device__ __noinline__ double inlet_rho(const P& p, int j) {
-        double f[Q];
-        gather(p, 1, j, f);
-        return node_macro(p, 1, j, f).rho;
     }
 };
 

@@ -59,6 +59,7 @@ struct alignas(64) StepParams {
     int do_stats;                 // stats step: forces + inlet density sum
     // curved wall
     int nb, nbblk;                // boundary nodes, boundary blocks at the start of the grid
+    int neblk;                    // edge blocks (one thread per domain-edge node) after them
     const int* __restrict__ bint; // IntField table [I_NFIELDS * nb]
     const T* __restrict__ bgeo;   // GeoField table [G_NFIELDS * nb]
     int closure, vel_interp, mom_interp;
@@ -110,10 +111,23 @@ struct TmaCfg { int bx, by, stages; };
     X(15, 224, 4, 3)
 constexpr int N_TMA_CFGS = 6;
 constexpr int TMA_CFG0 = N_TILE_CFGS;
-constexpr int N_ALL_CFGS = N_TILE_CFGS + N_TMA_CFGS;
 #define MRLBM_TMA_ENTRY(id, bx, by, st) {bx, by, st},
 constexpr TmaCfg TMA_CFGS[N_TMA_CFGS] = {MRLBM_TMA_LIST(MRLBM_TMA_ENTRY)};
 #undef MRLBM_TMA_ENTRY
+
+// 128-bit vector shapes of step_kernel_vec (WARPS warps per block, each lane 16 bytes of a
+// row; NJ rows per warp; MINB resident blocks per SM).
+#define MRLBM_VEC_LIST(X) \
+    X(16, 8, 1, 2)        \
+    X(17, 8, 2, 2)        \
+    X(18, 4, 2, 4)        \
+    X(19, 8, 1, 1)        \
+    X(20, 4, 1, 4)        \
+    X(21, 2, 4, 8)
+constexpr int N_VEC_CFGS = 6;
+constexpr int VEC_CFG0 = TMA_CFG0 + N_TMA_CFGS;
+constexpr int N_ALL_CFGS = VEC_CFG0 + N_VEC_CFGS;
+inline bool is_tma_cfg(int c) { return c >= TMA_CFG0 && c < VEC_CFG0; }
 
 // Host-side launch entry points (step_f64.cu / step_f32.cu).  `workers` is the persistent
 // CTA count for TMA shapes (ignored otherwise).  Return 0, -1 on a launch error, -2 when the

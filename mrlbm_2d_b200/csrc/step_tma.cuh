@@ -9,7 +9,7 @@
 // which holds exactly the pull-stream sources of plane k for every node of the tile.  The
 // copies complete on the stage's mbarrier (expect_tx); threads wait on it, read their nine
 // populations from shared memory, collide and store straight to global memory.  Edge and
-// curved-wall nodes take the same paths as in step_kernel.
+// curved-wall nodes belong to the edge and boundary blocks, as in step_kernel.
 //
 // Every mbarrier wait is bounded: after TMA_SPIN_LIMIT polls the CTA raises errflag bit 4,
 // drains its outstanding copies (again bounded) and returns.
@@ -139,10 +139,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
             if (i > nx || j > ny) continue;
             const int cls = node_class(p, i, j);
             if (cls >= 0) continue;                           // curved-wall node
-            if (i == 1 || i == nx || j == 1 || j == ny) {
-                Phys::edge_bulk_node(p, i, j, cls);
-                continue;
-            }
+            if (i == 1 || i == nx || j == 1 || j == ny) continue;   // edge blocks
             T f[Q];
 #pragma unroll
             for (int k = 0; k < Q; ++k)
@@ -161,10 +158,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
 
 template <class Phys, int BX, int BY, int STAGES>
 __global__ void __launch_bounds__(BX, 1) step_kernel_tma(const __grid_constant__ typename Phys::P p) {
-    if ((int)blockIdx.x < p.nbblk) {
-        boundary_block<Phys>(p);
-        return;
-    }
+    if (run_aux_block<Phys>(p)) return;
     tma_bulk_worker<Phys, BX, BY, STAGES>(p);
 }
 
@@ -176,6 +170,7 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
     const int nthr = BX;
     const int bn = nthr / BLANES;
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
+    p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int smem = STAGES * G::STAGE_BYTES + 128;
     if (smem > 200 * 1024) return -2;                        // shape too large for this precision
@@ -188,7 +183,7 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
             return -1;
         if (dev < 64) attr_set |= 1ull << dev;
     }
-    step_kernel_tma<Phys, BX, BY, STAGES><<<(unsigned)(p.nbblk + workers), nthr, smem, s>>>(p);
+    step_kernel_tma<Phys, BX, BY, STAGES><<<(unsigned)(p.nbblk + p.neblk + workers), nthr, smem, s>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
