@@ -71,6 +71,7 @@ __device__ __forceinline__ int node_class(const StepParams<T>& p, int i, int j) 
 constexpr int BNODES = 32;        // at most (256-thread blocks); blockDim.x / BLANES in general
 constexpr int BLANES = 8;
 constexpr int G_STAGED = G_SCC;   // GeoFields 0 .. G_SCC-1 live in shared memory
+constexpr int AUX_CHUNK = 256;    // terms per warp and round in the in-order force sums
 
 template <class T>
 struct BTab {
@@ -85,7 +86,7 @@ struct BTab {
 // index order, as the reference's sum() does (2d_mrlbm.f90:359, 488-489): the result does not
 // depend on the launch shape and equals the reference's sums bit for bit.
 template <class Phys>
-__device__ __forceinline__ void aux_tail(const typename Phys::P& p) {
+__device__ __forceinline__ void aux_tail(const typename Phys::P& p, unsigned char* smem) {
     if (!p.do_stats) return;
     __shared__ unsigned ticket;
     __shared__ double sm[3];
@@ -97,27 +98,27 @@ __device__ __forceinline__ void aux_tail(const typename Phys::P& p) {
     if (ticket != (unsigned)(p.nbblk + p.neblk - 1)) return;
     __threadfence();
     // Three sequential sums (Fx over nodes, Fy over nodes, rho over the inlet column), one per
-    // warp: the warp loads up to 512 terms at once and every lane accumulates them in index
-    // order from shuffles, so only the adds are serial.
+    // warp: the warp stages AUX_CHUNK terms at a time in shared memory with parallel loads and
+    // its lane 0 adds them in index order, so only the adds are serial.
     const int w = tid >> 5, lane = tid & 31;
     if (w < 3) {
         const int n = w < 2 ? p.nb : p.L.ny;
         const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
+        double* st = reinterpret_cast<double*>(smem) + w * AUX_CHUNK;
         double acc = 0.0;
-        constexpr int R = 16;
-        for (int q0 = 0; q0 < n; q0 += 32 * R) {
-            double x[R];
+        for (int q0 = 0; q0 < n; q0 += AUX_CHUNK) {
+            const int m = min(AUX_CHUNK, n - q0);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int q = q0 + r * 32 + lane;
-                x[r] = q < n ? __ldcg(v + q) : 0.0;
+            for (int r = 0; r < AUX_CHUNK / 32; ++r) {
+                const int q = r * 32 + lane;
+                if (q < m) st[q] = __ldcg(v + q0 + q);
             }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int m = min(32, n - (q0 + r * 32));
-#pragma unroll 8
-                for (int q = 0; q < m; ++q) acc = acc + __shfl_sync(0xffffffffu, x[r], q);
+            __syncwarp();
+            if (lane == 0) {
+#pragma unroll 16
+                for (int q = 0; q < m; ++q) acc = acc + st[q];
             }
+            __syncwarp();
         }
         if (lane == 0) sm[w] = acc;
     }
@@ -129,10 +130,10 @@ __device__ __forceinline__ void aux_tail(const typename Phys::P& p) {
 }
 
 template <class Phys>
-__device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
+__device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsigned char* smem) {
     using T = typename Phys::T;
-    __shared__ T sg[G_STAGED * BNODES];
-    __shared__ int sgi[I_NFIELDS * BNODES];
+    T* sg = reinterpret_cast<T*>(smem);                               // G_STAGED * BNODES
+    int* sgi = reinterpret_cast<int*>(smem + sizeof(T) * G_STAGED * BNODES);   // I_NFIELDS * BNODES
     const int nthr = blockDim.x, tid = threadIdx.x;
     const int bn = nthr / BLANES;
     const int l0 = blockIdx.x * bn;
@@ -184,7 +185,7 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
         Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
         if (p.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
     }
-    aux_tail<Phys>(p);
+    aux_tail<Phys>(p, smem);
 }
 
 // Edge blocks: one thread per domain-edge node (rows 1 and ny, then columns 1 and nx without
@@ -193,7 +194,7 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p) {
 // thread of node (1,j) also records rho(1,j) after the closures for the inlet running mean
 // (2d_mrlbm.f90:359).
 template <class Phys>
-__device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb) {
+__device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, unsigned char* smem) {
     const int nx = p.L.nx, ny = p.L.ny;
     const int e = eb * (int)blockDim.x + (int)threadIdx.x;
     if (e < 2 * nx + 2 * (ny - 2)) {
@@ -205,20 +206,25 @@ __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb) {
         const double rho = Phys::edge_bulk_node(p, i, j, CLS_FLUID);
         if (p.do_stats && i == 1) p.partials[2 * p.nb + j - 1] = rho;
     }
-    aux_tail<Phys>(p);
+    aux_tail<Phys>(p, smem);
 }
 
 // Boundary and edge blocks sit at the start of the grid.  True when this block is one of them
 // (and has done its work); bulk tile t is then blockIdx.x - nbblk - neblk.
 template <class Phys>
 __device__ __forceinline__ bool run_aux_block(const typename Phys::P& p) {
+    using T = typename Phys::T;
+    constexpr int STAGING = (int)(sizeof(T) * G_STAGED + sizeof(int) * I_NFIELDS) * BNODES;
+    constexpr int TAIL = 3 * AUX_CHUNK * (int)sizeof(double);
+    // one buffer for the boundary tables and, afterwards, the tail's staged terms
+    __shared__ __align__(16) unsigned char smem[STAGING > TAIL ? STAGING : TAIL];
     const int b = (int)blockIdx.x;
     if (b < p.nbblk) {
-        boundary_block<Phys>(p);
+        boundary_block<Phys>(p, smem);
         return true;
     }
     if (b < p.nbblk + p.neblk) {
-        edge_block<Phys>(p, b - p.nbblk);
+        edge_block<Phys>(p, b - p.nbblk, smem);
         return true;
     }
     return false;
