@@ -38,7 +38,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", type=int, choices=[32, 64], default=None)
-    ap.add_argument("--case", choices=["mid", "large", "small"], default="mid")
+    ap.add_argument("--case", choices=["mid", "large", "small", "quarter"], default="mid")
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", type=int, default=None,
@@ -51,8 +51,8 @@ def parse():
 
 
 def make_case(name, seed):
-    from mrlbm_2d_b200.config import case_large, case_mid, case_small
-    c = {"mid": case_mid, "large": case_large, "small": case_small}[name]()
+    from mrlbm_2d_b200.config import case_large, case_mid, case_quarter, case_small
+    c = {"mid": case_mid, "large": case_large, "small": case_small, "quarter": case_quarter}[name]()
     return c.replace(seed=seed)
 
 

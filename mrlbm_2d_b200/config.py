@@ -101,6 +101,12 @@ def case_adjoint():
     return cylinder_case(512, 128, 32, 128.0, 64.5, 100.0, 0.05)
 
 
+def case_quarter():
+    """8192 x 2048, D = 128 at (1024.0, 1024.5), Re = 500, U = 0.04: a quarter of the large case
+    (2.4 GB of FP32 populations), for profiler captures."""
+    return cylinder_case(8192, 2048, 128, 1024.0, 1024.5, 500.0, 0.04)
+
+
 def case_large():
     """16384 x 4096, D = 256 at (2048.0, 2048.5), Re = 1000, U = 0.04."""
     return cylinder_case(16384, 4096, 256, 2048.0, 2048.5, 1000.0, 0.04)
