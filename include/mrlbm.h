@@ -245,6 +245,19 @@ int mrlbm_get_tile_config(const mrlbm_handle* h, int32_t* cfg);
  * time per step in milliseconds. */
 int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, double* best_ms);
 
+/* Field statistics (no counterpart in the reference, whose 2d_statistics post-processes
+ * forces only): every step whose iteration lies in [begin_iter, end_iter] adds the
+ * post-closure u, v and p = rho cs2 (cs2 = 1/3, 2d_mrlbm.f90:153, 237) of every node to FP64
+ * running sums of x and x^2, fused into the step kernel (+96 bytes per node and step).  A call
+ * clears the sums and sets the window; iterations are those of mrlbm_get_iter. */
+int mrlbm_field_stats_window(mrlbm_handle* h, int32_t begin_iter, int32_t end_iter);
+
+/* Time-mean and fluctuation rms, sqrt(max(<x^2> - <x>^2, 0)), of u, v and p over the steps
+ * accumulated so far, each nx*ny in Fortran order; any pointer may be NULL.  n_samples
+ * receives the number of steps.  MRLBM_ESTATE before the first step in the window. */
+int mrlbm_field_stats_get(mrlbm_handle* h, double* mean_u, double* mean_v, double* mean_p, double* rms_u,
+                          double* rms_v, double* rms_p, int64_t* n_samples);
+
 /* Number of kernel launches issued by this handle so far (all kinds). */
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n);
 

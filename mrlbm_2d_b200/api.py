@@ -32,6 +32,7 @@ EXPORTED = [
     "mrlbm_get_iter", "mrlbm_get_macro", "mrlbm_get_forces", "mrlbm_get_launch_count",
     "mrlbm_force_statistics", "mrlbm_cp_statistics", "mrlbm_step_noalloc",
     "mrlbm_set_tile_config", "mrlbm_get_tile_config", "mrlbm_autotune",
+    "mrlbm_field_stats_window", "mrlbm_field_stats_get",
 ]
 
 
@@ -88,6 +89,8 @@ def load_library(path=None):
         "mrlbm_set_tile_config": [vp, i32],
         "mrlbm_get_tile_config": [vp, vp],
         "mrlbm_autotune": [vp, i32, vp, vp],
+        "mrlbm_field_stats_window": [vp, i32, i32],
+        "mrlbm_field_stats_get": [vp] * 8,
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -276,6 +279,21 @@ class Simulation:
         self._check(self._L.mrlbm_get_macro(self._h, *[_ptr(o) for o in outs]))
         names = ["rho", "ux", "uy", "mxx", "myy", "mxy"]
         return {n: o.reshape(self.ny, self.nx).T for n, o in zip(names, outs)}
+
+    def field_stats_window(self, begin_iter, end_iter):
+        """Accumulate FP64 mean/rms sums of u, v, p over steps begin_iter..end_iter (clears them)."""
+        self._check(self._L.mrlbm_field_stats_window(self._h, int(begin_iter), int(end_iter)))
+
+    def field_stats(self):
+        """dict of (nx, ny) arrays mean_u, mean_v, mean_p, rms_u, rms_v, rms_p, plus n (steps)."""
+        N = self.nx * self.ny
+        outs = [np.empty(N) for _ in range(6)]
+        n = ctypes.c_int64()
+        self._check(self._L.mrlbm_field_stats_get(self._h, *[_ptr(o) for o in outs], ctypes.byref(n)))
+        names = ["mean_u", "mean_v", "mean_p", "rms_u", "rms_v", "rms_p"]
+        d = {k: o.reshape(self.ny, self.nx).T for k, o in zip(names, outs)}
+        d["n"] = n.value
+        return d
 
     def forces(self, cap=1 << 22):
         """Drain the force history: (iter, F_drag_net, F_lift_net, sum(rho(1,:)))."""

@@ -53,6 +53,11 @@ struct mrlbm_handle {
     double* h_ring = nullptr;                 // pinned
     std::vector<double> hist;                 // drained records, REC_WORDS each
     int iter = 0;
+    // field statistics (mean/rms of u, v, p) over an iteration window
+    double* d_fstat = nullptr;                // 6 x N running sums
+    double* d_fstat_out = nullptr;            // 6 x N mean and rms
+    int32_t fstat_begin = 0, fstat_end = -1;
+    int64_t fstat_n = 0;
     int tile_cfg = 1;
     long long launches = 0;
     std::string err;
@@ -292,6 +297,7 @@ int prepare_tma(mrlbm_handle* h, int cfg) {
 
 int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     const int tc = h->tile_cfg;
+    const bool fstat = h->d_fstat && h->iter >= h->fstat_begin && h->iter <= h->fstat_end;
     const bool tma = is_tma_cfg(tc);
     if (tma) {
         int prc = prepare_tma(h, tc);
@@ -311,6 +317,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
         p.iter = h->iter;
         p.macro = macro ? h->d_macro : nullptr;
+        p.fstat = fstat ? h->d_fstat : nullptr;
         if (tma) {
             p.tmap = h->tmap[h->cur];
             p.tile_ctr = h->d_tile_ctr;
@@ -330,6 +337,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.rec = stats ? h->d_ring + (size_t)h->ring_n * REC_WORDS : nullptr;
         p.iter = h->iter;
         p.macro = macro ? h->d_macro : nullptr;
+        p.fstat = fstat ? h->d_fstat : nullptr;
         if (tma) {
             p.tmap = h->tmap[h->cur];
             p.tile_ctr = h->d_tile_ctr;
@@ -354,6 +362,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     h->cur ^= 1;
     h->ovr_live = false;
     if (stats) ++h->ring_n;
+    if (fstat) ++h->fstat_n;
     return MRLBM_OK;
 }
 
@@ -362,7 +371,7 @@ void free_all(mrlbm_handle* h) {
     cudaSetDevice(h->device);
     for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
                     (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, (void*)h->d_ovr, (void*)h->d_fstage,
-                    (void*)h->d_tile_ctr})
+                    (void*)h->d_tile_ctr, (void*)h->d_fstat, (void*)h->d_fstat_out})
         if (p) cudaFree(p);
     if (h->h_ring) cudaFreeHost(h->h_ring);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -662,6 +671,41 @@ int mrlbm_step(mrlbm_handle* h, int32_t nsteps, int32_t flags) {
 int mrlbm_get_iter(const mrlbm_handle* h, int32_t* iter) {
     if (!h || !iter) return MRLBM_EINVAL;
     *iter = h->iter;
+    return MRLBM_OK;
+}
+
+int mrlbm_field_stats_window(mrlbm_handle* h, int32_t begin_iter, int32_t end_iter) {
+    if (!h || begin_iter > end_iter) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    const size_t bytes = (size_t)6 * h->L.nx * h->L.ny * sizeof(double);
+    if (!h->d_fstat) {
+        CK(cudaMalloc((void**)&h->d_fstat, bytes));
+        CK(cudaMalloc((void**)&h->d_fstat_out, bytes));
+    }
+    CK(cudaMemsetAsync(h->d_fstat, 0, bytes, h->stream));
+    h->fstat_begin = begin_iter;
+    h->fstat_end = end_iter;
+    h->fstat_n = 0;
+    return MRLBM_OK;
+}
+
+int mrlbm_field_stats_get(mrlbm_handle* h, double* mean_u, double* mean_v, double* mean_p, double* rms_u,
+                          double* rms_v, double* rms_p, int64_t* n_samples) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    if (!h->d_fstat) return fail(h, MRLBM_ESTATE, "no field-statistics window (mrlbm_field_stats_window)");
+    if (n_samples) *n_samples = h->fstat_n;
+    if (h->fstat_n == 0) return fail(h, MRLBM_ESTATE, "no step inside the field-statistics window yet");
+    CK(cudaSetDevice(h->device));
+    const int64_t N = (int64_t)h->L.nx * h->L.ny;
+    CK(launch_field_stats_finalize(h->d_fstat, h->d_fstat_out, N, h->fstat_n, h->stream));
+    ++h->launches;
+    double* outs[6] = {mean_u, mean_v, mean_p, rms_u, rms_v, rms_p};
+    for (int q = 0; q < 6; ++q)
+        if (outs[q])
+            CK(cudaMemcpyAsync(outs[q], h->d_fstat_out + q * N, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return MRLBM_OK;
 }
 

@@ -1,5 +1,6 @@
 // state_io.cu -- device-side layout conversion for mrlbm_load_state / mrlbm_get_state /
 // mrlbm_step_noalloc: one bulk host<->device copy plus a kernel instead of a host loop.
+#include <algorithm>
 #include "state_io.h"
 
 namespace mrlbm {
@@ -81,6 +82,26 @@ cudaError_t launch_fill_overrides(int precision, const double* f0, OvrEntry* ovr
         fill_overrides<double><<<1, 64, 0, s>>>(f0, ovr, n, nx, ny, w[0], w[1], w[5], 0);
     else
         fill_overrides<float><<<1, 64, 0, s>>>(f0, ovr, n, nx, ny, w[0], w[1], w[5], 1);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void field_stats_finalize(const double* __restrict__ sums, double* __restrict__ out, int64_t N, double n) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double mean = __ddiv_rn(sums[c * N + q], n);
+            const double var = __dadd_rn(__ddiv_rn(sums[(3 + c) * N + q], n), -__dmul_rn(mean, mean));
+            out[c * N + q] = mean;
+            out[(3 + c) * N + q] = __dsqrt_rn(var > 0.0 ? var : 0.0);
+        }
+    }
+}
+}  // namespace
+
+cudaError_t launch_field_stats_finalize(const double* sums, double* out, int64_t N, int64_t n, cudaStream_t s) {
+    const int64_t blocks = std::min<int64_t>((N + 255) / 256, 148 * 16);
+    field_stats_finalize<<<(unsigned)blocks, 256, 0, s>>>(sums, out, N, (double)n);
     return cudaGetLastError();
 }
 

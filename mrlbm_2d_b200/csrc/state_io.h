@@ -18,4 +18,8 @@ cudaError_t launch_gather_state(int precision, const void* src, double* f, const
 cudaError_t launch_fill_overrides(int precision, const double* f0, OvrEntry* ovr, int n, int nx, int ny,
                                   const double* w, cudaStream_t s);
 
+// Running sums (6 x N: u, v, p, u^2, v^2, p^2) over n steps -> mean (3 x N) and rms of the
+// fluctuation sqrt(max(<x^2> - <x>^2, 0)) (3 x N).
+cudaError_t launch_field_stats_finalize(const double* sums, double* out, int64_t N, int64_t n, cudaStream_t s);
+
 }  // namespace mrlbm

@@ -54,6 +54,24 @@ __device__ __forceinline__ void store_macro(const StepParams<T>& p, int i, int j
     p.macro[5 * N + n] = mxy;
 }
 
+// Field statistics: this step's post-closure u, v and p = rho cs2 (cs2 = 1/3, 2d_mrlbm.f90:153,
+// 237) added to FP64 running sums of x and x^2.  Explicit round-to-nearest operations keep the
+// sums free of contraction in every build, so they equal a host loop adding the same fields.
+template <class T>
+__device__ __forceinline__ void accumulate_fields(const StepParams<T>& p, int i, int j, double rho, double ux,
+                                                  double uy) {
+    const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1);
+    const int64_t N = (int64_t)p.L.nx * p.L.ny;
+    const double pr = __dmul_rn(rho, 1.0 / 3.0);
+    double* a = p.fstat + n;
+    a[0] = __dadd_rn(a[0], ux);
+    a[N] = __dadd_rn(a[N], uy);
+    a[2 * N] = __dadd_rn(a[2 * N], pr);
+    a[3 * N] = __dadd_rn(a[3 * N], __dmul_rn(ux, ux));
+    a[4 * N] = __dadd_rn(a[4 * N], __dmul_rn(uy, uy));
+    a[5 * N] = __dadd_rn(a[5 * N], __dmul_rn(pr, pr));
+}
+
 // Node class inside the cylinder box: CLS_FLUID, CLS_SOLID or a boundary-node index.
 template <class T>
 __device__ __forceinline__ int node_class(const StepParams<T>& p, int i, int j) {

@@ -243,6 +243,7 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<float>& tb, i
     }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     float go[Q];
     collide(p, m, go);
     store(p, i, j, go);
@@ -268,6 +269,7 @@ __device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls)
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     float go[Q];
     collide(p, m, go);
     store(p, i, j, go);
@@ -280,6 +282,7 @@ __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     collide(p, m, go);
 }
 

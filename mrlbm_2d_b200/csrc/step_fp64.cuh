@@ -370,6 +370,7 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
     }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
@@ -395,6 +396,7 @@ __device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls)
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
@@ -408,6 +410,7 @@ __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     collide(p, m, fo);
 }
 

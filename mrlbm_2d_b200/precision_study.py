@@ -10,6 +10,8 @@ same seeded initial state, records the per-step drag and lift, and reports
     reference's first-two-maxima period is not thrown off by small ripples on the lift,
   * |dCd|/Cd, |dSt|, |dCl_rms|/Cl_rms of FP32 against FP64,
   * the relative L2 error of the final velocity field, max |du|/U,
+  * with --fields, the relative L2 and max errors of the FP64-accumulated mean and rms fields
+    of u, v and p over the statistics window,
 and the wall-clock MLUPS of each run.  One JSON line on stdout.
 """
 import argparse
@@ -24,8 +26,10 @@ from .config import case_adjoint, case_large, case_mid, case_small
 CASES = {"small": case_small, "mid": case_mid, "adjoint": case_adjoint, "large": case_large}
 
 
-def run(cfg, precision, steps, chunk=5000):
+def run(cfg, precision, steps, chunk=5000, fields_from=None):
     sim = api.Simulation(cfg, precision=precision)
+    if fields_from is not None:
+        sim.field_stats_window(fields_from, steps + 1)
     fd, fl = [], []
     t0 = time.perf_counter()
     done = 0
@@ -38,11 +42,12 @@ def run(cfg, precision, steps, chunk=5000):
         done += n
     mac = sim.macro()
     el = time.perf_counter() - t0
+    fields = sim.field_stats() if fields_from is not None else None
     st = sim.status()
     sim.close()
     if st != 0:
         raise RuntimeError(f"device error flag in fp{precision} run")
-    return np.concatenate(fd), np.concatenate(fl), mac, cfg.nx * cfg.ny * steps / el / 1e6
+    return np.concatenate(fd), np.concatenate(fl), mac, cfg.nx * cfg.ny * steps / el / 1e6, fields
 
 
 def spectral_strouhal(fl, D, U, rho_infty=1.0, pad=16):
@@ -68,6 +73,8 @@ def main(argv=None):
     ap.add_argument("--case", default="small", choices=sorted(CASES))
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--stats-from", type=int, default=None, help="first step of the statistics window")
+    ap.add_argument("--fields", action="store_true",
+                    help="also accumulate FP64 mean/rms fields of u, v, p over the statistics window")
     a = ap.parse_args(argv)
     cfg = CASES[a.case]()
     start = a.stats_from if a.stats_from is not None else a.steps // 2
@@ -76,7 +83,8 @@ def main(argv=None):
            "D": 2 * cfg.r_c, "U": cfg.uo, "Re": cfg.Re}
     res = {}
     for prec in (64, 32):
-        fd, fl, mac, mlups = run(cfg, prec, a.steps)
+        fd, fl, mac, mlups, fields = run(cfg, prec, a.steps, fields_from=start if a.fields else None)
+        res.setdefault("fields", {})[prec] = fields
         r = {"mlups_wall": mlups}
         try:
             s = api.force_statistics(fd, fl, cfg.r_c, cfg.uo, 1.0)
@@ -98,6 +106,13 @@ def main(argv=None):
     out["velocity_rel_l2"] = float(np.sqrt((du ** 2).sum() / (u64 ** 2).sum()))
     out["velocity_max_abs_over_U"] = float(du.max() / cfg.uo)
     out["drag_history_rel_l2"] = float(np.linalg.norm(fd32 - fd64) / np.linalg.norm(fd64))
+    if a.fields:
+        f32, f64 = res["fields"][32], res["fields"][64]
+        for k in ("mean_u", "mean_v", "mean_p", "rms_u", "rms_v", "rms_p"):
+            ref = f64[k] - (1.0 / 3.0 if k == "mean_p" else 0.0)   # p relative to rest pressure
+            out[f"{k}_rel_l2"] = float(np.linalg.norm(f32[k] - f64[k]) / max(np.linalg.norm(ref), 1e-300))
+            out[f"{k}_max_abs"] = float(np.abs(f32[k] - f64[k]).max())
+        out["field_samples"] = int(f64["n"])
     print(json.dumps(out), flush=True)
     return out
 

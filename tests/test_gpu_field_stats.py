@@ -1,0 +1,86 @@
+"""Field statistics (time-mean and rms of u, v, p accumulated in FP64 inside the step) against
+the oracle's per-step fields summed on the host in the same order: bit for bit in FP64."""
+import numpy as np
+import pytest
+
+from cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+
+def _host_stats(o, steps, begin, end):
+    su = sv = sp = suu = svv = spp = None
+    n = 0
+    for k in range(steps):
+        o.step(1)
+        it = 2 + k                       # fresh runs start at iteration 2 (restart_step = 1)
+        if not (begin <= it <= end):
+            continue
+        ux, uy = o.field("ux"), o.field("uy")
+        p = o.field("rho") * (1.0 / 3.0)
+        if su is None:
+            su, sv, sp = np.zeros_like(ux), np.zeros_like(ux), np.zeros_like(ux)
+            suu, svv, spp = np.zeros_like(ux), np.zeros_like(ux), np.zeros_like(ux)
+        su = su + ux
+        sv = sv + uy
+        sp = sp + p
+        suu = suu + ux * ux
+        svv = svv + uy * uy
+        spp = spp + p * p
+        n += 1
+    out = {}
+    for name, s, ss in (("u", su, suu), ("v", sv, svv), ("p", sp, spp)):
+        mean = s / n
+        var = ss / n - mean * mean
+        out["mean_" + name] = mean
+        out["rms_" + name] = np.sqrt(np.maximum(var, 0.0))
+    return out, n
+
+
+@pytest.mark.parametrize("name", ["freeslip_label15", "reference_default_bcs"])
+def test_fp64_field_stats_bit_exact(mrlbm, oracle_mod, name):
+    cfg = CASES[name]()
+    s = mrlbm.Simulation(cfg)
+    s.field_stats_window(5, 24)
+    o = oracle_mod.Oracle(cfg)
+    ref, n = _host_stats(o, 30, 5, 24)
+    s.step(30)
+    got = s.field_stats()
+    assert got["n"] == n == 20
+    for k, v in ref.items():
+        assert np.array_equal(got[k], v), k
+    s.close()
+
+
+def test_fp32_field_stats_track_fp64(mrlbm):
+    cfg = CASES["benchmark_small_400x100"]()
+    out = {}
+    for prec in (64, 32):
+        s = mrlbm.Simulation(cfg, precision=prec)
+        s.field_stats_window(101, 600)
+        s.step(600)
+        out[prec] = s.field_stats()
+        s.close()
+    assert out[32]["n"] == out[64]["n"] == 500
+    for k in ("mean_u", "mean_v", "rms_u", "rms_v"):
+        assert np.abs(out[32][k] - out[64][k]).max() / cfg.uo < 1e-4, k
+    assert np.abs(out[32]["mean_p"] - out[64]["mean_p"]).max() < 1e-6
+
+
+def test_field_stats_window_rules(mrlbm):
+    cfg = CASES["benchmark_small_400x100"]()
+    s = mrlbm.Simulation(cfg)
+    with pytest.raises(mrlbm.MrlbmError):
+        s.field_stats()                   # no window yet
+    with pytest.raises(mrlbm.MrlbmError):
+        s.field_stats_window(10, 5)
+    s.field_stats_window(100, 200)
+    s.step(10)
+    with pytest.raises(mrlbm.MrlbmError):
+        s.field_stats()                   # nothing inside the window yet
+    s.step(200)
+    assert s.field_stats()["n"] == 101
+    s.field_stats_window(1, 10 ** 9)      # a new window clears the sums
+    s.step(3)
+    assert s.field_stats()["n"] == 3
+    s.close()
