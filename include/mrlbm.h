@@ -258,6 +258,37 @@ int mrlbm_field_stats_window(mrlbm_handle* h, int32_t begin_iter, int32_t end_it
 int mrlbm_field_stats_get(mrlbm_handle* h, double* mean_u, double* mean_v, double* mean_p, double* rms_u,
                           double* rms_v, double* rms_p, int64_t* n_samples);
 
+/* ---- batched cases (no counterpart in the reference, which runs one case per process) ----
+ * Many independent cases of one precision on one device advance together: one kernel covers
+ * the work of every case, either as a persistent cooperative launch that loops over steps
+ * with a grid barrier (MRLBM_BATCH_PERSISTENT, steps_per_launch steps per launch) or as one
+ * launch per step captured once into a CUDA graph of steps_per_launch launches and replayed
+ * (MRLBM_BATCH_GRAPH).  Each case's results are bit-identical to stepping it alone.  The
+ * cases are ordinary handles owned by the batch (mrlbm_batch_case): read their forces,
+ * fields and state, load states, set inlet profiles and field-statistics windows with the
+ * single-case calls, but step them only through mrlbm_batch_step and do not destroy them. */
+typedef struct mrlbm_batch mrlbm_batch;
+#define MRLBM_BATCH_PERSISTENT 0
+#define MRLBM_BATCH_GRAPH      1
+
+int mrlbm_batch_create(const mrlbm_config* cfgs, int32_t ncases, int precision, int device, mrlbm_batch** out);
+int mrlbm_batch_destroy(mrlbm_batch* b);
+int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h);
+/* Advance every case by nsteps (flags: MRLBM_STEP_MACRO stores each case's fields on the last). */
+int mrlbm_batch_step(mrlbm_batch* b, int32_t nsteps, int32_t flags);
+/* tile_cfg: a 128-bit vector shape (16..21); schedule: MRLBM_BATCH_PERSISTENT or _GRAPH. */
+int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch);
+int mrlbm_batch_get_schedule(const mrlbm_batch* b, int32_t* tile_cfg, int32_t* schedule, int32_t* steps_per_launch);
+/* Time every vector shape under both schedules for trial_steps steps (states, counters and
+ * histories restored afterwards) and keep the fastest; returns its time per batch step. */
+int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_per_step);
+/* Sticky status: a grid-barrier timeout (MRLBM_EDEVICE_TIMEOUT) or the first case's error. */
+int mrlbm_batch_status(mrlbm_batch* b);
+int mrlbm_batch_last_error(const mrlbm_batch* b, char* buf, size_t len);
+int mrlbm_batch_launch_count(const mrlbm_batch* b, int64_t* n);
+/* The batch's own CUDA stream (all its cases' work is ordered on it), e.g. to time it with events. */
+int mrlbm_batch_get_stream(const mrlbm_batch* b, void** stream);
+
 /* Number of kernel launches issued by this handle so far (all kinds). */
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n);
 

@@ -33,7 +33,11 @@ EXPORTED = [
     "mrlbm_force_statistics", "mrlbm_cp_statistics", "mrlbm_step_noalloc",
     "mrlbm_set_tile_config", "mrlbm_get_tile_config", "mrlbm_autotune",
     "mrlbm_field_stats_window", "mrlbm_field_stats_get",
+    "mrlbm_batch_create", "mrlbm_batch_destroy", "mrlbm_batch_case", "mrlbm_batch_step",
+    "mrlbm_batch_set_schedule", "mrlbm_batch_get_schedule", "mrlbm_batch_autotune", "mrlbm_batch_status",
+    "mrlbm_batch_last_error", "mrlbm_batch_launch_count", "mrlbm_batch_get_stream",
 ]
+BATCH_PERSISTENT, BATCH_GRAPH = 0, 1
 
 
 class MrlbmError(RuntimeError):
@@ -91,6 +95,17 @@ def load_library(path=None):
         "mrlbm_autotune": [vp, i32, vp, vp],
         "mrlbm_field_stats_window": [vp, i32, i32],
         "mrlbm_field_stats_get": [vp] * 8,
+        "mrlbm_batch_create": [vp, i32, ctypes.c_int, ctypes.c_int, vp],
+        "mrlbm_batch_destroy": [vp],
+        "mrlbm_batch_case": [vp, i32, vp],
+        "mrlbm_batch_step": [vp, i32, i32],
+        "mrlbm_batch_set_schedule": [vp, i32, i32, i32],
+        "mrlbm_batch_get_schedule": [vp, vp, vp, vp],
+        "mrlbm_batch_autotune": [vp, i32, vp],
+        "mrlbm_batch_status": [vp],
+        "mrlbm_batch_last_error": [vp, ctypes.c_char_p, ctypes.c_size_t],
+        "mrlbm_batch_launch_count": [vp, vp],
+        "mrlbm_batch_get_stream": [vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -322,3 +337,94 @@ class Simulation:
         a, b, c = (np.empty(N, np.int32) for _ in range(3))
         self._check(self._L.mrlbm_get_node_classes(self._h, _ptr(a), _ptr(b), _ptr(c)))
         return {k: v.reshape(self.ny, self.nx).T for k, v in zip(["isfluid", "issolid", "isbound"], (a, b, c))}
+
+
+class _BorrowedSimulation(Simulation):
+    """A case owned by a Batch: the single-case calls work on it; closing does nothing."""
+
+    def __init__(self, lib, h, precision):
+        self._L = lib
+        self._h = h
+        self.precision = precision
+        info = GeometryInfo()
+        self._L.mrlbm_get_geometry_info(self._h, ctypes.byref(info))
+        self.info = info
+        self.nx, self.ny, self.nbct = info.nx, info.ny, info.nbct
+
+    def close(self):
+        self._h = ctypes.c_void_p()
+
+    def step(self, n=1, macro=False):
+        raise MrlbmError(1, "a batch case steps only through Batch.step")
+
+
+class Batch:
+    """Many independent cases of one precision advanced together by one kernel per step (or
+    one persistent launch per steps_per_launch steps); see mrlbm_batch_* in include/mrlbm.h."""
+
+    def __init__(self, cfgs, precision=FP32, device=0):
+        self._L = load_library()
+        arr = (Config * len(cfgs))(*cfgs)
+        self._b = ctypes.c_void_p()
+        rc = self._L.mrlbm_batch_create(arr, len(cfgs), int(precision), int(device), ctypes.byref(self._b))
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self._L.mrlbm_batch_last_error(None, buf, 1024)
+            raise MrlbmError(rc, buf.value.decode())
+        self.precision = precision
+        self.cases = []
+        for c in range(len(cfgs)):
+            h = ctypes.c_void_p()
+            self._check(self._L.mrlbm_batch_case(self._b, c, ctypes.byref(h)))
+            self.cases.append(_BorrowedSimulation(self._L, h, precision))
+
+    def _check(self, rc):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self._L.mrlbm_batch_last_error(self._b, buf, 1024)
+            raise MrlbmError(rc, buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            for c in self.cases:
+                c.close()
+            self._L.mrlbm_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1, macro=False):
+        self._check(self._L.mrlbm_batch_step(self._b, int(n), STEP_MACRO if macro else 0))
+
+    def set_schedule(self, tile_cfg, schedule, steps_per_launch):
+        self._check(self._L.mrlbm_batch_set_schedule(self._b, int(tile_cfg), int(schedule), int(steps_per_launch)))
+
+    @property
+    def schedule(self):
+        t, s, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._L.mrlbm_batch_get_schedule(self._b, ctypes.byref(t), ctypes.byref(s), ctypes.byref(n)))
+        return t.value, s.value, n.value
+
+    def autotune(self, trial_steps=50):
+        ms = ctypes.c_double()
+        self._check(self._L.mrlbm_batch_autotune(self._b, int(trial_steps), ctypes.byref(ms)))
+        return self.schedule, ms.value
+
+    def status(self):
+        return self._L.mrlbm_batch_status(self._b)
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        self._check(self._L.mrlbm_batch_launch_count(self._b, ctypes.byref(n)))
+        return n.value
+
+    @property
+    def stream(self):
+        """The batch's CUDA stream handle (an int), e.g. for torch.cuda.ExternalStream."""
+        p = ctypes.c_void_p()
+        self._check(self._L.mrlbm_batch_get_stream(self._b, ctypes.byref(p)))
+        return p.value or 0

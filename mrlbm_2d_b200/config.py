@@ -110,3 +110,18 @@ def case_quarter():
 def case_large():
     """16384 x 4096, D = 256 at (2048.0, 2048.5), Re = 1000, U = 0.04."""
     return cylinder_case(16384, 4096, 256, 2048.0, 2048.5, 1000.0, 0.04)
+
+
+def sweep_cases(n=64, seed=4242, U=0.05):
+    """A seeded sweep of independent cylinder cases: nx uniform in [256, 1024] in steps of 32,
+    ny = nx / 4, D = ny / 5 at (nx / 5, ny / 2 + 0.5), Re uniform in [40, 200], U = 0.05."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n):
+        nx = int(rng.integers(256 // 32, 1024 // 32 + 1)) * 32
+        ny = nx // 4
+        D = ny / 5.0
+        Re = float(rng.uniform(40.0, 200.0))
+        out.append(cylinder_case(nx, ny, D, nx / 5.0, ny / 2.0 + 0.5, Re, U, seed=seed * 1000 + c))
+    return out

@@ -14,6 +14,7 @@
 
 #include "../../include/mrlbm.h"
 #include "geometry.h"
+#include "batch_params.h"
 #include "noalloc.h"
 #include "state_io.h"
 #include "step_params.h"
@@ -860,6 +861,437 @@ int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, doub
 int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n) {
     if (!h || !n) return MRLBM_EINVAL;
     *n = h->launches;
+    return MRLBM_OK;
+}
+
+}  // extern "C"
+
+// ---- batched cases ----------------------------------------------------------------------
+
+struct mrlbm_batch {
+    std::vector<mrlbm_handle*> h;
+    int precision = MRLBM_FP64, device = 0;
+    cudaStream_t stream = nullptr;
+    int tile_cfg = VEC_CFG0 + 2;
+    int schedule = MRLBM_BATCH_PERSISTENT;
+    int steps_per_launch = 64;
+    int num_sms = 0;
+    int64_t launches = 0;
+    std::string err;
+    void* d_params = nullptr;          // ncases x StepParams<T>
+    BatchCase* d_cases = nullptr;
+    int* d_off = nullptr;              // aux_off[n + 1], tile_off[n + 1]
+    BatchBarrier* d_bar = nullptr;
+    unsigned char* h_stage[2] = {nullptr, nullptr};   // pinned upload staging, double-buffered
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    int stage_i = 0;
+    size_t stage_bytes = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_cfg = -1, graph_steps = 0, graph_macro = -1;
+};
+
+namespace {
+
+int bfail(mrlbm_batch* b, int code, const std::string& msg) {
+    b->err = msg;
+    return code;
+}
+
+#define BCK(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) return bfail(b, MRLBM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int stats_in(const mrlbm_config& c, int a, int z) {
+    if (!c.post_process) return 0;
+    const int lo = std::max(a, c.statsbegin), hi = std::min(z, c.statsend);
+    return hi >= lo ? hi - lo + 1 : 0;
+}
+
+// Work items of one step of case h for vector shape cfg.
+void batch_items(const mrlbm_handle* h, int cfg, int& aux, int& tiles, int& nbblk, int& neblk, int& tiles_x) {
+    const VecCfg v = VEC_CFGS[cfg - VEC_CFG0];
+    const int nthr = v.warps * 32, vw = 16 / h->elem;
+    const int bn = nthr / 8;
+    nbblk = h->geo.nb > 0 ? (h->geo.nb + bn - 1) / bn : 1;
+    neblk = (2 * h->L.nx + 2 * (h->L.ny - 2) + nthr - 1) / nthr;
+    tiles_x = (h->L.nx + 32 * vw - 1) / (32 * vw);
+    const int tiles_y = (h->L.ny + v.warps * v.nj - 1) / (v.warps * v.nj);
+    aux = nbblk + neblk;
+    tiles = tiles_x * tiles_y;
+}
+
+template <class T>
+void batch_fill(mrlbm_batch* b, unsigned char* stage, int want_macro) {
+    const int n = (int)b->h.size();
+    StepParams<T>* ps = reinterpret_cast<StepParams<T>*>(stage);
+    BatchCase* cs = reinterpret_cast<BatchCase*>(stage + n * sizeof(StepParams<T>));
+    int* off = reinterpret_cast<int*>(stage + n * (sizeof(StepParams<T>) + sizeof(BatchCase)));
+    int aux_acc = 0, tile_acc = 0;
+    for (int c = 0; c < n; ++c) {
+        mrlbm_handle* h = b->h[c];
+        StepParams<T> p{};
+        fill_common(h, p);
+        p.src = (const T*)h->buf[h->cur];
+        p.dst = (T*)h->buf[1 - h->cur];
+        p.u_in = h->has_uin ? (const T*)h->d_uin : nullptr;
+        p.ovr = h->ovr_live ? h->d_ovr : nullptr;
+        p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
+        int aux, tiles;
+        batch_items(h, b->tile_cfg, aux, tiles, p.nbblk, p.neblk, p.tiles_x);
+        ps[c] = p;
+        BatchCase bc{};
+        const mrlbm_config& k = h->cfg;
+        bc.iter0 = h->iter;
+        bc.cur0 = h->cur;
+        bc.ring_n0 = h->ring_n;
+        bc.ovr_live = h->ovr_live ? 1 : 0;
+        bc.post_process = k.post_process != 0;
+        bc.statsbegin = k.statsbegin;
+        bc.statsend = k.statsend;
+        bc.iplot = k.iplot;
+        bc.plot_cyl = (k.channel_with_cylinder || k.channel_with_square) ? 1 : 0;
+        bc.fs_begin = h->d_fstat ? h->fstat_begin : 1;
+        bc.fs_end = h->d_fstat ? h->fstat_end : 0;
+        bc.aux_items = aux;
+        bc.tiles = tiles;
+        bc.ring = h->d_ring;
+        bc.macro = want_macro ? h->d_macro : nullptr;
+        bc.fstat = h->d_fstat;
+        cs[c] = bc;
+        off[c] = aux_acc;
+        off[n + 1 + c] = tile_acc;
+        aux_acc += aux;
+        tile_acc += tiles;
+    }
+    off[n] = aux_acc;
+    off[2 * n + 1] = tile_acc;
+}
+
+size_t batch_param_bytes(const mrlbm_batch* b) {
+    const size_t n = b->h.size();
+    const size_t pb = b->precision == MRLBM_FP64 ? sizeof(StepParams<double>) : sizeof(StepParams<float>);
+    return n * (pb + sizeof(BatchCase)) + (2 * n + 2) * sizeof(int);
+}
+
+// One call of `steps` steps (at most RING_CAP stats records per case).
+int batch_call(mrlbm_batch* b, int steps, int want_macro) {
+    const int n = (int)b->h.size();
+    for (mrlbm_handle* h : b->h) {
+        if (h->ring_n + stats_in(h->cfg, h->iter + 1, h->iter + steps) > RING_CAP) {
+            int rc = drain_ring(h);
+            if (rc != MRLBM_OK) return bfail(b, rc, h->err);
+        }
+        if (want_macro && !h->d_macro)
+            BCK(cudaMalloc((void**)&h->d_macro, (size_t)6 * h->L.nx * h->L.ny * sizeof(double)));
+    }
+    // stage the per-call parameters in pinned memory and upload them
+    const int si = b->stage_i;
+    BCK(cudaEventSynchronize(b->staged[si]));
+    if (b->precision == MRLBM_FP64) batch_fill<double>(b, b->h_stage[si], want_macro);
+    else batch_fill<float>(b, b->h_stage[si], want_macro);
+    const size_t pb = (b->precision == MRLBM_FP64 ? sizeof(StepParams<double>) : sizeof(StepParams<float>)) * n;
+    const size_t cb = sizeof(BatchCase) * n;
+    BCK(cudaMemcpyAsync(b->d_params, b->h_stage[si], pb, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->d_cases, b->h_stage[si] + pb, cb, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->d_off, b->h_stage[si] + pb + cb, (2 * n + 2) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaEventRecord(b->staged[si], b->stream));
+    b->stage_i ^= 1;
+    const int* off = reinterpret_cast<const int*>(b->h_stage[si] + pb + cb);
+    const int items = off[n] + off[2 * n + 1];
+
+    BatchArgs<double> a64{};
+    BatchArgs<float> a32{};
+    auto setup = [&](auto& a, auto* params) {
+        a.params = params;
+        a.cases = b->d_cases;
+        a.aux_off = b->d_off;
+        a.tile_off = b->d_off + n + 1;
+        a.bar = b->d_bar;
+        a.ncases = n;
+        a.call_steps = steps;
+        a.want_macro = want_macro;
+    };
+    setup(a64, (const StepParams<double>*)b->d_params);
+    setup(a32, (const StepParams<float>*)b->d_params);
+    auto launch = [&](int nsteps, int step0, int grid, bool coop) {
+        a64.nsteps = a32.nsteps = nsteps;
+        a64.step0 = a32.step0 = step0;
+        return b->precision == MRLBM_FP64 ? launch_batch_f64(a64, b->tile_cfg, grid, coop, b->stream)
+                                          : launch_batch_f32(a32, b->tile_cfg, grid, coop, b->stream);
+    };
+    if (b->schedule == MRLBM_BATCH_PERSISTENT) {
+        const int per_sm = batch_blocks_per_sm(b->precision, b->tile_cfg);
+        if (per_sm <= 0) return bfail(b, MRLBM_EUNSUPPORTED, "batch shape does not fit");
+        const int grid = std::min(items, b->num_sms * per_sm);
+        if (launch(steps, 0, grid, steps > 1) != 0)
+            return bfail(b, MRLBM_ECUDA, std::string("batch launch: ") + cudaGetErrorString(cudaGetLastError()));
+        ++b->launches;
+    } else {
+        if (!b->graph || b->graph_cfg != b->tile_cfg || b->graph_steps != steps || b->graph_macro != want_macro) {
+            if (b->graph) cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+            BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = 0;
+            for (int k = 0; k < steps && rc == 0; ++k) rc = launch(1, k, items, false);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc != 0 || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return bfail(b, MRLBM_ECUDA, "capturing the batch step graph failed");
+            }
+            e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return bfail(b, MRLBM_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            b->graph_cfg = b->tile_cfg;
+            b->graph_steps = steps;
+            b->graph_macro = want_macro;
+        }
+        BCK(cudaGraphLaunch(b->graph, b->stream));
+        b->launches += steps;
+    }
+    for (mrlbm_handle* h : b->h) {
+        const int a0 = h->iter + 1, z = h->iter + steps;
+        h->ring_n += stats_in(h->cfg, a0, z);
+        if (h->d_fstat) {
+            const int lo = std::max(a0, h->fstat_begin), hi = std::min(z, h->fstat_end);
+            if (hi >= lo) h->fstat_n += hi - lo + 1;
+        }
+        h->iter = z;
+        h->cur ^= steps & 1;
+        h->ovr_live = false;
+    }
+    return MRLBM_OK;
+}
+
+void batch_free(mrlbm_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (mrlbm_handle* h : b->h) {
+        if (!h) continue;
+        h->stream = nullptr;
+        free_all(h);
+        delete h;
+    }
+    for (void* q : {(void*)b->d_params, (void*)b->d_cases, (void*)b->d_off, (void*)b->d_bar})
+        if (q) cudaFree(q);
+    for (int i = 0; i < 2; ++i) {
+        if (b->h_stage[i]) cudaFreeHost(b->h_stage[i]);
+        if (b->staged[i]) cudaEventDestroy(b->staged[i]);
+    }
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mrlbm_batch_create(const mrlbm_config* cfgs, int32_t ncases, int precision, int device, mrlbm_batch** out) {
+    if (!cfgs || !out || ncases <= 0 || device < 0) return MRLBM_EINVAL;
+    *out = nullptr;
+    mrlbm_batch* b = new mrlbm_batch();
+    b->precision = precision;
+    b->device = device;
+    auto bail = [&](int rc, const std::string& msg) {
+        g_create_error = msg;
+        batch_free(b);
+        delete b;
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(MRLBM_ENODEVICE, "cudaSetDevice failed");
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(MRLBM_ECUDA, "cudaStreamCreate failed");
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
+    for (int c = 0; c < ncases; ++c) {
+        mrlbm_handle* h = nullptr;
+        int rc = mrlbm_create(cfgs + c, precision, device, &h);
+        if (rc != MRLBM_OK) return bail(rc, "case " + std::to_string(c) + ": " + g_create_error);
+        b->h.push_back(h);
+        if (h->own_stream) {
+            cudaStreamSynchronize(h->own_stream);
+            cudaStreamDestroy(h->own_stream);
+            h->own_stream = nullptr;
+        }
+        h->stream = b->stream;
+    }
+    b->stage_bytes = batch_param_bytes(b);
+    bool ok = cudaMalloc(&b->d_params, b->stage_bytes) == cudaSuccess &&
+              cudaMalloc((void**)&b->d_cases, sizeof(BatchCase) * ncases) == cudaSuccess &&
+              cudaMalloc((void**)&b->d_off, sizeof(int) * (2 * ncases + 2)) == cudaSuccess &&
+              cudaMalloc((void**)&b->d_bar, sizeof(BatchBarrier)) == cudaSuccess &&
+              cudaMemsetAsync(b->d_bar, 0, sizeof(BatchBarrier), b->stream) == cudaSuccess;
+    for (int i = 0; ok && i < 2; ++i)
+        ok = cudaMallocHost((void**)&b->h_stage[i], b->stage_bytes) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventRecord(b->staged[i], b->stream) == cudaSuccess;
+    if (!ok || cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(MRLBM_ECUDA, "batch allocation failed");
+    *out = b;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_destroy(mrlbm_batch* b) {
+    if (!b) return MRLBM_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_free(b);
+    delete b;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h) {
+    if (!b || !h || c < 0 || c >= (int)b->h.size()) return MRLBM_EINVAL;
+    *h = b->h[c];
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch) {
+    if (!b || tile_cfg < VEC_CFG0 || tile_cfg >= N_ALL_CFGS || steps_per_launch < 1 || steps_per_launch > RING_CAP ||
+        (schedule != MRLBM_BATCH_PERSISTENT && schedule != MRLBM_BATCH_GRAPH))
+        return MRLBM_EINVAL;
+    b->tile_cfg = tile_cfg;
+    b->schedule = schedule;
+    b->steps_per_launch = steps_per_launch;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_get_schedule(const mrlbm_batch* b, int32_t* tile_cfg, int32_t* schedule, int32_t* steps_per_launch) {
+    if (!b) return MRLBM_EINVAL;
+    if (tile_cfg) *tile_cfg = b->tile_cfg;
+    if (schedule) *schedule = b->schedule;
+    if (steps_per_launch) *steps_per_launch = b->steps_per_launch;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_step(mrlbm_batch* b, int32_t nsteps, int32_t flags) {
+    if (!b || nsteps < 0) return MRLBM_EINVAL;
+    BCK(cudaSetDevice(b->device));
+    int done = 0;
+    while (done < nsteps) {
+        const int s = std::min(b->steps_per_launch, nsteps - done);
+        const int rc = batch_call(b, s, (flags & MRLBM_STEP_MACRO) && done + s == nsteps);
+        if (rc != MRLBM_OK) return rc;
+        done += s;
+    }
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_status(mrlbm_batch* b) {
+    if (!b) return MRLBM_EINVAL;
+    BCK(cudaSetDevice(b->device));
+    BatchBarrier bar{};
+    BCK(cudaMemcpyAsync(&bar, b->d_bar, sizeof(bar), cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (bar.err) return bfail(b, MRLBM_EDEVICE_TIMEOUT, "device flag: batch grid-barrier wait timed out");
+    for (size_t c = 0; c < b->h.size(); ++c) {
+        const int rc = mrlbm_status(b->h[c]);
+        if (rc != MRLBM_OK) return bfail(b, rc, "case " + std::to_string(c) + ": " + b->h[c]->err);
+    }
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_last_error(const mrlbm_batch* b, char* buf, size_t len) {
+    if (!buf || len == 0) return MRLBM_EINVAL;
+    std::snprintf(buf, len, "%s", b ? b->err.c_str() : g_create_error.c_str());
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_get_stream(const mrlbm_batch* b, void** stream) {
+    if (!b || !stream) return MRLBM_EINVAL;
+    *stream = (void*)b->stream;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_launch_count(const mrlbm_batch* b, int64_t* n) {
+    if (!b || !n) return MRLBM_EINVAL;
+    *n = b->launches;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_per_step) {
+    if (!b || trial_steps < 1) return MRLBM_EINVAL;
+    BCK(cudaSetDevice(b->device));
+    // drain the force rings and save every case's populations, counters and field sums
+    struct Saved { void* buf[2]; double* fstat; int iter, cur, ring_n; bool ovr; int64_t fstat_n; size_t hist; };
+    std::vector<Saved> sv(b->h.size());
+    int rc = MRLBM_OK;
+    for (size_t c = 0; c < b->h.size() && rc == MRLBM_OK; ++c) {
+        mrlbm_handle* h = b->h[c];
+        rc = drain_ring(h);
+        if (rc != MRLBM_OK) return bfail(b, rc, h->err);
+        Saved& s = sv[c];
+        s = Saved{{nullptr, nullptr}, nullptr, h->iter, h->cur, h->ring_n, h->ovr_live, h->fstat_n, h->hist.size()};
+        const size_t bytes = (size_t)h->L.total() * h->elem;
+        for (int k = 0; k < 2; ++k) {
+            BCK(cudaMalloc(&s.buf[k], bytes));
+            BCK(cudaMemcpyAsync(s.buf[k], h->buf[k], bytes, cudaMemcpyDeviceToDevice, b->stream));
+        }
+        if (h->d_fstat) {
+            const size_t fb = (size_t)6 * h->L.nx * h->L.ny * sizeof(double);
+            BCK(cudaMalloc((void**)&s.fstat, fb));
+            BCK(cudaMemcpyAsync(s.fstat, h->d_fstat, fb, cudaMemcpyDeviceToDevice, b->stream));
+        }
+    }
+    auto restore = [&]() {
+        for (size_t c = 0; c < b->h.size(); ++c) {
+            mrlbm_handle* h = b->h[c];
+            Saved& s = sv[c];
+            const size_t bytes = (size_t)h->L.total() * h->elem;
+            for (int k = 0; k < 2; ++k)
+                if (cudaMemcpyAsync(h->buf[k], s.buf[k], bytes, cudaMemcpyDeviceToDevice, b->stream) != cudaSuccess)
+                    rc = MRLBM_ECUDA;
+            if (s.fstat)
+                cudaMemcpyAsync(h->d_fstat, s.fstat, (size_t)6 * h->L.nx * h->L.ny * sizeof(double),
+                                cudaMemcpyDeviceToDevice, b->stream);
+            h->iter = s.iter;
+            h->cur = s.cur;
+            h->ring_n = s.ring_n;
+            h->ovr_live = s.ovr;
+            h->fstat_n = s.fstat_n;
+            h->hist.resize(s.hist);
+        }
+    };
+    const int tile0 = b->tile_cfg, sched0 = b->schedule, spl0 = b->steps_per_launch;
+    int best_tile = tile0, best_sched = sched0, best_spl = spl0;
+    double best = 1e300;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int steps = std::min(trial_steps, RING_CAP);
+    for (int cfg = VEC_CFG0; cfg < N_ALL_CFGS && rc == MRLBM_OK; ++cfg) {
+        for (int sched = MRLBM_BATCH_PERSISTENT; sched <= MRLBM_BATCH_GRAPH && rc == MRLBM_OK; ++sched) {
+            b->tile_cfg = cfg;
+            b->schedule = sched;
+            b->steps_per_launch = steps;
+            rc = batch_call(b, steps, 0);                    // warm-up (and graph capture)
+            if (rc == MRLBM_EUNSUPPORTED) { rc = MRLBM_OK; continue; }
+            if (rc != MRLBM_OK) break;
+            cudaEventRecord(e0, b->stream);
+            rc = batch_call(b, steps, 0);
+            cudaEventRecord(e1, b->stream);
+            if (rc != MRLBM_OK || cudaEventSynchronize(e1) != cudaSuccess) { rc = rc ? rc : MRLBM_ECUDA; break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; best_tile = cfg; best_sched = sched; best_spl = steps; }
+            restore();
+        }
+    }
+    restore();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(b->stream);
+    for (Saved& s : sv) {
+        for (void* q : s.buf) if (q) cudaFree(q);
+        if (s.fstat) cudaFree(s.fstat);
+    }
+    if (rc != MRLBM_OK) {
+        b->tile_cfg = tile0; b->schedule = sched0; b->steps_per_launch = spl0;
+        return rc;
+    }
+    b->tile_cfg = best_tile;
+    b->schedule = best_sched;
+    b->steps_per_launch = best_spl;
+    if (best_ms_per_step) *best_ms_per_step = best / steps;
     return MRLBM_OK;
 }
 

@@ -1,0 +1,149 @@
+// step_batch.cuh -- many independent cylinder cases advanced by one kernel.
+//
+// Work items of one step, over all cases: first every case's boundary and edge blocks
+// (aux items), then every case's bulk tiles of the 128-bit vector shape (step_common.cuh).
+// A block copies the item's case parameters to shared memory, sets the per-step fields
+// (time level, iteration, statistics flags, force-record slot) and runs the same device
+// functions as the single-case kernels, so each case steps exactly as it would alone.
+//
+// Two schedules:
+//   * persistent: one cooperative launch of resident blocks loops over the items of a step,
+//     then meets the others at a grid barrier and goes on with the next step, for nsteps steps;
+//   * per-step: one launch per step with one block per item (nsteps = 1), a sequence the
+//     host captures in a CUDA graph and replays.
+// Per-call state (iteration, time level, force-ring position) is uploaded before each call,
+// so a captured graph replays correctly.  The grid barrier's wait is bounded: after
+// BAR_SPIN_LIMIT polls a block raises ERR_BARRIER_TIMEOUT, sets the abort flag that every
+// waiting block also polls, and the kernel returns.
+#pragma once
+#include "batch_params.h"
+#include "step_common.cuh"
+
+namespace mrlbm {
+
+constexpr unsigned BAR_SPIN_LIMIT = 1u << 24;
+
+__device__ __forceinline__ int batch_find(const int* off, int n, int item) {
+    int lo = 0, hi = n;                                  // off[lo] <= item < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Stats steps (post_process and statsbegin <= it <= statsend) among iterations a..b.
+__device__ __forceinline__ int batch_stats_count(const BatchCase& c, int a, int b) {
+    if (!c.post_process) return 0;
+    const int lo = max(a, c.statsbegin), hi = min(b, c.statsend);
+    return hi >= lo ? hi - lo + 1 : 0;
+}
+
+// Bounded grid barrier of a cooperative launch (all blocks resident).  False after an abort.
+__device__ __forceinline__ bool batch_barrier(BatchBarrier* bar) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = &bar->gen;
+        volatile int* abort = &bar->abort;
+        const unsigned g = *gen;
+        __threadfence();
+        ok = 1;
+        if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+            bar->count = 0u;
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            for (unsigned it = 0; *gen == g; ++it) {
+                if (*abort) { ok = 0; break; }
+                if (it >= BAR_SPIN_LIMIT) {
+                    atomicOr(&bar->err, ERR_BARRIER_TIMEOUT);
+                    atomicExch(&bar->abort, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <class Phys, int WARPS, int NJ>
+__global__ void __launch_bounds__(WARPS * 32) step_kernel_batch(const __grid_constant__ BatchArgs<typename Phys::T> a) {
+    using T = typename Phys::T;
+    using P = typename Phys::P;
+    __shared__ __align__(64) unsigned char sp_raw[sizeof(P)];
+    __shared__ __align__(16) unsigned char smem[aux_smem_bytes<T>()];
+    P& sp = *reinterpret_cast<P*>(sp_raw);
+    const int n_aux = __ldg(a.aux_off + a.ncases);
+    const int n_items = n_aux + __ldg(a.tile_off + a.ncases);
+    for (int s = 0; s < a.nsteps; ++s) {
+        const int cs = a.step0 + s;                     // step index within the call
+        for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+            const bool aux = item < n_aux;
+            const int c = aux ? batch_find(a.aux_off, a.ncases, item) : batch_find(a.tile_off, a.ncases, item - n_aux);
+            {   // case parameters -> shared memory, 16 bytes per thread
+                const uint4* src = reinterpret_cast<const uint4*>(a.params + c);
+                uint4* dst = reinterpret_cast<uint4*>(sp_raw);
+                for (int q = threadIdx.x; q < (int)(sizeof(P) / 16); q += blockDim.x) dst[q] = src[q];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const BatchCase& bc = a.cases[c];
+                const int iter = bc.iter0 + cs + 1;
+                if (cs & 1) {                           // params hold the call's first time level
+                    const T* t = sp.src;
+                    sp.src = sp.dst;
+                    sp.dst = const_cast<T*>(t);
+                }
+                const bool stats = bc.post_process && iter >= bc.statsbegin && iter <= bc.statsend;
+                sp.iter = iter;
+                sp.do_stats = stats;
+                sp.rec = stats ? bc.ring + (size_t)(bc.ring_n0 + batch_stats_count(bc, bc.iter0 + 1, iter - 1)) * REC_WORDS
+                               : nullptr;
+                sp.zero_solid_u = bc.post_process && bc.iplot > 0 && iter % bc.iplot == 0 && bc.plot_cyl;
+                sp.macro = (a.want_macro && cs == a.call_steps - 1) ? bc.macro : nullptr;
+                sp.fstat = (bc.fstat && iter >= bc.fs_begin && iter <= bc.fs_end) ? bc.fstat : nullptr;
+                if (!(cs == 0 && bc.ovr_live)) {
+                    sp.ovr = nullptr;
+                    sp.n_ovr = 0;
+                }
+            }
+            __syncthreads();
+            if (aux) aux_item<Phys>(sp, smem, item - __ldg(a.aux_off + c));
+            else vec_tile<Phys, WARPS, NJ>(sp, item - n_aux - __ldg(a.tile_off + c));
+            __syncthreads();
+        }
+        if (a.nsteps > 1 && !batch_barrier(a.bar)) return;
+    }
+}
+
+// Block sizes of the batch kernels: the vector shapes' warps per block.
+template <class Phys, int WARPS, int NJ>
+int launch_step_batch(const BatchArgs<typename Phys::T>& a, int grid, bool cooperative, cudaStream_t s) {
+    auto k = step_kernel_batch<Phys, WARPS, NJ>;
+    if (!cooperative) {
+        k<<<(unsigned)grid, WARPS * 32, 0, s>>>(a);
+        return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    }
+    void* args[] = {(void*)&a};
+    return cudaLaunchCooperativeKernel((const void*)k, dim3((unsigned)grid), dim3(WARPS * 32), args, 0, s) ==
+                   cudaSuccess
+               ? 0
+               : -1;
+}
+
+template <class Phys, int WARPS, int NJ>
+int batch_blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_batch<Phys, WARPS, NJ>, WARPS * 32, 0) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
+}  // namespace mrlbm

@@ -118,8 +118,8 @@ __device__ __forceinline__ void aux_tail(const typename Phys::P& p, unsigned cha
     // Three sequential sums (Fx over nodes, Fy over nodes, rho over the inlet column), one per
     // warp: the warp stages AUX_CHUNK terms at a time in shared memory with parallel loads and
     // its lane 0 adds them in index order, so only the adds are serial.
-    const int w = tid >> 5, lane = tid & 31;
-    if (w < 3) {
+    const int lane = tid & 31;
+    for (int w = tid >> 5; w < 3; w += (int)(blockDim.x >> 5)) {   // 64-thread blocks: a warp does two
         const int n = w < 2 ? p.nb : p.L.ny;
         const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
         double* st = reinterpret_cast<double*>(smem) + w * AUX_CHUNK;
@@ -148,13 +148,13 @@ __device__ __forceinline__ void aux_tail(const typename Phys::P& p, unsigned cha
 }
 
 template <class Phys>
-__device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsigned char* smem) {
+__device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsigned char* smem, int bb) {
     using T = typename Phys::T;
     T* sg = reinterpret_cast<T*>(smem);                               // G_STAGED * BNODES
     int* sgi = reinterpret_cast<int*>(smem + sizeof(T) * G_STAGED * BNODES);   // I_NFIELDS * BNODES
     const int nthr = blockDim.x, tid = threadIdx.x;
     const int bn = nthr / BLANES;
-    const int l0 = blockIdx.x * bn;
+    const int l0 = bb * bn;
     for (int idx = tid; idx < G_STAGED * bn; idx += nthr) {
         const int f = idx / bn, n = idx - f * bn;
         sg[idx] = (l0 + n < p.nb) ? p.bgeo[f * p.nb + l0 + n] : T(0);
@@ -227,25 +227,31 @@ __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, un
     aux_tail<Phys>(p, smem);
 }
 
+// Shared memory of an auxiliary block: the boundary tables and, afterwards, the tail's
+// staged terms.
+template <class T>
+constexpr int aux_smem_bytes() {
+    return (int)(sizeof(T) * G_STAGED + sizeof(int) * I_NFIELDS) * BNODES > 3 * AUX_CHUNK * (int)sizeof(double)
+               ? (int)(sizeof(T) * G_STAGED + sizeof(int) * I_NFIELDS) * BNODES
+               : 3 * AUX_CHUNK * (int)sizeof(double);
+}
+
+// Auxiliary work item b of a step: boundary block b (b < nbblk) or edge block b - nbblk.
+template <class Phys>
+__device__ __forceinline__ void aux_item(const typename Phys::P& p, unsigned char* smem, int b) {
+    if (b < p.nbblk) boundary_block<Phys>(p, smem, b);
+    else edge_block<Phys>(p, b - p.nbblk, smem);
+}
+
 // Boundary and edge blocks sit at the start of the grid.  True when this block is one of them
 // (and has done its work); bulk tile t is then blockIdx.x - nbblk - neblk.
 template <class Phys>
 __device__ __forceinline__ bool run_aux_block(const typename Phys::P& p) {
-    using T = typename Phys::T;
-    constexpr int STAGING = (int)(sizeof(T) * G_STAGED + sizeof(int) * I_NFIELDS) * BNODES;
-    constexpr int TAIL = 3 * AUX_CHUNK * (int)sizeof(double);
-    // one buffer for the boundary tables and, afterwards, the tail's staged terms
-    __shared__ __align__(16) unsigned char smem[STAGING > TAIL ? STAGING : TAIL];
+    __shared__ __align__(16) unsigned char smem[aux_smem_bytes<typename Phys::T>()];
     const int b = (int)blockIdx.x;
-    if (b < p.nbblk) {
-        boundary_block<Phys>(p, smem);
-        return true;
-    }
-    if (b < p.nbblk + p.neblk) {
-        edge_block<Phys>(p, b - p.nbblk, smem);
-        return true;
-    }
-    return false;
+    if (b >= p.nbblk + p.neblk) return false;
+    aux_item<Phys>(p, smem, b);
+    return true;
 }
 
 inline int edge_blocks(int nx, int ny, int nthr) { return (2 * nx + 2 * (ny - 2) + nthr - 1) / nthr; }
@@ -327,13 +333,11 @@ template <> struct Vec16<double> {
     }
 };
 
-template <class Phys, int WARPS, int NJ, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
+template <class Phys, int WARPS, int NJ>
+__device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
     using T = typename Phys::T;
     using VT = Vec16<T>;
     constexpr int VW = VT::N;
-    if (run_aux_block<Phys>(p)) return;
-    const int t = blockIdx.x - p.nbblk - p.neblk;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nx = p.L.nx, ny = p.L.ny;
@@ -396,6 +400,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid
             for (int k = 0; k < Q; ++k) VT::store(d + k * plane, out[k]);
         }
     }
+}
+
+template <class Phys, int WARPS, int NJ, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
+    if (run_aux_block<Phys>(p)) return;
+    vec_tile<Phys, WARPS, NJ>(p, (int)blockIdx.x - p.nbblk - p.neblk);
 }
 
 template <class Phys, int WARPS, int NJ, int MINB>

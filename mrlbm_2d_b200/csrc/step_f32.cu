@@ -1,6 +1,7 @@
 // step_f32.cu -- FP32 deviation-form fused step instantiations (contraction allowed).
 #include "step_fp32.cuh"
 #include "step_tma.cuh"
+#include "step_batch.cuh"
 
 namespace mrlbm {
 
@@ -46,6 +47,43 @@ void tma_box(int precision, int tile_cfg, int* box_w, int* box_h, int* stages) {
     *box_w = c.bx + 2 * m;
     *box_h = c.by;
     *stages = c.stages;
+}
+
+int launch_batch_f32(const BatchArgs<float>& a, int tile_cfg, int grid, bool cooperative, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    using Ph = fp32::Physics;
+    switch (tile_cfg) {
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return launch_step_batch<Ph, w, nj>(a, grid, cooperative, s);
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return -2;
+    }
+}
+
+int batch_blocks_per_sm_f32(int tile_cfg) {
+    using Ph = fp32::Physics;
+    switch (tile_cfg) {
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return batch_blocks_per_sm<Ph, w, nj>();
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return 0;
+    }
+}
+
+int batch_blocks_per_sm(int precision, int tile_cfg) {
+    return precision == 64 ? batch_blocks_per_sm_f64(tile_cfg) : batch_blocks_per_sm_f32(tile_cfg);
+}
+
+int batch_block_threads(int tile_cfg) {
+    switch (tile_cfg) {
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return w * 32;
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return 0;
+    }
 }
 
 }  // namespace mrlbm

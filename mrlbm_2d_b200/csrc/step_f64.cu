@@ -2,6 +2,7 @@
 // and sum rounds separately, as in the reference's x86-64 FP64 arithmetic.
 #include "step_fp64.cuh"
 #include "step_tma.cuh"
+#include "step_batch.cuh"
 
 namespace mrlbm {
 
@@ -35,6 +36,29 @@ int tma_ctas_per_sm_f64(int tile_cfg) {
     default: n = 0;
     }
     return n;
+}
+
+int launch_batch_f64(const BatchArgs<double>& a, int tile_cfg, int grid, bool cooperative, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    using Ph = fp64::Physics;
+    switch (tile_cfg) {
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return launch_step_batch<Ph, w, nj>(a, grid, cooperative, s);
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return -2;
+    }
+}
+
+int batch_blocks_per_sm_f64(int tile_cfg) {
+    using Ph = fp64::Physics;
+    switch (tile_cfg) {
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return batch_blocks_per_sm<Ph, w, nj>();
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return 0;
+    }
 }
 
 }  // namespace mrlbm

@@ -126,6 +126,10 @@ constexpr TmaCfg TMA_CFGS[N_TMA_CFGS] = {MRLBM_TMA_LIST(MRLBM_TMA_ENTRY)};
     X(20, 4, 1, 4)        \
     X(21, 2, 4, 8)
 constexpr int N_VEC_CFGS = 6;
+struct VecCfg { int warps, nj, minb; };
+#define MRLBM_VEC_ENTRY(id, w, nj, mb) {w, nj, mb},
+constexpr VecCfg VEC_CFGS[N_VEC_CFGS] = {MRLBM_VEC_LIST(MRLBM_VEC_ENTRY)};
+#undef MRLBM_VEC_ENTRY
 constexpr int VEC_CFG0 = TMA_CFG0 + N_TMA_CFGS;
 constexpr int N_ALL_CFGS = VEC_CFG0 + N_VEC_CFGS;
 inline bool is_tma_cfg(int c) { return c >= TMA_CFG0 && c < VEC_CFG0; }

@@ -1,0 +1,98 @@
+"""Batched cases: one kernel advancing several independent cases (persistent cooperative
+launches or CUDA-graph replays of per-step launches) gives every case exactly the bits it gets
+when stepped alone."""
+import numpy as np
+import pytest
+
+from cases import CASES
+from mrlbm_2d_b200.config import cylinder_case
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["freeslip_label15", "reference_default_bcs", "x_and_y_periodic", "reference_walls", "freeslip_xperiodic"]
+
+
+def _cfgs():
+    return [CASES[n]() for n in NAMES] + [cylinder_case(256, 64, 12.8, 51.2, 32.5, 150.0, 0.05)]
+
+
+def _alone(mrlbm, cfg, prec, steps, macro=False, fields=None):
+    s = mrlbm.Simulation(cfg, precision=prec)
+    s.tile_config = 18
+    if fields:
+        s.field_stats_window(*fields)
+    s.step(steps, macro=macro)
+    out = dict(f=s.get_state(), forces=s.forces(), status=s.status())
+    if macro:
+        out["macro"] = s.macro()
+    if fields:
+        out["fields"] = s.field_stats()
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("tile,sched,spl", [(18, 0, 7), (16, 1, 5), (21, 0, 1), (17, 1, 13), (20, 0, 23)])
+def test_batch_matches_single_cases(mrlbm, prec, tile, sched, spl):
+    cfgs = _cfgs()
+    b = mrlbm.Batch(cfgs, precision=prec)
+    b.set_schedule(tile, sched, spl)
+    b.step(10)
+    b.step(13)                                   # calls that do not divide into launches
+    assert b.status() == 0
+    for cfg, c in zip(cfgs, b.cases):
+        ref = _alone(mrlbm, cfg, prec, 23)
+        assert np.array_equal(c.get_state(), ref["f"])
+        it, fd, fl, rin = c.forces()
+        assert np.array_equal(it, ref["forces"][0])
+        assert np.array_equal(fd, ref["forces"][1]) and np.array_equal(fl, ref["forces"][2])
+        assert np.array_equal(rin, ref["forces"][3])
+    b.close()
+
+
+@pytest.mark.parametrize("sched", [0, 1])
+def test_batch_macro_fields_and_loaded_state(mrlbm, sched):
+    cfgs = _cfgs()
+    b = mrlbm.Batch(cfgs, precision=64)
+    b.set_schedule(18, sched, 6)
+    # a loaded state (x-and-y periodic case: override list on the first step) and field stats
+    f0 = [c.get_state() for c in b.cases]
+    for c, f in zip(b.cases, f0):
+        c.load_state(f, iter=0)
+        c.field_stats_window(3, 17)
+    b.step(20, macro=True)
+    for cfg, c, f in zip(cfgs, b.cases, f0):
+        s = mrlbm.Simulation(cfg, precision=64)
+        s.tile_config = 18
+        s.load_state(f, iter=0)
+        s.field_stats_window(3, 17)
+        s.step(20, macro=True)
+        assert np.array_equal(c.get_state(), s.get_state())
+        m1, m2 = c.macro(), s.macro()
+        for k in m1:
+            assert np.array_equal(m1[k], m2[k]), k
+        f1, f2 = c.field_stats(), s.field_stats()
+        assert f1["n"] == f2["n"] == 15
+        for k in ("mean_u", "rms_v", "mean_p"):
+            assert np.array_equal(f1[k], f2[k]), k
+        s.close()
+    b.close()
+
+
+def test_batch_autotune_restores_state(mrlbm):
+    cfgs = _cfgs()
+    b = mrlbm.Batch(cfgs, precision=32)
+    b.step(4)
+    before = [c.get_state() for c in b.cases]
+    (tile, sched, spl), ms = b.autotune(trial_steps=8)
+    assert 16 <= tile <= 21 and sched in (0, 1) and ms > 0
+    for c, f in zip(b.cases, before):
+        assert np.array_equal(c.get_state(), f)
+        assert c.iter == 5
+    b.step(6)
+    for cfg, c in zip(cfgs, b.cases):
+        ref = _alone(mrlbm, cfg, 32, 10)
+        assert np.array_equal(c.get_state(), ref["f"])
+        assert np.array_equal(c.forces()[1], ref["forces"][1])
+    assert b.status() == 0
+    b.close()

@@ -25,13 +25,14 @@ def test_all_tile_shapes_bit_identical(mrlbm, prec):
         ran.append(c)
         assert s.status() == 0
         st = s.get_state()
-        _, fd, fl, _ = s.forces()
+        _, fd, fl, rin = s.forces()
         s.close()
         if ref is None:
-            ref = (st, fd, fl)
+            ref = (st, fd, fl, rin)
         else:
             assert np.array_equal(st, ref[0]), f"tile shape {c}"
             assert np.array_equal(fd, ref[1]) and np.array_equal(fl, ref[2]), f"tile shape {c}"
+            assert np.array_equal(rin, ref[3]), f"tile shape {c}: inlet density sum"
     assert len([c for c in ran if c >= 10]) >= 3, ran
 
 
