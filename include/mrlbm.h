@@ -258,6 +258,23 @@ int mrlbm_field_stats_window(mrlbm_handle* h, int32_t begin_iter, int32_t end_it
 int mrlbm_field_stats_get(mrlbm_handle* h, double* mean_u, double* mean_v, double* mean_p, double* rms_u,
                           double* rms_v, double* rms_p, int64_t* n_samples);
 
+/* ---- body force and the adjoint of mean drag (no counterpart in the reference) ----------
+ * Body force: g (2 x nx*ny, x components then y, Fortran node order) adds the momentum
+ * source fout_k += 3 w_k (c_k . g) after collision at every bulk and edge node (not at
+ * curved-wall nodes); NULL removes it.  An extension: the reference has no forcing term. */
+int mrlbm_set_body_force(mrlbm_handle* h, const double* g);
+
+/* Gradient of J = mean net drag over the last `window` of the next `nsteps` steps, from the
+ * handle's current state (the handle is not advanced), with respect to the body force (grad_body,
+ * 2 x nx*ny) and the inlet profile u_in(j) (grad_uin, ny; the uniform inlet value when no
+ * profile is set).  Discrete adjoint of the FP64 step: a forward pass keeps a checkpoint every
+ * checkpoint_every steps; the backward pass recomputes each segment from its checkpoint and runs
+ * the adjoint kernels step by step.  Either gradient pointer may be NULL; both NULL computes J
+ * only.  FP64 handles with inlet/outlet columns, free-slip or y-periodic walls and the rotated
+ * strong closure (the defaults); MRLBM_EUNSUPPORTED otherwise. */
+int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t window, int32_t checkpoint_every, double* J,
+                       double* grad_body, double* grad_uin);
+
 /* ---- batched cases (no counterpart in the reference, which runs one case per process) ----
  * Many independent cases of one precision on one device advance together: one kernel covers
  * the work of every case, either as a persistent cooperative launch that loops over steps

@@ -36,6 +36,7 @@ EXPORTED = [
     "mrlbm_batch_create", "mrlbm_batch_destroy", "mrlbm_batch_case", "mrlbm_batch_step",
     "mrlbm_batch_set_schedule", "mrlbm_batch_get_schedule", "mrlbm_batch_autotune", "mrlbm_batch_status",
     "mrlbm_batch_last_error", "mrlbm_batch_launch_count", "mrlbm_batch_get_stream",
+    "mrlbm_set_body_force", "mrlbm_adjoint_drag",
 ]
 BATCH_PERSISTENT, BATCH_GRAPH = 0, 1
 
@@ -106,6 +107,8 @@ def load_library(path=None):
         "mrlbm_batch_last_error": [vp, ctypes.c_char_p, ctypes.c_size_t],
         "mrlbm_batch_launch_count": [vp, vp],
         "mrlbm_batch_get_stream": [vp, vp],
+        "mrlbm_set_body_force": [vp, vp],
+        "mrlbm_adjoint_drag": [vp, i32, i32, i32, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -294,6 +297,29 @@ class Simulation:
         self._check(self._L.mrlbm_get_macro(self._h, *[_ptr(o) for o in outs]))
         names = ["rho", "ux", "uy", "mxx", "myy", "mxy"]
         return {n: o.reshape(self.ny, self.nx).T for n, o in zip(names, outs)}
+
+    def set_body_force(self, g):
+        """Body force g of shape (2, nx, ny) (x and y components, [c, i-1, j-1]); None removes it."""
+        if g is None:
+            self._check(self._L.mrlbm_set_body_force(self._h, None))
+            return
+        g = np.asarray(g, dtype=np.float64)
+        assert g.shape == (2, self.nx, self.ny)
+        flat = np.ascontiguousarray(g.transpose(0, 2, 1)).ravel()     # Fortran node order per component
+        self._check(self._L.mrlbm_set_body_force(self._h, _ptr(flat)))
+
+    def adjoint_drag(self, nsteps, window, checkpoint_every=100, grads=True):
+        """J = mean drag over the last `window` of the next `nsteps` steps (state not advanced)
+        and, with grads, dJ/d(body force) as (2, nx, ny) and dJ/d(u_in) as (ny,)."""
+        J = ctypes.c_double()
+        gb = np.zeros(2 * self.nx * self.ny) if grads else None
+        gu = np.zeros(self.ny) if grads else None
+        self._check(self._L.mrlbm_adjoint_drag(self._h, int(nsteps), int(window), int(checkpoint_every),
+                                               ctypes.byref(J), _ptr(gb) if grads else None,
+                                               _ptr(gu) if grads else None))
+        if not grads:
+            return J.value
+        return J.value, gb.reshape(2, self.ny, self.nx).transpose(0, 2, 1).copy(), gu
 
     def field_stats_window(self, begin_iter, end_iter):
         """Accumulate FP64 mean/rms sums of u, v, p over steps begin_iter..end_iter (clears them)."""

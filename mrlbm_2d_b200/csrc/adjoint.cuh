@@ -1,0 +1,394 @@
+// adjoint.cuh -- discrete adjoint of the FP64 step for the gradient of time-averaged drag.
+//
+// State of step n: the post-collision field F^n (the buffer a step writes).  Step n maps
+// F^{n-1} to F^n node by node: node x gathers its inputs g_x from F^{n-1} (pull streaming),
+// and its local map C_x gives the nine outputs F^n(x, :).  With J = (1/T) sum_{n in window}
+// D^n, D^n the net drag of step n (a function of the wall nodes' inputs and outputs), the
+// adjoint field lambda^n = dJ/dF^n obeys
+//     lambda^{n-1}(slot) = sum over the consumers x of the slot of (dC_x/dg_x)^T lambda^n(x)
+//                          + w_n dD^n/dF^{n-1}(slot),      w_n = 1/T inside the window,
+// and the parameter gradients collect (dC_x/dtheta)^T lambda^n(x).  One adjoint step runs
+// three kernels, each node's contribution added atomically to lambda^{n-1} at the slots it
+// pulled (a slot can feed several nodes: stencils, the outlet copy, corner wraps):
+//   * bulk nodes (fluid and solid, not edge columns, not curved-wall nodes): reverse mode
+//     written out by hand: reconstruction -> collision -> moments (adjoint_bulk_node);
+//   * edge columns (inlet i = 1, outlet i = nx): one thread per (node, input), the node's
+//     local map evaluated on dual numbers carrying the derivative along that input, then
+//     contracted with lambda^n (the transposed Jacobian column); the inlet's extra input is
+//     u_in(j), whose column gives the inlet-profile gradient;
+//   * curved-wall nodes: likewise, over the node's 9 own inputs and the 72 inputs of its 8
+//     bilinear stencil nodes, with the drag contribution of the node in the same pass.
+// The local maps below restate the FP64 step's arithmetic (step_fp64.cuh) for a generic
+// scalar; they cover the closures the adjoint supports: rotated strong curved-wall closure
+// with velocity and moment extrapolation, inlet and outlet edge closures (apply_bc), free-slip
+// or y-periodic top and bottom, no incompressible variants.
+#pragma once
+#include "adjoint.h"
+#include "step_fp64.cuh"
+
+namespace mrlbm {
+namespace adj {
+
+using P = StepParams<double>;
+
+// ---- dual numbers (value, derivative along one input) -----------------------------------
+struct Dual {
+    double v, d;
+    __device__ Dual() : v(0.0), d(0.0) {}
+    __device__ Dual(double a) : v(a), d(0.0) {}
+    __device__ Dual(double a, double b) : v(a), d(b) {}
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+__device__ __forceinline__ Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) {
+    const double q = a.v / b.v;
+    return Dual(q, (a.d - q * b.d) / b.v);
+}
+__device__ __forceinline__ Dual operator+(Dual a, double b) { return Dual(a.v + b, a.d); }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return Dual(a + b.v, b.d); }
+__device__ __forceinline__ Dual operator-(Dual a, double b) { return Dual(a.v - b, a.d); }
+__device__ __forceinline__ Dual operator-(double a, Dual b) { return Dual(a - b.v, -b.d); }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return Dual(a.v * b, a.d * b); }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return Dual(a * b.v, a * b.d); }
+__device__ __forceinline__ Dual operator/(Dual a, double b) { return Dual(a.v / b, a.d / b); }
+__device__ __forceinline__ Dual operator/(double a, Dual b) {
+    const double q = a / b.v;
+    return Dual(q, -q * b.d / b.v);
+}
+
+template <class S>
+struct MacS { S rho, ux, uy, mxx, myy, mxy; };
+
+template <class S>
+__device__ __forceinline__ MacS<S> moments_s(const S f[Q], double hm, double hp) {
+    MacS<S> m;
+    S r = f[0];
+    for (int k = 1; k < Q; ++k) r = r + f[k];
+    const S inv = 1.0 / r;
+    const S sx = ((((f[1] - f[3]) + f[5]) - f[6]) - f[7]) + f[8];
+    const S sy = ((((f[2] - f[4]) + f[5]) + f[6]) - f[7]) - f[8];
+    S sxx = f[0] * hm, syy = f[0] * hm;
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+        sxx = sxx + f[k] * (ex(k) != 0 ? hp : hm);
+        syy = syy + f[k] * (ey(k) != 0 ? hp : hm);
+    }
+    const S sxy = ((f[5] - f[6]) + f[7]) - f[8];
+    m.rho = r;
+    m.ux = sx * inv;
+    m.uy = sy * inv;
+    m.mxx = sxx * inv;
+    m.myy = syy * inv;
+    m.mxy = sxy * inv;
+    return m;
+}
+
+// Collision and Hermite reconstruction (2d_mrlbm.f90:407-415, 445-457), no incomp_bulk.
+template <class S>
+__device__ __forceinline__ void collide_s(const P& p, const MacS<S>& m, S fo[Q]) {
+    const double om = p.omega, om1 = p.omega1;
+    const S mxx = om1 * m.mxx + om * m.ux * m.ux;
+    const S myy = om1 * m.myy + om * m.uy * m.uy;
+    const S mxy = om1 * m.mxy + om * m.ux * m.uy;
+    const S a = 4.5 * mxx, b = 4.5 * myy, c = 9.0 * mxy;
+    const S am = a * p.hm, ap = a * p.hp, bm = b * p.hm, bp = b * p.hp;
+    const S t1 = 3.0 * m.ux, t2 = 3.0 * m.uy, t5 = 3.0 * (m.ux + m.uy), t8 = 3.0 * (m.ux - m.uy);
+    const S w0 = p.w[0] * m.rho, w1 = p.w[1] * m.rho, w5 = p.w[5] * m.rho;
+    fo[0] = w0 * ((1.0 + am) + bm);
+    fo[1] = w1 * (((1.0 + t1) + ap) + bm);
+    fo[2] = w1 * (((1.0 + t2) + am) + bp);
+    fo[3] = w1 * (((1.0 - t1) + ap) + bm);
+    fo[4] = w1 * (((1.0 - t2) + am) + bp);
+    fo[5] = w5 * ((((1.0 + t5) + ap) + bp) + c);
+    fo[6] = w5 * ((((1.0 - t8) + ap) + bp) - c);
+    fo[7] = w5 * ((((1.0 - t5) + ap) + bp) + c);
+    fo[8] = w5 * ((((1.0 + t8) + ap) + bp) - c);
+}
+
+// Sums over an incoming mask normalised by rho_I (apply_bc prologue, 2d_mrlbm.f90:1249-1269).
+template <class S>
+__device__ __forceinline__ void incoming_s(const S f[Q], int mask, double hm, double hp, S& rhoI, S& mxxI, S& myyI,
+                                           S& mxyI) {
+    S r = 0.0, a = 0.0, b = 0.0, c = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        if (!((mask >> k) & 1)) continue;
+        r = r + f[k];
+        a = a + f[k] * (ex(k) != 0 ? hp : hm);
+        b = b + f[k] * (ey(k) != 0 ? hp : hm);
+        const int hxy = ex(k) * ey(k);
+        if (hxy > 0) c = c + f[k];
+        if (hxy < 0) c = c - f[k];
+    }
+    rhoI = r;
+    const S inv = 1.0 / r;
+    mxxI = a * inv;
+    myyI = b * inv;
+    mxyI = c * inv;
+}
+
+// Edge column node (i = 1 inlet or i = nx outlet) of a free-slip / y-periodic case:
+// moments, Dirichlet values and the apply_bc closure (2d_mrlbm.f90:249-272, 1237-1366).
+template <class S>
+__device__ __forceinline__ void edge_map(const P& p, int i, const S f[Q], const S fn[Q], S uin, S fo[Q]) {
+    MacS<S> m = moments_s(f, p.hm, p.hp);
+    S rhoI, mxxI, myyI, mxyI;
+    if (i == 1) {
+        m.ux = uin;
+        m.uy = S(p.vinlet);
+        incoming_s(f, fp64::M_INLET, p.hm, p.hp, rhoI, mxxI, myyI, mxyI);
+        m.rho = (4.0 * rhoI + 3.0 * rhoI * mxxI) / (3.0 - 3.0 * m.ux);
+        const S rp = m.rho;
+        m.mxx = (rp + 9.0 * rhoI * mxxI + 3.0 * rp * m.ux) / (6.0 * rp);
+        m.myy = 6.0 * rhoI * myyI / (5.0 * rp);
+        m.mxy = 2.0 * rhoI * mxyI / rp;
+    } else {
+        S r = fn[0];
+        for (int k = 1; k < Q; ++k) r = r + fn[k];
+        const S inv = 1.0 / r;
+        m.rho = r;
+        m.ux = (((((fn[1] - fn[3]) + fn[5]) - fn[6]) - fn[7]) + fn[8]) * inv;
+        m.uy = (((((fn[2] - fn[4]) + fn[5]) + fn[6]) - fn[7]) - fn[8]) * inv;
+        incoming_s(f, fp64::M_OUTLET, p.hm, p.hp, rhoI, mxxI, myyI, mxyI);
+        const S rp = m.rho;
+        m.mxx = (rp + 9.0 * rhoI * mxxI - 3.0 * rp * m.ux) / (6.0 * rp);
+        m.myy = 6.0 * rhoI * myyI / (5.0 * rp);
+        m.mxy = (6.0 * rhoI * mxyI - rp * m.uy) / (3.0 * rp);
+    }
+    collide_s(p, m, fo);
+}
+
+__device__ __forceinline__ double gf(const P& p, int field, int l) { return __ldg(p.bgeo + (int64_t)field * p.nb + l); }
+__device__ __forceinline__ int gi(const P& p, int field, int l) { return __ldg(p.bint + (int64_t)field * p.nb + l); }
+
+// Curved-wall node l: stencil moments, bilinear interpolation at reference points 2 and 3,
+// extrapolation to the node, rotated strong closure, collision (2d_mrlbm.f90:294-311,
+// 768-928, 1635-1765, 407-457) and the node's drag term (2d_mrlbm.f90:558-591).
+// f: own inputs; fs: the 8 stencil nodes' inputs (stencil s at fs[9 s .. 9 s + 8]).
+template <class S>
+__device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const S fs[8 * Q], S fo[Q], S& drag) {
+    S u[2], v[2], mx[2], my[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const double xd = gf(p, r == 0 ? G_XD2 : G_XD3, l), yd = gf(p, r == 0 ? G_YD2 : G_YD3, l);
+        S row_u[2], row_v[2], row_mx[2], row_my[2];
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+            S su = 0.0, sv = 0.0, smx = 0.0, smy = 0.0;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int s = 4 * r + 2 * rr + cc;
+                const MacS<S> m = moments_s(fs + Q * s, p.hm, p.hp);
+                const double c2 = gf(p, G_SCC + s, l), s2q = gf(p, G_SSS + s, l), sn2 = gf(p, G_SS2 + s, l);
+                const S rmx = m.mxx * c2 + m.myy * s2q + m.mxy * sn2;
+                const S rmy = m.mxx * s2q + m.myy * c2 - m.mxy * sn2;
+                const double wx = cc ? xd : (1.0 - xd);
+                su = su + wx * m.ux;
+                sv = sv + wx * m.uy;
+                smx = smx + wx * rmx;
+                smy = smy + wx * rmy;
+            }
+            row_u[rr] = su; row_v[rr] = sv; row_mx[rr] = smx; row_my[rr] = smy;
+        }
+        u[r] = (1.0 - yd) * row_u[0] + yd * row_u[1];
+        v[r] = (1.0 - yd) * row_v[0] + yd * row_v[1];
+        mx[r] = (1.0 - yd) * row_mx[0] + yd * row_mx[1];
+        my[r] = (1.0 - yd) * row_my[0] + yd * row_my[1];
+    }
+    const double t2 = gf(p, G_T2, l), t3 = gf(p, G_T3, l);
+    MacS<S> m;
+    m.ux = t2 * u[0] - t3 * u[1];
+    m.uy = t2 * v[0] - t3 * v[1];
+    const S Mxx = t2 * mx[0] - t3 * mx[1];
+    const S Myy = t2 * my[0] - t3 * my[1];
+    const double c = gf(p, G_CTH, l), sn = gf(p, G_STH, l);
+    const S uxp = m.ux * c + m.uy * sn;
+    const S uyp = m.uy * c - m.ux * sn;
+    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const double omega = p.omega;
+    S rhoI = 0.0, mxyI = 0.0, A_p = 0.0, E_p = 0.0, D_xy = 0.0;
+    double B11 = 0, B22 = 0, B12 = 0, F11 = 0, F22 = 0, F12 = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double cxp = gf(p, G_CXP + k, l), cyp = gf(p, G_CYP + k, l);
+        const double hxx = gf(p, G_HXXP + k, l), hyy = gf(p, G_HYYP + k, l), hxy = gf(p, G_HXYP + k, l);
+        const double wk = p.w[k];
+        const S A_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp);
+        const S E_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp + 4.5 * (uxp * uxp) * hxx + 4.5 * (uyp * uyp) * hyy +
+                            9.0 * (uxp * uyp) * hxy);
+        const double B11_i = 4.5 * wk * hxx, B22_i = 4.5 * wk * hyy, B12_i = 4.5 * wk * hxy;
+        if ((Os >> k) & 1) { A_p = A_p + A_i; E_p = E_p + E_i; B11 += B11_i; B22 += B22_i; B12 += B12_i; }
+        if ((Is >> k) & 1) {
+            rhoI = rhoI + f[k];
+            mxyI = mxyI + f[k] * hxy;
+            D_xy = D_xy + A_i * hxy;
+            F11 += B11_i * hxy;
+            F22 += B22_i * hxy;
+            F12 += B12_i * hxy;
+        }
+    }
+    mxyI = mxyI / rhoI;
+    const S G_p = (1.0 - omega) * A_p + omega * E_p;
+    const double J11 = (1.0 - omega) * B11, J22 = (1.0 - omega) * B22, J12 = (1.0 - omega) * B12;
+    const S L11 = J11 * mxyI - F11, L22 = J22 * mxyI - F22, L12 = 2.0 * (J12 * mxyI - F12);
+    const S R = D_xy - G_p * mxyI;
+    const S Mxy = (R - Mxx * L11 - Myy * L22) / L12;
+    const S den = (1.0 - omega) * A_p + (1.0 - omega) * (Mxx * B11 + Myy * B22 + 2.0 * Mxy * B12) + omega * E_p;
+    m.rho = rhoI / den;
+    const double cc = gf(p, G_CC, l), ss = gf(p, G_SS, l), s2 = gf(p, G_S2TH, l), c2 = gf(p, G_C2TH, l);
+    m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
+    m.myy = Mxx * ss + Myy * cc + Mxy * s2;
+    m.mxy = (Mxx - Myy) * 0.5 * s2 + Mxy * c2;
+    collide_s(p, m, fo);
+    S fxo = 0.0, fxi = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        if (ex(k) == 0) continue;
+        if ((Os >> k) & 1) fxo = fxo + fo[k] * (double)ex(k);
+        if ((Is >> k) & 1) fxi = fxi + f[k] * (double)ex(k);
+    }
+    drag = fxi - fxo;
+}
+
+// ---- kernels ------------------------------------------------------------------------------
+
+// Add c to lambda^{n-1} at the slot node (i, j) pulled for direction k (ghost slots hold
+// constants and take nothing).
+__device__ __forceinline__ void scatter(const P& p, const AdjArgs& a, int i, int j, int k, double c) {
+    const SrcSlot sl = stream_source(p.L.nx, p.L.ny, i, j, k, p.xper, p.yper, p.freeslip);
+    if (sl.i < 1 || sl.i > p.L.nx || sl.j < 1 || sl.j > p.L.ny) return;
+    atomicAdd(a.lam_out + p.L.at(sl.i, sl.j, sl.k), c);
+}
+
+__device__ __forceinline__ void body_grad(const P& p, const AdjArgs& a, int i, int j, const double lam[Q]) {
+    if (!a.grad_body) return;
+    const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1), N = (int64_t)p.L.nx * p.L.ny;
+    double gx = 0.0, gy = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        gx += 3.0 * p.w[k] * ex(k) * lam[k];
+        gy += 3.0 * p.w[k] * ey(k) * lam[k];
+    }
+    a.grad_body[n] += gx;
+    a.grad_body[N + n] += gy;
+}
+
+// Bulk node, reverse mode by hand.  Forward: rho = sum g, u = j / rho, m = Pi / rho,
+// m' = (1 - w) m + w u u, fo_k = w_k rho A_k with A_k = 1 + 3 c.u + 4.5 m'_xx Hxx
+// + 4.5 m'_yy Hyy + 9 m'_xy Hxy.
+__global__ void adjoint_bulk(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    const int nx = p.L.nx, ny = p.L.ny;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nx * ny) return;
+    const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
+    if (!p.xper && (i == 1 || i == nx)) return;            // edge columns: adjoint_edge
+    const int cls = node_class(p, i, j);
+    if (cls >= 0) return;                                  // curved-wall node: adjoint_wall
+    double g[Q], lam[Q];
+    gather(p, i, j, g);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) lam[k] = a.lam_in[p.L.at(i, j, k)];
+    const fp64::Mac m = fp64::moments(g, p.hm, p.hp);
+    const bool u_zero = cls == CLS_SOLID && p.zero_solid_u;
+    const double ux = u_zero ? 0.0 : m.ux, uy = u_zero ? 0.0 : m.uy;
+    const double om = p.omega, om1 = p.omega1;
+    const double mxx = om1 * m.mxx + om * ux * ux, myy = om1 * m.myy + om * uy * uy, mxy = om1 * m.mxy + om * ux * uy;
+    double rb = 0.0, uxb = 0.0, uyb = 0.0, mxxb = 0.0, myyb = 0.0, mxyb = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double hxx = ex(k) != 0 ? p.hp : p.hm, hyy = ey(k) != 0 ? p.hp : p.hm, hxy = (double)(ex(k) * ey(k));
+        const double A = 1.0 + 3.0 * (ex(k) * ux + ey(k) * uy) + 4.5 * mxx * hxx + 4.5 * myy * hyy + 9.0 * mxy * hxy;
+        rb += lam[k] * p.w[k] * A;
+        const double Ab = lam[k] * p.w[k] * m.rho;
+        uxb += 3.0 * ex(k) * Ab;
+        uyb += 3.0 * ey(k) * Ab;
+        mxxb += 4.5 * hxx * Ab;
+        myyb += 4.5 * hyy * Ab;
+        mxyb += 9.0 * hxy * Ab;
+    }
+    // collision: m' = (1 - w) m + w u u
+    uxb += om * (2.0 * ux * mxxb + uy * mxyb);
+    uyb += om * (2.0 * uy * myyb + ux * mxyb);
+    mxxb *= om1;
+    myyb *= om1;
+    mxyb *= om1;
+    if (u_zero) { uxb = 0.0; uyb = 0.0; }
+    const double inv = 1.0 / m.rho;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double hxx = ex(k) != 0 ? p.hp : p.hm, hyy = ey(k) != 0 ? p.hp : p.hm, hxy = (double)(ex(k) * ey(k));
+        const double mu = rb + inv * (uxb * (ex(k) - m.ux) + uyb * (ey(k) - m.uy) + mxxb * (hxx - m.mxx) +
+                                      myyb * (hyy - m.myy) + mxyb * (hxy - m.mxy));
+        scatter(p, a, i, j, k, mu);
+    }
+    if (p.body) body_grad(p, a, i, j, lam);
+}
+
+// Edge columns: thread (e, q), e over the 2 ny nodes of columns 1 and nx, q over 18 inputs:
+// own inputs 0..8; at the outlet the copied neighbour's inputs 9..17; at the inlet q = 9 is u_in(j).
+__global__ void adjoint_edge(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)a.n_edge * 18) return;
+    const int e = (int)(t / 18), q = (int)(t % 18);
+    const int ny = p.L.ny, nx = p.L.nx;
+    const int i = e < ny ? 1 : nx, j = 1 + (e < ny ? e : e - ny);
+    const bool inlet = i == 1;
+    if (inlet && q > 9) return;
+    double g[Q], gn[Q];
+    gather(p, i, j, g);
+    if (!inlet) gather(p, nx - 1, j, gn);
+    Dual f[Q], fn[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        f[k] = Dual(g[k], q == k ? 1.0 : 0.0);
+        fn[k] = Dual(inlet ? 0.0 : gn[k], (!inlet && q == 9 + k) ? 1.0 : 0.0);
+    }
+    const double u0 = p.u_in ? p.u_in[j - 1] : p.uinlet;
+    const Dual uin(u0, (inlet && q == 9) ? 1.0 : 0.0);
+    Dual fo[Q];
+    edge_map(p, i, f, fn, uin, fo);
+    double lam[Q], c = 0.0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        lam[k] = a.lam_in[p.L.at(i, j, k)];
+        c += lam[k] * fo[k].d;
+    }
+    if (q < 9) scatter(p, a, i, j, q, c);
+    else if (!inlet) scatter(p, a, nx - 1, j, q - 9, c);
+    else if (a.grad_uin) a.grad_uin[j - 1] += c;
+    if (q == 0 && p.body) body_grad(p, a, i, j, lam);
+}
+
+// Curved-wall nodes: thread (l, q), q over the node's 9 own inputs and 72 stencil inputs.
+__global__ void adjoint_wall(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= (int64_t)p.nb * 81) return;
+    const int l = (int)(t / 81), q = (int)(t % 81);
+    const int i = gi(p, I_NODEI, l), j = gi(p, I_NODEJ, l);
+    double g[Q];
+    gather(p, i, j, g);
+    Dual f[Q], fs[8 * Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) f[k] = Dual(g[k], q == k ? 1.0 : 0.0);
+    for (int s = 0; s < 8; ++s) {
+        double h[Q];
+        gather(p, gi(p, I_SI + s, l), gi(p, I_SJ + s, l), h);
+#pragma unroll
+        for (int k = 0; k < Q; ++k) fs[Q * s + k] = Dual(h[k], q == 9 + Q * s + k ? 1.0 : 0.0);
+    }
+    Dual fo[Q], drag;
+    wall_map(p, l, f, fs, fo, drag);
+    double c = a.wJ * drag.d;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) c += a.lam_in[p.L.at(i, j, k)] * fo[k].d;
+    if (q < 9) scatter(p, a, i, j, q, c);
+    else {
+        const int s = (q - 9) / Q, k = (q - 9) % Q;
+        scatter(p, a, gi(p, I_SI + s, l), gi(p, I_SJ + s, l), k, c);
+    }
+}
+
+}  // namespace adj
+}  // namespace mrlbm

@@ -1,0 +1,23 @@
+// adjoint.h -- host interface of the adjoint step kernels (adjoint.cuh, launched from step_f64.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "step_params.h"
+
+namespace mrlbm {
+namespace adj {
+
+struct AdjArgs {
+    const double* lam_in;      // lambda^n = dJ/dF^n, padded layout
+    double* lam_out;           // lambda^{n-1}, padded layout, zeroed before the step
+    double* grad_body;         // [2 N] accumulated dJ/d(body force), or null
+    double* grad_uin;          // [ny] accumulated dJ/d(u_in), or null
+    double wJ;                 // weight of this step's drag in J (1/T inside the window, else 0)
+    int n_edge;                // edge-column nodes: 2 ny
+};
+
+}  // namespace adj
+
+// One adjoint step: p describes forward step n (src = F^{n-1}); lambda^{n-1} must be zero.
+int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s);
+
+}  // namespace mrlbm

@@ -14,6 +14,7 @@
 
 #include "../../include/mrlbm.h"
 #include "geometry.h"
+#include "adjoint.h"
 #include "batch_params.h"
 #include "noalloc.h"
 #include "state_io.h"
@@ -51,6 +52,8 @@ struct mrlbm_handle {
     double* d_macro = nullptr;
     double* d_uin = nullptr;
     bool has_uin = false;
+    void* d_body = nullptr;                   // 2 x N body force (T), or null
+    bool has_body = false;
     double* h_ring = nullptr;                 // pinned
     std::vector<double> hist;                 // drained records, REC_WORDS each
     int iter = 0;
@@ -311,6 +314,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.src = (const double*)h->buf[h->cur];
         p.dst = (double*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? h->d_uin : nullptr;
+        p.body = h->has_body ? (const double*)h->d_body : nullptr;
         p.ovr = h->ovr_live ? h->d_ovr : nullptr;
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         p.zero_solid_u = plot;
@@ -331,6 +335,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.src = (const float*)h->buf[h->cur];
         p.dst = (float*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? (const float*)h->d_uin : nullptr;
+        p.body = h->has_body ? (const float*)h->d_body : nullptr;
         p.ovr = h->ovr_live ? h->d_ovr : nullptr;
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         p.zero_solid_u = plot;
@@ -371,7 +376,7 @@ void free_all(mrlbm_handle* h) {
     if (h->host_only) return;
     cudaSetDevice(h->device);
     for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
-                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, (void*)h->d_ovr, (void*)h->d_fstage,
+                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, h->d_body, (void*)h->d_ovr, (void*)h->d_fstage,
                     (void*)h->d_tile_ctr, (void*)h->d_fstat, (void*)h->d_fstat_out})
         if (p) cudaFree(p);
     if (h->h_ring) cudaFreeHost(h->h_ring);
@@ -646,6 +651,25 @@ int mrlbm_set_inlet_profile(mrlbm_handle* h, const double* u_in) {
     return MRLBM_OK;
 }
 
+int mrlbm_set_body_force(mrlbm_handle* h, const double* g) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    if (!g) { h->has_body = false; return MRLBM_OK; }
+    const size_t n2 = (size_t)2 * h->L.nx * h->L.ny;
+    if (!h->d_body) CK(cudaMalloc(&h->d_body, n2 * h->elem));
+    if (h->precision == MRLBM_FP64) {
+        CK(cudaMemcpyAsync(h->d_body, g, n2 * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    } else {
+        std::vector<float> t(g, g + n2);
+        CK(cudaMemcpyAsync(h->d_body, t.data(), n2 * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->has_body = true;
+    return MRLBM_OK;
+}
+
 int mrlbm_step(mrlbm_handle* h, int32_t nsteps, int32_t flags) {
     if (!h || nsteps < 0) return MRLBM_EINVAL;
     if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
@@ -866,6 +890,145 @@ int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n) {
 
 }  // extern "C"
 
+
+// ---- adjoint of the mean drag -------------------------------------------------------------
+
+namespace {
+
+// One forward FP64 step from src into dst at iteration `iter` (drag record into rec if given).
+int adj_forward(mrlbm_handle* h, const double* src, double* dst, int iter, double* rec, bool ovr, int tile) {
+    StepParams<double> p{};
+    fill_common(h, p);
+    const mrlbm_config& c = h->cfg;
+    p.src = src;
+    p.dst = dst;
+    p.u_in = h->has_uin ? h->d_uin : nullptr;
+    p.body = h->has_body ? (const double*)h->d_body : nullptr;
+    p.ovr = ovr ? h->d_ovr : nullptr;
+    p.n_ovr = ovr ? (int)h->ovr.size() : 0;
+    p.zero_solid_u = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
+    p.do_stats = rec != nullptr;
+    p.rec = rec;
+    p.iter = iter;
+    ++h->launches;
+    return launch_step_f64(p, tile, h->stream, 0);
+}
+
+}  // namespace
+
+extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t window, int32_t checkpoint_every,
+                                  double* J, double* grad_body, double* grad_uin) {
+    if (!h || nsteps < 1 || window < 1 || window > nsteps || checkpoint_every < 1 || !J) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    const mrlbm_config& c = h->cfg;
+    if (h->precision != MRLBM_FP64) return fail(h, MRLBM_EUNSUPPORTED, "the adjoint runs on FP64 handles");
+    if (c.x_periodic || (c.wall_mode == MRLBM_WALL_REFERENCE && !c.y_periodic) || c.incomp_bc || c.incomp_bulk ||
+        (h->geo.nb > 0 && (h->closure != CLOSURE_STRONG || !c.vel_interp || !c.mom_interp)))
+        return fail(h, MRLBM_EUNSUPPORTED,
+                    "adjoint: needs inlet/outlet columns, free-slip or y-periodic walls and the rotated strong closure");
+    CK(cudaSetDevice(h->device));
+    int rc = drain_ring(h);
+    if (rc != MRLBM_OK) return rc;
+    const int N = nsteps, K = std::min(checkpoint_every, nsteps), T = window;
+    const int ncp = (N + K - 1) / K;
+    const size_t LB = (size_t)h->L.total() * sizeof(double);
+    const int64_t nodes = (int64_t)h->L.nx * h->L.ny;
+    const int tile = is_tma_cfg(h->tile_cfg) ? 1 : h->tile_cfg;
+    const bool grads = grad_body || grad_uin;
+    std::vector<double*> cp(ncp, nullptr), seg(grads ? K : 0, nullptr);
+    double *work[2] = {nullptr, nullptr}, *lam[2] = {nullptr, nullptr}, *d_rec = nullptr, *gb = nullptr, *gu = nullptr;
+    auto release = [&]() {
+        for (double* q : cp) if (q) cudaFree(q);
+        for (size_t q = 1; q < seg.size(); ++q) if (seg[q]) cudaFree(seg[q]);   // seg[0] borrows a checkpoint
+        for (double* q : {work[0], work[1], lam[0], lam[1], d_rec, gb, gu}) if (q) cudaFree(q);
+    };
+    auto alloc_level = [&](double** q) {
+        if (cudaMalloc((void**)q, LB) != cudaSuccess) return false;
+        // every level carries the never-written ghost values of the current state
+        return cudaMemcpyAsync(*q, h->buf[h->cur], LB, cudaMemcpyDeviceToDevice, h->stream) == cudaSuccess;
+    };
+    bool ok = true;
+    for (int q = 0; q < ncp && ok; ++q) ok = alloc_level(&cp[q]);
+    for (int q = 1; q < (int)seg.size() && ok; ++q) ok = alloc_level(&seg[q]);
+    ok = ok && alloc_level(&work[0]) && alloc_level(&work[1]) &&
+         cudaMalloc((void**)&d_rec, (size_t)N * REC_WORDS * sizeof(double)) == cudaSuccess;
+    if (ok && grads)
+        ok = cudaMalloc((void**)&lam[0], LB) == cudaSuccess && cudaMalloc((void**)&lam[1], LB) == cudaSuccess &&
+             cudaMalloc((void**)&gb, (size_t)2 * nodes * sizeof(double)) == cudaSuccess &&
+             cudaMalloc((void**)&gu, (size_t)h->L.ny * sizeof(double)) == cudaSuccess &&
+             cudaMemsetAsync(lam[0], 0, LB, h->stream) == cudaSuccess &&
+             cudaMemsetAsync(gb, 0, (size_t)2 * nodes * sizeof(double), h->stream) == cudaSuccess &&
+             cudaMemsetAsync(gu, 0, (size_t)h->L.ny * sizeof(double), h->stream) == cudaSuccess;
+    if (!ok) {
+        release();
+        cudaGetLastError();
+        return fail(h, MRLBM_ECUDA, "adjoint: device memory for checkpoints and adjoint fields");
+    }
+    const int it0 = h->iter;
+    // forward pass: F^0 .. F^N, checkpoint F^{cK}, drag records of the window
+    const double* prev = cp[0];
+    for (int n = 1; n <= N && rc == MRLBM_OK; ++n) {
+        double* dst = work[n & 1];
+        double* rec = n > N - T ? d_rec + (size_t)(n - 1) * REC_WORDS : nullptr;
+        if (adj_forward(h, prev, dst, it0 + n, rec, n == 1 && h->ovr_live, tile) != 0) rc = MRLBM_ECUDA;
+        if (n % K == 0 && n / K < ncp && cudaMemcpyAsync(cp[n / K], dst, LB, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+            rc = MRLBM_ECUDA;
+        prev = dst;
+    }
+    std::vector<double> recs((size_t)N * REC_WORDS);
+    if (rc == MRLBM_OK &&
+        (cudaMemcpyAsync(recs.data(), d_rec, recs.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+         cudaStreamSynchronize(h->stream) != cudaSuccess))
+        rc = MRLBM_ECUDA;
+    if (rc == MRLBM_OK) {
+        double acc = 0.0;
+        for (int n = N - T + 1; n <= N; ++n) acc = acc + recs[(size_t)(n - 1) * REC_WORDS + 1];
+        *J = acc / T;
+    }
+    // backward pass, segment by segment from the last checkpoint
+    int li = 0;
+    for (int cseg = ncp - 1; grads && cseg >= 0 && rc == MRLBM_OK; --cseg) {
+        const int n0 = cseg * K, m = std::min(K, N - n0);
+        seg[0] = cp[cseg];
+        for (int t = 1; t < m && rc == MRLBM_OK; ++t)
+            if (adj_forward(h, seg[t - 1], seg[t], it0 + n0 + t, nullptr, n0 + t == 1 && h->ovr_live, tile) != 0) rc = MRLBM_ECUDA;
+        for (int n = n0 + m; n > n0 && rc == MRLBM_OK; --n) {
+            const int t = n - n0 - 1;                  // seg[t] = F^{n-1}
+            if (cudaMemsetAsync(lam[li ^ 1], 0, LB, h->stream) != cudaSuccess) { rc = MRLBM_ECUDA; break; }
+            StepParams<double> p{};
+            fill_common(h, p);
+            p.src = seg[t];
+            p.u_in = h->has_uin ? h->d_uin : nullptr;
+            p.body = h->has_body ? (const double*)h->d_body : nullptr;
+            p.ovr = (n == 1 && h->ovr_live) ? h->d_ovr : nullptr;
+            p.n_ovr = p.ovr ? (int)h->ovr.size() : 0;
+            const int iter = it0 + n;
+            p.zero_solid_u = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
+            p.iter = iter;
+            adj::AdjArgs a{};
+            a.lam_in = lam[li];
+            a.lam_out = lam[li ^ 1];
+            a.grad_body = gb;
+            a.grad_uin = gu;
+            a.wJ = n > N - T ? 1.0 / T : 0.0;
+            a.n_edge = 2 * h->L.ny;
+            h->launches += 3;
+            if (launch_adjoint_step(p, a, h->stream) != 0) rc = MRLBM_ECUDA;
+            li ^= 1;
+        }
+    }
+    if (rc == MRLBM_OK && grads) {
+        if (grad_body && cudaMemcpyAsync(grad_body, gb, (size_t)2 * nodes * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+            rc = MRLBM_ECUDA;
+        if (grad_uin && cudaMemcpyAsync(grad_uin, gu, (size_t)h->L.ny * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+            rc = MRLBM_ECUDA;
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = MRLBM_ECUDA;
+    release();
+    if (rc != MRLBM_OK) return fail(h, rc, std::string("adjoint: ") + cudaGetErrorString(cudaGetLastError()));
+    return MRLBM_OK;
+}
+
 // ---- batched cases ----------------------------------------------------------------------
 
 struct mrlbm_batch {
@@ -936,6 +1099,7 @@ void batch_fill(mrlbm_batch* b, unsigned char* stage, int want_macro) {
         p.src = (const T*)h->buf[h->cur];
         p.dst = (T*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? (const T*)h->d_uin : nullptr;
+        p.body = h->has_body ? (const T*)h->d_body : nullptr;
         p.ovr = h->ovr_live ? h->d_ovr : nullptr;
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         int aux, tiles;

@@ -72,6 +72,25 @@ __device__ __forceinline__ void accumulate_fields(const StepParams<T>& p, int i,
     a[5 * N] = __dadd_rn(a[5 * N], __dmul_rn(pr, pr));
 }
 
+// Body force (an extension: the reference has no forcing term).  A first-order momentum
+// source added to the post-collision populations, fout_k += 3 w_k (c_k . g): it adds g to the
+// node's momentum each step and leaves its mass unchanged.  Applied at bulk and edge nodes,
+// not at curved-wall nodes.  In the FP32 form the same term is added to the deviations.
+template <class T>
+__device__ __forceinline__ void add_body_force(const StepParams<T>& p, int i, int j, T fo[Q]) {
+    const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1);
+    const T fx = T(3) * p.body[n], fy = T(3) * p.body[(int64_t)p.L.nx * p.L.ny + n];
+    const T w1 = p.w[1], w5 = p.w[5];
+    fo[1] = fo[1] + w1 * fx;
+    fo[3] = fo[3] - w1 * fx;
+    fo[2] = fo[2] + w1 * fy;
+    fo[4] = fo[4] - w1 * fy;
+    fo[5] = fo[5] + w5 * (fx + fy);
+    fo[7] = fo[7] - w5 * (fx + fy);
+    fo[6] = fo[6] + w5 * (fy - fx);
+    fo[8] = fo[8] - w5 * (fy - fx);
+}
+
 // Node class inside the cylinder box: CLS_FLUID, CLS_SOLID or a boundary-node index.
 template <class T>
 __device__ __forceinline__ int node_class(const StepParams<T>& p, int i, int j) {

@@ -3,6 +3,7 @@
 #include "step_fp64.cuh"
 #include "step_tma.cuh"
 #include "step_batch.cuh"
+#include "adjoint.cuh"
 
 namespace mrlbm {
 
@@ -59,6 +60,15 @@ int batch_blocks_per_sm_f64(int tile_cfg) {
 #undef MRLBM_VEC_CASE
     default: return 0;
     }
+}
+
+// Adjoint step (adjoint.cuh): bulk nodes, edge columns, curved-wall nodes.
+int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s) {
+    const int64_t nodes = (int64_t)p.L.nx * p.L.ny;
+    adj::adjoint_bulk<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(p, a);
+    if (a.n_edge > 0) adj::adjoint_edge<<<(unsigned)((a.n_edge * 18 + 127) / 128), 128, 0, s>>>(p, a);
+    if (p.nb > 0) adj::adjoint_wall<<<(unsigned)((p.nb * 81 + 127) / 128), 128, 0, s>>>(p, a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace mrlbm

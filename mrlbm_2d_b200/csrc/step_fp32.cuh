@@ -272,6 +272,7 @@ __device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls)
     if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     float go[Q];
     collide(p, m, go);
+    if (p.body) add_body_force(p, i, j, go);
     store(p, i, j, go);
     return 1.0 + (double)m.drho;
 }
@@ -284,6 +285,7 @@ __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     collide(p, m, go);
+    if (p.body) add_body_force(p, i, j, go);
 }
 
 __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const float g[Q]) {

@@ -399,6 +399,7 @@ __device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls)
     if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     double fo[Q];
     collide(p, m, fo);
+    if (p.body) add_body_force(p, i, j, fo);
     store(p, i, j, fo);
     return m.rho;
 }
@@ -412,6 +413,7 @@ __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     collide(p, m, fo);
+    if (p.body) add_body_force(p, i, j, fo);
 }
 
 __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const double f[Q]) {

@@ -76,6 +76,7 @@ struct alignas(64) StepParams {
     // optional macroscopic output (Fortran order nx*ny): rho, ux, uy, mxx, myy, mxy
     double* macro;                // [6 * nx * ny] or null
     double* fstat;                // [6 * nx * ny] running sums of u, v, p, u^2, v^2, p^2, or null
+    const T* body;                // [2 * nx * ny] body force (x then y), node order, or null
     int tiles_x;                  // bulk tiles along x
     DevConsts dc;                 // deviation-form constants (FP32 only)
 };

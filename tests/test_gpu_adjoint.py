@@ -1,0 +1,141 @@
+"""Adjoint of mean drag: gradient w.r.t. a per-node body force and the inlet profile, checked
+against central finite differences of the FP64 forward run, plus the body-force forward term
+and the torch.autograd bridge."""
+import numpy as np
+import pytest
+
+from cases import CASES
+from mrlbm_2d_b200.config import cylinder_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _case():
+    # 96 x 32 channel, D = 8 at (24, 16.5): curved wall with label-15 poles, free-slip walls
+    return cylinder_case(96, 32, 8, 24.0, 16.5, 100.0, 0.05, seed=11, noise=1e-2)
+
+
+def _params(sim, seed):
+    rng = np.random.default_rng(seed)
+    body = 1e-5 * rng.standard_normal((2, sim.nx, sim.ny))
+    uin = 0.05 + 1e-3 * rng.standard_normal(sim.ny)
+    return body, uin
+
+
+def test_body_force_adds_its_momentum(mrlbm):
+    """A uniform body force g adds g per node and step to the momentum (the run without the
+    force is subtracted; the reference's periodic corner wraps duplicate a few populations, so
+    the balance holds to 1e-3) and leaves the mass unchanged."""
+    cfg = CASES["periodic_channel_no_cylinder"]()
+    ex = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1])
+    ey = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1])
+    out = []
+    for force in (False, True):
+        s = mrlbm.Simulation(cfg)
+        if force:
+            g = np.zeros((2, s.nx, s.ny))
+            g[0] = 2e-6
+            g[1] = -1e-6
+            s.set_body_force(g)
+        s.step(10)
+        f = s.get_state()
+        out.append(((f * ex).sum(), (f * ey).sum(), f.sum()))
+        nodes = s.nx * s.ny
+        s.close()
+    for c, gc in ((0, 2e-6), (1, -1e-6)):
+        dm = out[1][c] - out[0][c]
+        assert abs(dm - 10 * gc * nodes) < 1e-3 * abs(10 * gc * nodes)
+    assert abs(out[1][2] - out[0][2]) < 1e-10 * out[0][2]
+
+
+def test_adjoint_objective_is_the_forward_mean_drag(mrlbm):
+    s = mrlbm.Simulation(_case())
+    body, uin = _params(s, 1)
+    s.set_body_force(body)
+    s.set_inlet_profile(uin)
+    J = s.adjoint_drag(120, 50, 40, grads=False)
+    assert s.iter == 1                               # the handle is not advanced
+    s.step(120)
+    it, fd, fl, _ = s.forces()
+    acc = 0.0
+    for v in fd[-50:]:
+        acc = acc + v
+    assert J == acc / 50
+    s.close()
+
+
+@pytest.mark.parametrize("K", [37, 1000])
+def test_adjoint_matches_central_differences(mrlbm, K):
+    s = mrlbm.Simulation(_case())
+    body, uin = _params(s, 2)
+    s.set_body_force(body)
+    s.set_inlet_profile(uin)
+    N, T = 200, 80
+    J, gb, gu = s.adjoint_drag(N, T, K)
+    assert np.all(np.isfinite(gb)) and np.all(np.isfinite(gu))
+    rng = np.random.default_rng(5)
+    for _ in range(4):
+        db = 1e-5 * rng.standard_normal(body.shape)
+        du = 1e-3 * rng.standard_normal(uin.shape)
+        eps = 1e-4
+        vals = []
+        for sgn in (1.0, -1.0):
+            s.set_body_force(body + sgn * eps * db)
+            s.set_inlet_profile(uin + sgn * eps * du)
+            vals.append(s.adjoint_drag(N, T, K, grads=False))
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        ad = float((gb * db).sum() + (gu * du).sum())
+        assert abs(ad - fd) <= 1e-3 * abs(fd) + 1e-15, (ad, fd)
+        # each block separately too
+        for part in ("body", "inlet"):
+            vals = []
+            for sgn in (1.0, -1.0):
+                s.set_body_force(body + (sgn * eps * db if part == "body" else 0.0))
+                s.set_inlet_profile(uin + (sgn * eps * du if part == "inlet" else 0.0))
+                vals.append(s.adjoint_drag(N, T, K, grads=False))
+            fdp = (vals[0] - vals[1]) / (2 * eps)
+            adp = float((gb * db).sum()) if part == "body" else float((gu * du).sum())
+            assert abs(adp - fdp) <= 1e-3 * abs(fdp) + 1e-15, (part, adp, fdp)
+    s.set_body_force(body)
+    s.set_inlet_profile(uin)
+    s.close()
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(mrlbm):
+    s = mrlbm.Simulation(_case())
+    body, uin = _params(s, 3)
+    s.set_body_force(body)
+    s.set_inlet_profile(uin)
+    J1, gb1, gu1 = s.adjoint_drag(150, 60, 7)
+    J2, gb2, gu2 = s.adjoint_drag(150, 60, 150)
+    assert J1 == J2
+    assert np.abs(gb1 - gb2).max() <= 1e-10 * np.abs(gb1).max()
+    assert np.abs(gu1 - gu2).max() <= 1e-10 * np.abs(gu1).max()
+    s.close()
+
+
+def test_torch_autograd_bridge(mrlbm):
+    torch = pytest.importorskip("torch")
+    from mrlbm_2d_b200.autograd import mean_drag
+    s = mrlbm.Simulation(_case())
+    body, uin = _params(s, 4)
+    b = torch.tensor(body, requires_grad=True)
+    u = torch.tensor(uin, requires_grad=True)
+    J = mean_drag(s, b, u, 100, 40, 25)
+    (2.0 * J).backward()
+    J0, gb, gu = s.adjoint_drag(100, 40, 25)
+    assert float(J) == J0
+    assert np.allclose(b.grad.numpy(), 2.0 * gb, rtol=1e-10, atol=1e-14 * np.abs(gb).max())
+    assert np.allclose(u.grad.numpy(), 2.0 * gu, rtol=1e-10, atol=1e-14 * np.abs(gu).max())
+    s.close()
+
+
+def test_adjoint_rejects_unsupported_cases(mrlbm):
+    s = mrlbm.Simulation(_case(), precision=32)
+    with pytest.raises(mrlbm.MrlbmError):
+        s.adjoint_drag(10, 5, 5)
+    s.close()
+    s = mrlbm.Simulation(CASES["freeslip_xperiodic"]())
+    with pytest.raises(mrlbm.MrlbmError):
+        s.adjoint_drag(10, 5, 5)
+    s.close()
