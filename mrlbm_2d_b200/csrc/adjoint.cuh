@@ -7,9 +7,10 @@
 // adjoint field lambda^n = dJ/dF^n obeys
 //     lambda^{n-1}(slot) = sum over the consumers x of the slot of (dC_x/dg_x)^T lambda^n(x)
 //                          + w_n dD^n/dF^{n-1}(slot),      w_n = 1/T inside the window,
-// and the parameter gradients collect (dC_x/dtheta)^T lambda^n(x).  One adjoint step runs
-// three kernels, each node's contribution added atomically to lambda^{n-1} at the slots it
-// pulled (a slot can feed several nodes: stencils, the outlet copy, corner wraps):
+// and the parameter gradients collect (dC_x/dtheta)^T lambda^n(x).  One adjoint step is one
+// launch with three kinds of blocks, each node's contribution added atomically to
+// lambda^{n-1} at the slots it pulled (a slot can feed several nodes: stencils, the outlet
+// copy, corner wraps):
 //   * bulk nodes (fluid and solid, not edge columns, not curved-wall nodes): reverse mode
 //     written out by hand: reconstruction -> collision -> moments (adjoint_bulk_node);
 //   * edge columns (inlet i = 1, outlet i = nx): one thread per (node, input), the node's
@@ -163,12 +164,24 @@ __device__ __forceinline__ void edge_map(const P& p, int i, const S f[Q], const 
 __device__ __forceinline__ double gf(const P& p, int field, int l) { return __ldg(p.bgeo + (int64_t)field * p.nb + l); }
 __device__ __forceinline__ int gi(const P& p, int field, int l) { return __ldg(p.bint + (int64_t)field * p.nb + l); }
 
-// Curved-wall node l: stencil moments, bilinear interpolation at reference points 2 and 3,
-// extrapolation to the node, rotated strong closure, collision (2d_mrlbm.f90:294-311,
-// 768-928, 1635-1765, 407-457) and the node's drag term (2d_mrlbm.f90:558-591).
-// f: own inputs; fs: the 8 stencil nodes' inputs (stencil s at fs[9 s .. 9 s + 8]).
+// Rotated velocity and second moments of one bilinear stencil node (2d_mrlbm.f90:842-867).
 template <class S>
-__device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const S fs[8 * Q], S fo[Q], S& drag) {
+__device__ __forceinline__ void stencil_quad(const P& p, int l, int s, const S f[Q], S& u, S& v, S& mx, S& my) {
+    const MacS<S> m = moments_s(f, p.hm, p.hp);
+    const double c2 = gf(p, G_SCC + s, l), s2q = gf(p, G_SSS + s, l), sn2 = gf(p, G_SS2 + s, l);
+    u = m.ux;
+    v = m.uy;
+    mx = m.mxx * c2 + m.myy * s2q + m.mxy * sn2;
+    my = m.mxx * s2q + m.myy * c2 - m.mxy * sn2;
+}
+
+// Curved-wall node l from its own inputs f and its 8 stencil nodes' (u, v, mx, my): bilinear
+// interpolation at reference points 2 and 3, extrapolation to the node, rotated strong
+// closure, collision (2d_mrlbm.f90:294-311, 768-928, 1635-1765, 407-457) and the node's drag
+// term (2d_mrlbm.f90:558-591).
+template <class S>
+__device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const S su[8], const S sv[8], const S smx[8],
+                                         const S smy[8], S fo[Q], S& drag) {
     S u[2], v[2], mx[2], my[2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
@@ -176,21 +189,11 @@ __device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const 
         S row_u[2], row_v[2], row_mx[2], row_my[2];
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr) {
-            S su = 0.0, sv = 0.0, smx = 0.0, smy = 0.0;
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const int s = 4 * r + 2 * rr + cc;
-                const MacS<S> m = moments_s(fs + Q * s, p.hm, p.hp);
-                const double c2 = gf(p, G_SCC + s, l), s2q = gf(p, G_SSS + s, l), sn2 = gf(p, G_SS2 + s, l);
-                const S rmx = m.mxx * c2 + m.myy * s2q + m.mxy * sn2;
-                const S rmy = m.mxx * s2q + m.myy * c2 - m.mxy * sn2;
-                const double wx = cc ? xd : (1.0 - xd);
-                su = su + wx * m.ux;
-                sv = sv + wx * m.uy;
-                smx = smx + wx * rmx;
-                smy = smy + wx * rmy;
-            }
-            row_u[rr] = su; row_v[rr] = sv; row_mx[rr] = smx; row_my[rr] = smy;
+            const int s0 = 4 * r + 2 * rr;
+            row_u[rr] = (1.0 - xd) * su[s0] + xd * su[s0 + 1];
+            row_v[rr] = (1.0 - xd) * sv[s0] + xd * sv[s0 + 1];
+            row_mx[rr] = (1.0 - xd) * smx[s0] + xd * smx[s0 + 1];
+            row_my[rr] = (1.0 - xd) * smy[s0] + xd * smy[s0 + 1];
         }
         u[r] = (1.0 - yd) * row_u[0] + yd * row_u[1];
         v[r] = (1.0 - yd) * row_v[0] + yd * row_v[1];
@@ -278,9 +281,8 @@ __device__ __forceinline__ void body_grad(const P& p, const AdjArgs& a, int i, i
 // Bulk node, reverse mode by hand.  Forward: rho = sum g, u = j / rho, m = Pi / rho,
 // m' = (1 - w) m + w u u, fo_k = w_k rho A_k with A_k = 1 + 3 c.u + 4.5 m'_xx Hxx
 // + 4.5 m'_yy Hyy + 9 m'_xy Hxy.
-__global__ void adjoint_bulk(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+__device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int64_t t) {
     const int nx = p.L.nx, ny = p.L.ny;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= (int64_t)nx * ny) return;
     const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
     if (!p.xper && (i == 1 || i == nx)) return;            // edge columns: adjoint_edge
@@ -289,7 +291,11 @@ __global__ void adjoint_bulk(const __grid_constant__ P p, const __grid_constant_
     double g[Q], lam[Q];
     gather(p, i, j, g);
 #pragma unroll
-    for (int k = 0; k < Q; ++k) lam[k] = a.lam_in[p.L.at(i, j, k)];
+    for (int k = 0; k < Q; ++k) {
+        const int64_t at = p.L.at(i, j, k);
+        lam[k] = a.lam_in[at];
+        a.lam_in[at] = 0.0;                      // read once: the buffer becomes step n-2's target
+    }
     const fp64::Mac m = fp64::moments(g, p.hm, p.hp);
     const bool u_zero = cls == CLS_SOLID && p.zero_solid_u;
     const double ux = u_zero ? 0.0 : m.ux, uy = u_zero ? 0.0 : m.uy;
@@ -328,10 +334,8 @@ __global__ void adjoint_bulk(const __grid_constant__ P p, const __grid_constant_
 
 // Edge columns: thread (e, q), e over the 2 ny nodes of columns 1 and nx, q over 18 inputs:
 // own inputs 0..8; at the outlet the copied neighbour's inputs 9..17; at the inlet q = 9 is u_in(j).
-__global__ void adjoint_edge(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)a.n_edge * 18) return;
-    const int e = (int)(t / 18), q = (int)(t % 18);
+__device__ __forceinline__ void adjoint_edge(const P& p, const AdjArgs& a, int e, int q, const double* lam) {
+    if (e >= a.n_edge) return;
     const int ny = p.L.ny, nx = p.L.nx;
     const int i = e < ny ? 1 : nx, j = 1 + (e < ny ? e : e - ny);
     const bool inlet = i == 1;
@@ -349,45 +353,103 @@ __global__ void adjoint_edge(const __grid_constant__ P p, const __grid_constant_
     const Dual uin(u0, (inlet && q == 9) ? 1.0 : 0.0);
     Dual fo[Q];
     edge_map(p, i, f, fn, uin, fo);
-    double lam[Q], c = 0.0;
+    double c = 0.0;
 #pragma unroll
-    for (int k = 0; k < Q; ++k) {
-        lam[k] = a.lam_in[p.L.at(i, j, k)];
-        c += lam[k] * fo[k].d;
-    }
+    for (int k = 0; k < Q; ++k) c += lam[k] * fo[k].d;
     if (q < 9) scatter(p, a, i, j, q, c);
     else if (!inlet) scatter(p, a, nx - 1, j, q - 9, c);
     else if (a.grad_uin) a.grad_uin[j - 1] += c;
     if (q == 0 && p.body) body_grad(p, a, i, j, lam);
 }
 
-// Curved-wall nodes: thread (l, q), q over the node's 9 own inputs and 72 stencil inputs.
-__global__ void adjoint_wall(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= (int64_t)p.nb * 81) return;
-    const int l = (int)(t / 81), q = (int)(t % 81);
+// Curved-wall node l, one block: the block stages the node's 81 inputs (9 own, 9 for each of
+// its 8 stencil nodes) and the stencil quantities in shared memory; thread q < 81 then runs
+// the node's map with the derivative along input q (only its stencil node's quantities carry
+// a derivative) and scatters the contracted column.
+__device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l) {
+    __shared__ double in[81], lam[Q], qd[4][8];
+    __shared__ int slot[81];
+    const int q = threadIdx.x;
     const int i = gi(p, I_NODEI, l), j = gi(p, I_NODEJ, l);
-    double g[Q];
-    gather(p, i, j, g);
-    Dual f[Q], fs[8 * Q];
+    if (q < 81) {
+        int ni = i, nj = j, k = q;
+        if (q >= 9) {
+            const int s = (q - 9) / Q;
+            ni = gi(p, I_SI + s, l);
+            nj = gi(p, I_SJ + s, l);
+            k = (q - 9) % Q;
+        }
+        const SrcSlot sl = stream_source(p.L.nx, p.L.ny, ni, nj, k, p.xper, p.yper, p.freeslip);
+        const int64_t at = p.L.at(sl.i, sl.j, sl.k);
+        in[q] = __ldg(p.src + at);
+        const bool ghost = sl.i < 1 || sl.i > p.L.nx || sl.j < 1 || sl.j > p.L.ny;
+        slot[q] = ghost ? -1 : (int)at;
+    } else if (q < 81 + Q) {
+        const int64_t at = p.L.at(i, j, q - 81);
+        lam[q - 81] = a.lam_in[at];
+        a.lam_in[at] = 0.0;                      // read once, into shared memory
+    }
+    __syncthreads();
+    if (q < 8) {
+        double f[Q], u, v, mx, my;
 #pragma unroll
-    for (int k = 0; k < Q; ++k) f[k] = Dual(g[k], q == k ? 1.0 : 0.0);
-    for (int s = 0; s < 8; ++s) {
-        double h[Q];
-        gather(p, gi(p, I_SI + s, l), gi(p, I_SJ + s, l), h);
+        for (int k = 0; k < Q; ++k) f[k] = in[9 + Q * q + k];
+        stencil_quad(p, l, q, f, u, v, mx, my);
+        qd[0][q] = u; qd[1][q] = v; qd[2][q] = mx; qd[3][q] = my;
+    }
+    __syncthreads();
+    if (q >= 81) return;
+    Dual f[Q], su[8], sv[8], smx[8], smy[8];
 #pragma unroll
-        for (int k = 0; k < Q; ++k) fs[Q * s + k] = Dual(h[k], q == 9 + Q * s + k ? 1.0 : 0.0);
+    for (int k = 0; k < Q; ++k) f[k] = Dual(in[k], q == k ? 1.0 : 0.0);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) { su[s] = qd[0][s]; sv[s] = qd[1][s]; smx[s] = qd[2][s]; smy[s] = qd[3][s]; }
+    if (q >= 9) {
+        const int s = (q - 9) / Q, kk = (q - 9) % Q;
+        Dual g[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) g[k] = Dual(in[9 + Q * s + k], k == kk ? 1.0 : 0.0);
+        Dual u, v, mx, my;
+        stencil_quad(p, l, s, g, u, v, mx, my);
+        // only stencil s depends on input q
+        for (int t = 0; t < 8; ++t)
+            if (t == s) { su[t] = u; sv[t] = v; smx[t] = mx; smy[t] = my; }
     }
     Dual fo[Q], drag;
-    wall_map(p, l, f, fs, fo, drag);
+    wall_map(p, l, f, su, sv, smx, smy, fo, drag);
     double c = a.wJ * drag.d;
 #pragma unroll
-    for (int k = 0; k < Q; ++k) c += a.lam_in[p.L.at(i, j, k)] * fo[k].d;
-    if (q < 9) scatter(p, a, i, j, q, c);
-    else {
-        const int s = (q - 9) / Q, k = (q - 9) % Q;
-        scatter(p, a, gi(p, I_SI + s, l), gi(p, I_SJ + s, l), k, c);
+    for (int k = 0; k < Q; ++k) c += lam[k] * fo[k].d;
+    if (slot[q] >= 0) atomicAdd(a.lam_out + slot[q], c);
+}
+
+// One adjoint step in one launch of 128-thread blocks: [nb wall blocks][edge blocks, 7 nodes
+// x 18 inputs each][bulk blocks, 128 nodes each].
+__global__ void __launch_bounds__(128) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    const int b = (int)blockIdx.x;
+    const int n_edge_blk = (a.n_edge + 6) / 7;
+    if (b < p.nb) {
+        adjoint_wall(p, a, b);
+        return;
     }
+    if (b < p.nb + n_edge_blk) {
+        // lambda^n of the block's 7 edge nodes, staged once and cleared for reuse
+        __shared__ double lam[7][Q];
+        const int t = threadIdx.x, e0 = 7 * (b - p.nb);
+        if (t < 7 * Q) {
+            const int e = e0 + t / Q, k = t % Q;
+            if (e < a.n_edge) {
+                const int i = e < p.L.ny ? 1 : p.L.nx, j = 1 + (e < p.L.ny ? e : e - p.L.ny);
+                const int64_t at = p.L.at(i, j, k);
+                lam[t / Q][k] = a.lam_in[at];
+                a.lam_in[at] = 0.0;
+            }
+        }
+        __syncthreads();
+        if (t < 126) adjoint_edge(p, a, e0 + t / 18, t % 18, lam[t / 18]);
+        return;
+    }
+    adjoint_bulk(p, a, (int64_t)(b - p.nb - n_edge_blk) * 128 + threadIdx.x);
 }
 
 }  // namespace adj

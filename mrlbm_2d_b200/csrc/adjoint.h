@@ -7,7 +7,7 @@ namespace mrlbm {
 namespace adj {
 
 struct AdjArgs {
-    const double* lam_in;      // lambda^n = dJ/dF^n, padded layout
+    double* lam_in;            // lambda^n = dJ/dF^n, padded layout; cleared as it is read
     double* lam_out;           // lambda^{n-1}, padded layout, zeroed before the step
     double* grad_body;         // [2 N] accumulated dJ/d(body force), or null
     double* grad_uin;          // [ny] accumulated dJ/d(u_in), or null
@@ -18,6 +18,8 @@ struct AdjArgs {
 }  // namespace adj
 
 // One adjoint step: p describes forward step n (src = F^{n-1}); lambda^{n-1} must be zero.
+// The step reads every in-domain slot of lambda^n exactly once and leaves it zero, so the two
+// adjoint buffers alternate without clearing.
 int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s);
 
 }  // namespace mrlbm

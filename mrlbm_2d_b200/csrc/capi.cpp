@@ -957,6 +957,7 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
              cudaMalloc((void**)&gb, (size_t)2 * nodes * sizeof(double)) == cudaSuccess &&
              cudaMalloc((void**)&gu, (size_t)h->L.ny * sizeof(double)) == cudaSuccess &&
              cudaMemsetAsync(lam[0], 0, LB, h->stream) == cudaSuccess &&
+             cudaMemsetAsync(lam[1], 0, LB, h->stream) == cudaSuccess &&
              cudaMemsetAsync(gb, 0, (size_t)2 * nodes * sizeof(double), h->stream) == cudaSuccess &&
              cudaMemsetAsync(gu, 0, (size_t)h->L.ny * sizeof(double), h->stream) == cudaSuccess;
     if (!ok) {
@@ -994,7 +995,6 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             if (adj_forward(h, seg[t - 1], seg[t], it0 + n0 + t, nullptr, n0 + t == 1 && h->ovr_live, tile) != 0) rc = MRLBM_ECUDA;
         for (int n = n0 + m; n > n0 && rc == MRLBM_OK; --n) {
             const int t = n - n0 - 1;                  // seg[t] = F^{n-1}
-            if (cudaMemsetAsync(lam[li ^ 1], 0, LB, h->stream) != cudaSuccess) { rc = MRLBM_ECUDA; break; }
             StepParams<double> p{};
             fill_common(h, p);
             p.src = seg[t];

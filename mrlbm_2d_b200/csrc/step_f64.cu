@@ -62,12 +62,11 @@ int batch_blocks_per_sm_f64(int tile_cfg) {
     }
 }
 
-// Adjoint step (adjoint.cuh): bulk nodes, edge columns, curved-wall nodes.
+// Adjoint step (adjoint.cuh): one launch with wall, edge-column and bulk blocks.
 int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s) {
     const int64_t nodes = (int64_t)p.L.nx * p.L.ny;
-    adj::adjoint_bulk<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(p, a);
-    if (a.n_edge > 0) adj::adjoint_edge<<<(unsigned)((a.n_edge * 18 + 127) / 128), 128, 0, s>>>(p, a);
-    if (p.nb > 0) adj::adjoint_wall<<<(unsigned)((p.nb * 81 + 127) / 128), 128, 0, s>>>(p, a);
+    const int64_t blocks = (int64_t)p.nb + (a.n_edge + 6) / 7 + (nodes + 127) / 128;
+    adj::adjoint_step<<<(unsigned)blocks, 128, 0, s>>>(p, a);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
