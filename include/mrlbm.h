@@ -258,6 +258,22 @@ int mrlbm_field_stats_window(mrlbm_handle* h, int32_t begin_iter, int32_t end_it
 int mrlbm_field_stats_get(mrlbm_handle* h, double* mean_u, double* mean_v, double* mean_p, double* rms_u,
                           double* rms_v, double* rms_p, int64_t* n_samples);
 
+/* ---- surface pressure and probes (write_statistics_out and the probe files) -------------
+ * When enabled, every statistics step (post_process, statsbegin <= iter <= statsend) also
+ * records, from the populations that step gathers: the wall pressure p = rho cs2 extrapolated
+ * quadratically in r from reference points 2, 3 and 4 (extrapolate_var_on_cylinder,
+ * 2d_mrlbm.f90:619-672), ordered by theta (the rows of data_mean/p_surface_time.dat,
+ * 2d_mrlbm.f90:602-612); its Gaussian smoothing over theta, sigma = 0.1 (gaussian_smoothing,
+ * 2d_mrlbm.f90:718-740, p_surface_smooth_time.dat); and the four probes' rho/3, ux/3, uy/3
+ * (the data_probe files, 2d_mrlbm.f90:468-476; probe nodes 2d_mrlbm.f90:102-109, or 1, 1.5, 2 and
+ * 2.5 diameters behind the centre, one row above it, for explicit geometry). */
+int mrlbm_surface_enable(mrlbm_handle* h, int32_t enable);
+int mrlbm_get_probe_nodes(const mrlbm_handle* h, int32_t* pi, int32_t* pj);
+/* Drain up to cap records: iter[r], p_surface[r*nbct + k], p_smooth[r*nbct + k] (k in theta
+ * order) and probes[r*12 + q] = (p1..p4, ux1..ux4, uy1..uy4); any array may be NULL. */
+int mrlbm_get_surface(mrlbm_handle* h, int32_t* iter, double* p_surface, double* p_smooth, double* probes,
+                      int32_t cap, int32_t* n);
+
 /* ---- body force and the adjoint of mean drag (no counterpart in the reference) ----------
  * Body force: g (2 x nx*ny, x components then y, Fortran node order) adds the momentum
  * source fout_k += 3 w_k (c_k . g) after collision at every bulk and edge node (not at

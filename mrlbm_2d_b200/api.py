@@ -37,6 +37,7 @@ EXPORTED = [
     "mrlbm_batch_set_schedule", "mrlbm_batch_get_schedule", "mrlbm_batch_autotune", "mrlbm_batch_status",
     "mrlbm_batch_last_error", "mrlbm_batch_launch_count", "mrlbm_batch_get_stream",
     "mrlbm_set_body_force", "mrlbm_adjoint_drag",
+    "mrlbm_surface_enable", "mrlbm_get_probe_nodes", "mrlbm_get_surface",
 ]
 BATCH_PERSISTENT, BATCH_GRAPH = 0, 1
 
@@ -109,6 +110,9 @@ def load_library(path=None):
         "mrlbm_batch_get_stream": [vp, vp],
         "mrlbm_set_body_force": [vp, vp],
         "mrlbm_adjoint_drag": [vp, i32, i32, i32, vp, vp, vp],
+        "mrlbm_surface_enable": [vp, i32],
+        "mrlbm_get_probe_nodes": [vp, vp, vp],
+        "mrlbm_get_surface": [vp, vp, vp, vp, vp, i32, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -297,6 +301,25 @@ class Simulation:
         self._check(self._L.mrlbm_get_macro(self._h, *[_ptr(o) for o in outs]))
         names = ["rho", "ux", "uy", "mxx", "myy", "mxy"]
         return {n: o.reshape(self.ny, self.nx).T for n, o in zip(names, outs)}
+
+    def surface_enable(self, on=True):
+        """Record wall pressure, its smoothing and the probes on every statistics step."""
+        self._check(self._L.mrlbm_surface_enable(self._h, 1 if on else 0))
+
+    def probe_nodes(self):
+        pi, pj = (ctypes.c_int32 * 4)(), (ctypes.c_int32 * 4)()
+        self._check(self._L.mrlbm_get_probe_nodes(self._h, pi, pj))
+        return list(zip(pi, pj))
+
+    def surface(self, cap=1 << 16):
+        """Drain: (iter, p_surface (n, nbct), p_smooth (n, nbct), probes (n, 12) = p1..4, ux1..4, uy1..4)."""
+        nb = self.nbct
+        it = np.empty(cap, np.int32)
+        ps, pf, pr = np.empty((cap, nb)), np.empty((cap, nb)), np.empty((cap, 12))
+        n = ctypes.c_int32()
+        self._check(self._L.mrlbm_get_surface(self._h, _ptr(it), _ptr(ps), _ptr(pf), _ptr(pr), cap, ctypes.byref(n)))
+        m = n.value
+        return it[:m].copy(), ps[:m].copy(), pf[:m].copy(), pr[:m].copy()
 
     def set_body_force(self, g):
         """Body force g of shape (2, nx, ny) (x and y components, [c, i-1, j-1]); None removes it."""

@@ -18,6 +18,7 @@
 #include "batch_params.h"
 #include "noalloc.h"
 #include "state_io.h"
+#include "surface.h"
 #include "step_params.h"
 
 using namespace mrlbm;
@@ -54,6 +55,15 @@ struct mrlbm_handle {
     bool has_uin = false;
     void* d_body = nullptr;                   // 2 x N body force (T), or null
     bool has_body = false;
+    // surface pressure / probe output on statistics steps (2d_mrlbm.f90:462-476, 593-766)
+    bool surf_on = false;
+    SurfaceTables surf{};
+    double *d_quad = nullptr, *d_W = nullptr, *d_sumw = nullptr, *d_sring = nullptr, *d_pring = nullptr;
+    int* d_sidx = nullptr;
+    int surf_cap = 0, surf_n = 0;
+    std::vector<int32_t> surf_iter_dev;       // iterations of the records in the device ring
+    std::vector<int32_t> surf_iter;           // drained history
+    std::vector<double> surf_hist, probe_hist;
     double* h_ring = nullptr;                 // pinned
     std::vector<double> hist;                 // drained records, REC_WORDS each
     int iter = 0;
@@ -299,6 +309,51 @@ int prepare_tma(mrlbm_handle* h, int cfg) {
     return MRLBM_OK;
 }
 
+// Surface pressure and probes of the step just launched (its input level is buf[cur]).
+int drain_surface(mrlbm_handle* h) {
+    if (h->surf_n == 0) return MRLBM_OK;
+    const int nb = h->geo.nb;
+    const size_t a = h->surf_hist.size(), b = h->probe_hist.size();
+    h->surf_hist.resize(a + (size_t)h->surf_n * 2 * nb);
+    h->probe_hist.resize(b + (size_t)h->surf_n * 12);
+    CK(cudaMemcpyAsync(h->surf_hist.data() + a, h->d_sring, (size_t)h->surf_n * 2 * nb * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->probe_hist.data() + b, h->d_pring, (size_t)h->surf_n * 12 * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->surf_iter.insert(h->surf_iter.end(), h->surf_iter_dev.begin(), h->surf_iter_dev.end());
+    h->surf_iter_dev.clear();
+    h->surf_n = 0;
+    return MRLBM_OK;
+}
+
+int surface_step(mrlbm_handle* h) {
+    if (h->surf_n == h->surf_cap) {
+        int rc = drain_surface(h);
+        if (rc != MRLBM_OK) return rc;
+    }
+    const int nb = h->geo.nb;
+    double* rec = h->d_sring + (size_t)h->surf_n * 2 * nb;
+    double* prec = h->d_pring + (size_t)h->surf_n * 12;
+    int rc;
+    if (h->precision == MRLBM_FP64) {
+        StepParams<double> p{};
+        fill_common(h, p);
+        p.src = (const double*)h->buf[h->cur];
+        rc = launch_surface_f64(p, h->surf, rec, prec, h->stream);
+    } else {
+        StepParams<float> p{};
+        fill_common(h, p);
+        p.src = (const float*)h->buf[h->cur];
+        rc = launch_surface_f32(p, h->surf, rec, prec, h->stream);
+    }
+    h->launches += 2;
+    if (rc != 0) return fail(h, MRLBM_ECUDA, "surface kernel launch failed");
+    h->surf_iter_dev.push_back(h->iter);
+    ++h->surf_n;
+    return MRLBM_OK;
+}
+
 int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     const int tc = h->tile_cfg;
     const bool fstat = h->d_fstat && h->iter >= h->fstat_begin && h->iter <= h->fstat_end;
@@ -365,6 +420,10 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         tma_box(h->precision, tc, &bw, &bh, &st);
         h->tile_base += tma_claims_host(h->L.nx, h->L.ny, TMA_CFGS[tc - TMA_CFG0].bx, bh, st, h->workers);
     }
+    if (stats && h->surf_on) {
+        int src = surface_step(h);
+        if (src != MRLBM_OK) return src;
+    }
     h->cur ^= 1;
     h->ovr_live = false;
     if (stats) ++h->ring_n;
@@ -377,7 +436,8 @@ void free_all(mrlbm_handle* h) {
     cudaSetDevice(h->device);
     for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
                     (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, h->d_body, (void*)h->d_ovr, (void*)h->d_fstage,
-                    (void*)h->d_tile_ctr, (void*)h->d_fstat, (void*)h->d_fstat_out})
+                    (void*)h->d_tile_ctr, (void*)h->d_fstat, (void*)h->d_fstat_out, (void*)h->d_quad, (void*)h->d_W,
+                    (void*)h->d_sumw, (void*)h->d_sring, (void*)h->d_pring, (void*)h->d_sidx})
         if (p) cudaFree(p);
     if (h->h_ring) cudaFreeHost(h->h_ring);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -648,6 +708,118 @@ int mrlbm_set_inlet_profile(mrlbm_handle* h, const double* u_in) {
     }
     CK(cudaStreamSynchronize(h->stream));
     h->has_uin = true;
+    return MRLBM_OK;
+}
+
+int mrlbm_surface_enable(mrlbm_handle* h, int32_t enable) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    if (!enable) { h->surf_on = false; return MRLBM_OK; }
+    const Geometry& g = h->geo;
+    const int nb = g.nb;
+    if (nb == 0) return fail(h, MRLBM_EUNSUPPORTED, "no cylinder: no surface to sample");
+    if ((size_t)nb * sizeof(double) > 48 * 1024) return fail(h, MRLBM_EUNSUPPORTED, "more than 6144 wall nodes");
+    const mrlbm_config& c = h->cfg;
+    // probes (2d_mrlbm.f90:102-109): 1, 1.5, 2 and 2.5 diameters behind the centre, one row above it
+    int pi[4], pj[4];
+    if (c.geometry_mode == MRLBM_GEOM_REFERENCE) {
+        const int nfront = c.L_front * c.ncy, nbot = c.L_bot * c.ncy, ncy = c.ncy;
+        const int base = nfront + ncy + 1;
+        pi[0] = base + ncy / 2; pi[1] = base + ncy; pi[2] = base + 3 * ncy / 2; pi[3] = base + 2 * ncy;
+        for (int k = 0; k < 4; ++k) pj[k] = nbot + ncy / 2 + 1;
+    } else {
+        for (int k = 0; k < 4; ++k) {
+            pi[k] = (int)std::floor(g.x_c + (1.0 + 0.5 * k) * 2.0 * g.r_c + 0.5);
+            pj[k] = (int)std::floor(g.y_c) + 1;
+        }
+    }
+    for (int k = 0; k < 4; ++k) {
+        if (pi[k] < 1 || pi[k] > h->L.nx || pj[k] < 1 || pj[k] > h->L.ny)
+            return fail(h, MRLBM_EUNSUPPORTED, "a probe falls outside the domain");
+        if (g.cls[(size_t)(pi[k] - 1) + (size_t)h->L.nx * (pj[k] - 1)] != 0)
+            return fail(h, MRLBM_EUNSUPPORTED, "a probe falls on a solid or wall node");
+    }
+    CK(cudaSetDevice(h->device));
+    if (!h->d_quad) {
+        // radii for quadratic_interpolation (2d_mrlbm.f90:742-765), points 2, 3, 4 and the wall point
+        std::vector<double> quad(5 * (size_t)nb);
+        auto rad = [](double x, double y) { return std::sqrt((x * x) + (y * y)); };
+        for (int l = 0; l < nb; ++l) {
+            const double* r = &g.ref[8 * (size_t)l];
+            const double r1 = rad(r[1] - g.x_c, r[5] - g.y_c), r2 = rad(r[2] - g.x_c, r[6] - g.y_c);
+            const double r3 = rad(r[3] - g.x_c, r[7] - g.y_c), rs = rad(r[0] - g.x_c, r[4] - g.y_c);
+            double* q = &quad[5 * (size_t)l];
+            q[0] = r1; q[1] = r2; q[2] = r3; q[3] = rs;
+            q[4] = (r1 - r2) * (r1 - r3) * (r2 - r3);
+        }
+        // theta order by the reference's selection swap (2d_mrlbm.f90:1138-1156)
+        std::vector<int> idx(nb);
+        for (int i = 0; i < nb; ++i) idx[i] = i;
+        for (int i = 0; i < nb - 1; ++i)
+            for (int j = i + 1; j < nb; ++j)
+                if (g.theta[idx[i]] > g.theta[idx[j]]) std::swap(idx[i], idx[j]);
+        // Gaussian weights over the sorted angles (gaussian_smoothing, 2d_mrlbm.f90:718-740)
+        std::vector<double> W((size_t)nb * nb), sumw(nb);
+        const double sigma = 0.1;
+        for (int i = 0; i < nb; ++i) {
+            double sw = 0.0;
+            for (int j = 0; j < nb; ++j) {
+                const double d = g.theta[idx[i]] - g.theta[idx[j]];
+                const double w = std::exp(-(d * d) / (2.0 * (sigma * sigma)));
+                W[(size_t)j * nb + i] = w;
+                sw = sw + w;
+            }
+            sumw[i] = sw;
+        }
+        h->surf_cap = (int)std::max<size_t>(1, std::min<size_t>(RING_CAP, ((size_t)64 << 20) / ((size_t)2 * nb * sizeof(double))));
+        CK(cudaMalloc((void**)&h->d_quad, quad.size() * sizeof(double)));
+        CK(cudaMalloc((void**)&h->d_sidx, nb * sizeof(int)));
+        CK(cudaMalloc((void**)&h->d_W, W.size() * sizeof(double)));
+        CK(cudaMalloc((void**)&h->d_sumw, nb * sizeof(double)));
+        CK(cudaMalloc((void**)&h->d_sring, (size_t)h->surf_cap * 2 * nb * sizeof(double)));
+        CK(cudaMalloc((void**)&h->d_pring, (size_t)h->surf_cap * 12 * sizeof(double)));
+        CK(cudaMemcpyAsync(h->d_quad, quad.data(), quad.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_sidx, idx.data(), nb * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_W, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d_sumw, sumw.data(), nb * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->surf.quad = h->d_quad;
+    h->surf.idx = h->d_sidx;
+    h->surf.W = h->d_W;
+    h->surf.sumw = h->d_sumw;
+    h->surf.nb = nb;
+    for (int k = 0; k < 4; ++k) { h->surf.probe_i[k] = pi[k]; h->surf.probe_j[k] = pj[k]; }
+    h->surf_on = true;
+    return MRLBM_OK;
+}
+
+int mrlbm_get_probe_nodes(const mrlbm_handle* h, int32_t* pi, int32_t* pj) {
+    if (!h || !pi || !pj || !h->surf_on) return MRLBM_EINVAL;
+    for (int k = 0; k < 4; ++k) { pi[k] = h->surf.probe_i[k]; pj[k] = h->surf.probe_j[k]; }
+    return MRLBM_OK;
+}
+
+int mrlbm_get_surface(mrlbm_handle* h, int32_t* iter, double* p_surface, double* p_smooth, double* probes,
+                      int32_t cap, int32_t* n) {
+    if (!h || !n || cap < 0) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    int rc = drain_surface(h);
+    if (rc != MRLBM_OK) return rc;
+    const int nb = h->geo.nb;
+    const int m = std::min<int>(cap, (int)h->surf_iter.size());
+    for (int r = 0; r < m; ++r) {
+        if (iter) iter[r] = h->surf_iter[r];
+        const double* src = h->surf_hist.data() + (size_t)r * 2 * nb;
+        if (p_surface) std::memcpy(p_surface + (size_t)r * nb, src, nb * sizeof(double));
+        if (p_smooth) std::memcpy(p_smooth + (size_t)r * nb, src + nb, nb * sizeof(double));
+        if (probes) std::memcpy(probes + (size_t)r * 12, h->probe_hist.data() + (size_t)r * 12, 12 * sizeof(double));
+    }
+    h->surf_iter.erase(h->surf_iter.begin(), h->surf_iter.begin() + m);
+    h->surf_hist.erase(h->surf_hist.begin(), h->surf_hist.begin() + (size_t)m * 2 * nb);
+    h->probe_hist.erase(h->probe_hist.begin(), h->probe_hist.begin() + (size_t)m * 12);
+    *n = m;
     return MRLBM_OK;
 }
 

@@ -10,6 +10,9 @@
 //   output/master.p3d                   index of the function files                [2334-2367]
 //   restart/restart.dat                 soln_time, f, f_eq, ux, uy, rho            [2186-2202]
 //   data_mean/forces_time.dat           iter, F_drag_net, F_lift_net per stats step [492-494]
+//   data_mean/p_surface_time.dat,       unformatted records (iter, wall pressure by theta) and
+//   data_mean/p_surface_smooth_time.dat its Gaussian smoothing, per stats step          [593-616]
+//   data_probe/{p,ux,uy}_probe.dat      iter and the 4 probes' rho/3, ux/3, uy/3        [462-476]
 //   data_mean/theta.dat                 sorted wall angles                         [1158-1162]
 //   rho_mean_inlet.dat                  running mean inlet density /100 stats steps [362-366]
 //   data_probe/probe_loc.dat, simulation_parameters.dat                            [113-118, 157-168]
@@ -44,7 +47,7 @@ void die(const char* what, int rc, mrlbm_handle* h) {
 struct FortranWriter {
     FILE* f = nullptr;
     std::vector<char> rec;
-    explicit FortranWriter(const std::string& path) { f = std::fopen(path.c_str(), "wb"); }
+    explicit FortranWriter(const std::string& path, const char* mode = "wb") { f = std::fopen(path.c_str(), mode); }
     ~FortranWriter() { if (f) std::fclose(f); }
     template <class T> void put(const T* p, size_t n) {
         const char* c = (const char*)p;
@@ -241,6 +244,46 @@ int main(int argc, char** argv) {
                           "data_mean/forces_time.dat", "rho_mean_inlet.dat"})
         if (FILE* f = std::fopen(p, "w")) std::fclose(f);
     const bool pp = cfg.post_process != 0;
+    const int nbct = gi.nbct;
+    // surface pressure and probe records of every statistics step (2d_mrlbm.f90:462-476, 593-616)
+    const bool surf = pp && nbct > 0 && mrlbm_surface_enable(h, 1) == MRLBM_OK;
+    // the reference opens the probe files when iter == statsbegin; a run that starts later
+    // writes to the units' default files
+    const bool probes_named = cfg.statsbegin > iter;
+    const char* probe_file[3] = {probes_named ? "data_probe/p_probe.dat" : "fort.101",
+                                 probes_named ? "data_probe/ux_probe.dat" : "fort.102",
+                                 probes_named ? "data_probe/uy_probe.dat" : "fort.103"};
+    if (surf)
+        for (const char* pf : probe_file)
+            if (FILE* f = std::fopen(pf, "w")) std::fclose(f);
+    std::vector<int32_t> sit(1024);
+    std::vector<double> sps((size_t)1024 * std::max(nbct, 1)), spf((size_t)1024 * std::max(nbct, 1)), spr(1024 * 12);
+    auto drain_surface = [&]() {
+        if (!surf) return;
+        int32_t n = 0;
+        do {
+            if ((rc = mrlbm_get_surface(h, sit.data(), sps.data(), spf.data(), spr.data(), 1024, &n)) != MRLBM_OK)
+                die("mrlbm_get_surface", rc, h);
+            FortranWriter ws("data_mean/p_surface_time.dat", "ab"), wf("data_mean/p_surface_smooth_time.dat", "ab");
+            FILE* fp[3];
+            for (int q = 0; q < 3; ++q) fp[q] = std::fopen(probe_file[q], "a");
+            for (int t = 0; t < n; ++t) {
+                ws.put1(sit[t]);
+                ws.put(sps.data() + (size_t)t * nbct, nbct);
+                ws.end_record();
+                wf.put1(sit[t]);
+                wf.put(spf.data() + (size_t)t * nbct, nbct);
+                wf.end_record();
+                for (int q = 0; q < 3; ++q) {
+                    if (!fp[q]) continue;
+                    std::fprintf(fp[q], "%s", ld_int(sit[t]).c_str());
+                    for (int k = 0; k < 4; ++k) std::fprintf(fp[q], "%s", ld_real(spr[(size_t)t * 12 + 4 * q + k]).c_str());
+                    std::fprintf(fp[q], "\n");
+                }
+            }
+            for (int q = 0; q < 3; ++q) if (fp[q]) std::fclose(fp[q]);
+        } while (n == 1024);
+    };
     double rho_inf_mean = 0.0;
     auto t0 = std::chrono::steady_clock::now();
     std::vector<int32_t> rit(8192);
@@ -265,6 +308,7 @@ int main(int argc, char** argv) {
             std::fclose(ff);
             if (fr) std::fclose(fr);
         } while (n == 8192);
+        drain_surface();
     };
     const int iplot = std::max(cfg.iplot, 1), isave = std::max(cfg.isave, 1);
     while (iter < cfg.max_iter) {

@@ -4,6 +4,7 @@
 #include "step_tma.cuh"
 #include "step_batch.cuh"
 #include "adjoint.cuh"
+#include "surface.cuh"
 
 namespace mrlbm {
 
@@ -68,6 +69,14 @@ int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cuda
     const int64_t blocks = (int64_t)p.nb + (a.n_edge + 6) / 7 + (nodes + 127) / 128;
     adj::adjoint_step<<<(unsigned)blocks, 128, 0, s>>>(p, a);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_surface_f64(const StepParams<double>& p, const SurfaceTables& t, double* rec, double* prec, cudaStream_t s) {
+    return surf::launch_surface(p, t, rec, prec, s);
+}
+
+int launch_surface_f32(const StepParams<float>& p, const SurfaceTables& t, double* rec, double* prec, cudaStream_t s) {
+    return surf::launch_surface(p, t, rec, prec, s);
 }
 
 }  // namespace mrlbm

@@ -79,6 +79,9 @@ def test_fp64_gpu_matches_reference_execution(mrlbm, tmp_path, name):
     d = _load(name)
     cfg = _config(mrlbm, d, tmp_path)
     s = mrlbm.Simulation(cfg, precision=mrlbm.FP64)
+    surf = s.nbct > 0 and "p_surface" in d
+    if surf:
+        s.surface_enable()
     if "restart_in_f" in d:
         s.load_state(d["restart_in_f"], iter=int(d["restart_in_iter"]))
     it = s.iter
@@ -99,4 +102,16 @@ def test_fp64_gpu_matches_reference_execution(mrlbm, tmp_path, name):
     ref = d["forces"]
     assert np.array_equal(its, ref[:, 0].astype(int))
     assert np.array_equal(fd, ref[:, 1]) and np.array_equal(fl, ref[:, 2]), "force sums"
+    if surf:
+        # write_statistics_out and the probe records (2d_mrlbm.f90:468-476, 593-616)
+        sit, ps, pf, pr = s.surface()
+        assert np.array_equal(sit, d["p_surface"][:, 0].astype(int))
+        assert np.array_equal(ps, d["p_surface"][:, 1:]), "surface pressure"
+        assert np.array_equal(pf, d["p_surface_smooth"][:, 1:]), "smoothed surface pressure"
+        for q, key in enumerate(("probe_p", "probe_ux", "probe_uy")):
+            if d[key].size == 0:
+                # the reference opens the probe files only at iter == statsbegin (2d_mrlbm.f90:
+                # 464-466); a run that starts past statsbegin writes them to unnamed units
+                continue
+            assert np.array_equal(pr[:, 4 * q:4 * q + 4], d[key][:, 1:]), key
     s.close()

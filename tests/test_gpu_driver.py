@@ -63,3 +63,10 @@ def test_driver_reproduces_reference_outputs(mrlbm, tmp_path):
     np.testing.assert_allclose(rows[:, 1:], d["forces"][:, 1:], rtol=1e-12, atol=1e-13)
     theta = np.loadtxt(tmp_path / "data_mean" / "theta.dat")
     np.testing.assert_allclose(theta, d["theta"], rtol=1e-15, atol=0)
+    # unformatted wall-pressure records: iter and the theta-ordered values (2d_mrlbm.f90:609-616)
+    for fname, key in (("p_surface_time.dat", "p_surface"), ("p_surface_smooth_time.dat", "p_surface_smooth")):
+        recs = read_records(tmp_path / "data_mean" / fname)
+        assert len(recs) == len(d[key])
+        for rec, ref in zip(recs, d[key]):
+            assert int(np.frombuffer(rec[:4], np.int32)[0]) == int(ref[0])
+            assert np.array_equal(np.frombuffer(rec[4:], np.float64), ref[1:]), fname
