@@ -50,6 +50,45 @@ def parse():
     return ap.parse_args()
 
 
+class RankGroup:
+    """One process per GPU (torchrun env: RANK, WORLD_SIZE, LOCAL_RANK, MASTER_*): the
+    barrier and max-over-ranks reductions the timing needs; no collective touches the data
+    path (every rank advances its own replica).  backend "nccl" on GPUs, "gloo" on CPU."""
+
+    def __init__(self, backend="nccl"):
+        import datetime
+        import torch
+        import torch.distributed as dist
+        self.dist, self.torch = dist, torch
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = torch.device("cuda", self.local) if backend == "nccl" else torch.device("cpu")
+        if self.world > 1:
+            kw = {"device_id": self.device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return float(x)
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+def replica_seed(rank):
+    """Each rank's replica is the same case with its own noise seed."""
+    return 1234 + rank
+
+
 def make_case(name, seed):
     from mrlbm_2d_b200.config import case_large, case_mid, case_quarter, case_small
     c = {"mid": case_mid, "large": case_large, "small": case_small, "quarter": case_quarter}[name]()
@@ -222,25 +261,18 @@ def main():
 
     import numpy as np
     import torch
-    import torch.distributed as dist
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    ranks = RankGroup("nccl")
+    rank, world = ranks.rank, ranks.world
 
     from mrlbm_2d_b200 import build
     if rank == 0:
         build.build()
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     import mrlbm_2d_b200 as m
 
-    cfg = make_case(args.case, 1234 + rank)
+    cfg = make_case(args.case, replica_seed(rank))
     nodes = cfg.nx * cfg.ny
     dev = torch.cuda.current_device()
     # one non-default stream carries the library's kernels, the L2 flush and the events
@@ -249,16 +281,11 @@ def main():
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        ranks.barrier()
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max(x)
 
     def pick_tile(sim):
         if args.tile is not None:
@@ -314,7 +341,10 @@ def main():
         sim = m.Simulation(cfg, precision=precision, device=dev)
         sim.set_stream(stream.cuda_stream)
         sim.tile_config = tile               # the autotuner's choice for this case (untimed setup)
-        f0 = sim.get_state()                 # host copy of the seeded initial populations
+        # pinned host buffers: the initial populations (Fortran order) and rho, ux, uy
+        f0 = torch.empty(nodes * 9, dtype=torch.float64).pin_memory().numpy()
+        sim.get_state(out=f0)                # host copy of the seeded initial populations
+        mac = [torch.empty(nodes, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
         sim.step(3)
         sim.forces()
         barrier()
@@ -325,7 +355,7 @@ def main():
             n = min(100, K - s0)
             sim.step(n, macro=(s0 + n == K))
             nrec += len(sim.forces()[0])
-        mac = sim.macro()
+        sim.macro(out=mac)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
         el = max_over_ranks(el)
@@ -336,8 +366,8 @@ def main():
         del mac
         return {"value": world * nodes * K / el / 1e6, "unit": "MLUPS",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "note": "load_state(host f) + K x step + force drain every 100 steps + rho/ux/uy of the "
-                        "last step, wall clock, max over ranks"}
+                "note": "load_state(pinned host f, FP64) + K x step + force drain every 100 steps + "
+                        "rho/ux/uy of the last step into pinned buffers, wall clock, max over ranks"}
 
     precisions = [args.precision] if args.precision else ([32, 64] if _fp32_available(m, cfg) else [64])
     head = precisions[0]
@@ -412,8 +442,7 @@ def main():
         t0 = min(w[0] for w in wins) - 1.2
         t1 = max(w[1] for w in wins)
         line["clocks"] = sampler.summary(t0, t1)
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(args.case, args.cpu_sample_seconds)
@@ -421,8 +450,7 @@ def main():
             line["cpu_baseline"] = {"value": None, "error": str(ex)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 

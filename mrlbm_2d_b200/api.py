@@ -275,15 +275,24 @@ class Simulation:
         return rec[:n.value].copy()
 
     # -- state and outputs -----------------------------------------------------------
-    def get_state(self):
-        """Post-streaming populations f as an (nx, ny, 9) array, f[i-1, j-1, k]."""
-        f = np.empty(self.nx * self.ny * 9)
+    def get_state(self, out=None):
+        """Post-streaming populations f as an (nx, ny, 9) array, f[i-1, j-1, k].  With `out` (a
+        flat float64 array of nx*ny*9, e.g. a pinned buffer) the reference's Fortran-order f
+        is written there and `out` is returned as is."""
+        f = np.empty(self.nx * self.ny * 9) if out is None else out
+        assert f.dtype == np.float64 and f.size == self.nx * self.ny * 9 and f.flags.c_contiguous
         self._check(self._L.mrlbm_get_state(self._h, _ptr(f)))
-        return f.reshape(9, self.ny, self.nx).transpose(2, 1, 0)
+        return f.reshape(9, self.ny, self.nx).transpose(2, 1, 0) if out is None else out
 
     def load_state(self, f, iter=0):
-        a = np.asfortranarray(np.asarray(f, dtype=np.float64).reshape(self.nx, self.ny, 9))
-        flat = np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()
+        """Load populations: an (nx, ny, 9) array f[i-1, j-1, k], or a flat float64 array in the
+        reference's Fortran order f(i, j, k) (passed to the device as is)."""
+        f = np.asarray(f)
+        if f.ndim == 1 and f.dtype == np.float64 and f.flags.c_contiguous and f.size == self.nx * self.ny * 9:
+            flat = f
+        else:
+            a = np.asfortranarray(np.asarray(f, dtype=np.float64).reshape(self.nx, self.ny, 9))
+            flat = np.ascontiguousarray(a.transpose(2, 1, 0)).ravel()
         self._check(self._L.mrlbm_load_state(self._h, _ptr(flat), int(iter)))
 
     def set_inlet_profile(self, u_in):
@@ -294,9 +303,13 @@ class Simulation:
         assert a.size == self.ny
         self._check(self._L.mrlbm_set_inlet_profile(self._h, _ptr(a)))
 
-    def macro(self):
-        """dict of (nx, ny) arrays rho, ux, uy, mxx, myy, mxy of the last MACRO step."""
+    def macro(self, out=None):
+        """dict of (nx, ny) arrays rho, ux, uy, mxx, myy, mxy of the last MACRO step.  With
+        `out` = [rho, ux, uy] flat float64 buffers (e.g. pinned), only those three are read back."""
         N = self.nx * self.ny
+        if out is not None:
+            self._check(self._L.mrlbm_get_macro(self._h, *[_ptr(o) for o in out], None, None, None))
+            return out
         outs = [np.empty(N) for _ in range(6)]
         self._check(self._L.mrlbm_get_macro(self._h, *[_ptr(o) for o in outs]))
         names = ["rho", "ux", "uy", "mxx", "myy", "mxy"]
