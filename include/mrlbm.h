@@ -286,8 +286,9 @@ int mrlbm_set_body_force(mrlbm_handle* h, const double* g);
  * profile is set).  Discrete adjoint of the FP64 step: a forward pass keeps a checkpoint every
  * checkpoint_every steps; the backward pass recomputes each segment from its checkpoint and runs
  * the adjoint kernels step by step.  Either gradient pointer may be NULL; both NULL computes J
- * only.  FP64 handles with inlet/outlet columns, free-slip or y-periodic walls and the rotated
- * strong closure (the defaults); MRLBM_EUNSUPPORTED otherwise. */
+ * only.  Handles with inlet/outlet columns, free-slip or y-periodic walls and the rotated strong
+ * closure (the defaults); MRLBM_EUNSUPPORTED otherwise.  On an FP32 handle the trajectory is the
+ * FP32 step's (checkpoints in FP32) and the adjoint arithmetic is FP64. */
 int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t window, int32_t checkpoint_every, double* J,
                        double* grad_body, double* grad_uin);
 

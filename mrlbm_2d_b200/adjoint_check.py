@@ -29,6 +29,8 @@ def main(argv=None):
     ap.add_argument("--directions", type=int, default=16)
     ap.add_argument("--rel-step", type=float, default=1e-4)
     ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--fp32", action="store_true",
+                    help="also run the adjoint on an FP32 handle (FP32 trajectory, FP64 adjoint) and compare")
     a = ap.parse_args(argv)
     cfg = case_adjoint()
     sim = api.Simulation(cfg, precision=api.FP64)
@@ -58,11 +60,27 @@ def main(argv=None):
         ad = float((gb * db).sum() + (gu * du).sum())
         errs.append({"adjoint": ad, "fd": fd, "rel_err": abs(ad - fd) / abs(fd)})
     sim.close()
+    fp32 = None
+    if a.fp32:
+        s32 = api.Simulation(cfg, precision=api.FP32)
+        s32.set_body_force(body)
+        s32.set_inlet_profile(uin)
+        J32, gb32, gu32 = s32.adjoint_drag(N, T, K)
+        s32.close()
+        rel = []
+        for _ in range(a.directions):
+            db = rng.standard_normal(body.shape)
+            du = rng.standard_normal(uin.shape)
+            d64 = float((gb * db).sum() + (gu * du).sum())
+            d32 = float((gb32 * db).sum() + (gu32 * du).sum())
+            rel.append(abs(d32 - d64) / abs(d64))
+        fp32 = {"J": J32, "rel_err_J": abs(J32 - J) / abs(J), "max_rel_err_vs_fp64_adjoint": max(rel)}
     out = {"case": "512x128 D=32 Re=100 U=0.05", "steps": N, "window": T, "checkpoint_every": K, "J": J,
            "J_forward_only": J0, "directions": a.directions, "rel_step": h,
            "max_rel_err": max(e["rel_err"] for e in errs), "median_rel_err": float(np.median([e["rel_err"] for e in errs])),
            "forward_s": t1 - t0, "gradient_s": t2 - t1, "gradient_over_forward": (t2 - t1) / (t1 - t0),
-           "grad_body_max": float(np.abs(gb).max()), "grad_uin_max": float(np.abs(gu).max()), "checks": errs}
+           "grad_body_max": float(np.abs(gb).max()), "grad_uin_max": float(np.abs(gu).max()), "fp32": fp32,
+           "checks": errs}
     print(json.dumps(out), flush=True)
     return out
 

@@ -30,7 +30,19 @@
 namespace mrlbm {
 namespace adj {
 
-using P = StepParams<double>;
+// Populations of node (i, j) as FP64 f: FP64 storage as is, FP32 storage holds f - w_k.
+template <class T>
+__device__ __forceinline__ double to_f(const StepParams<T>& p, int k, T v) {
+    return sizeof(T) == 8 ? (double)v : (double)p.w[k] + (double)v;
+}
+
+template <class T>
+__device__ __forceinline__ void gather_d(const StepParams<T>& p, int i, int j, double f[Q]) {
+    T g[Q];
+    gather(p, i, j, g);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) f[k] = to_f(p, k, g[k]);
+}
 
 // ---- dual numbers (value, derivative along one input) -----------------------------------
 struct Dual {
@@ -87,7 +99,7 @@ __device__ __forceinline__ MacS<S> moments_s(const S f[Q], double hm, double hp)
 }
 
 // Collision and Hermite reconstruction (2d_mrlbm.f90:407-415, 445-457), no incomp_bulk.
-template <class S>
+template <class P, class S>
 __device__ __forceinline__ void collide_s(const P& p, const MacS<S>& m, S fo[Q]) {
     const double om = p.omega, om1 = p.omega1;
     const S mxx = om1 * m.mxx + om * m.ux * m.ux;
@@ -132,7 +144,7 @@ __device__ __forceinline__ void incoming_s(const S f[Q], int mask, double hm, do
 
 // Edge column node (i = 1 inlet or i = nx outlet) of a free-slip / y-periodic case:
 // moments, Dirichlet values and the apply_bc closure (2d_mrlbm.f90:249-272, 1237-1366).
-template <class S>
+template <class P, class S>
 __device__ __forceinline__ void edge_map(const P& p, int i, const S f[Q], const S fn[Q], S uin, S fo[Q]) {
     MacS<S> m = moments_s(f, p.hm, p.hp);
     S rhoI, mxxI, myyI, mxyI;
@@ -161,11 +173,13 @@ __device__ __forceinline__ void edge_map(const P& p, int i, const S f[Q], const 
     collide_s(p, m, fo);
 }
 
-__device__ __forceinline__ double gf(const P& p, int field, int l) { return __ldg(p.bgeo + (int64_t)field * p.nb + l); }
+template <class P>
+__device__ __forceinline__ double gf(const P& p, int field, int l) { return (double)__ldg(p.bgeo + (int64_t)field * p.nb + l); }
+template <class P>
 __device__ __forceinline__ int gi(const P& p, int field, int l) { return __ldg(p.bint + (int64_t)field * p.nb + l); }
 
 // Rotated velocity and second moments of one bilinear stencil node (2d_mrlbm.f90:842-867).
-template <class S>
+template <class P, class S>
 __device__ __forceinline__ void stencil_quad(const P& p, int l, int s, const S f[Q], S& u, S& v, S& mx, S& my) {
     const MacS<S> m = moments_s(f, p.hm, p.hp);
     const double c2 = gf(p, G_SCC + s, l), s2q = gf(p, G_SSS + s, l), sn2 = gf(p, G_SS2 + s, l);
@@ -179,7 +193,7 @@ __device__ __forceinline__ void stencil_quad(const P& p, int l, int s, const S f
 // interpolation at reference points 2 and 3, extrapolation to the node, rotated strong
 // closure, collision (2d_mrlbm.f90:294-311, 768-928, 1635-1765, 407-457) and the node's drag
 // term (2d_mrlbm.f90:558-591).
-template <class S>
+template <class P, class S>
 __device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const S su[8], const S sv[8], const S smx[8],
                                          const S smy[8], S fo[Q], S& drag) {
     S u[2], v[2], mx[2], my[2];
@@ -259,12 +273,14 @@ __device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const 
 
 // Add c to lambda^{n-1} at the slot node (i, j) pulled for direction k (ghost slots hold
 // constants and take nothing).
+template <class P>
 __device__ __forceinline__ void scatter(const P& p, const AdjArgs& a, int i, int j, int k, double c) {
     const SrcSlot sl = stream_source(p.L.nx, p.L.ny, i, j, k, p.xper, p.yper, p.freeslip);
     if (sl.i < 1 || sl.i > p.L.nx || sl.j < 1 || sl.j > p.L.ny) return;
     atomicAdd(a.lam_out + p.L.at(sl.i, sl.j, sl.k), c);
 }
 
+template <class P>
 __device__ __forceinline__ void body_grad(const P& p, const AdjArgs& a, int i, int j, const double lam[Q]) {
     if (!a.grad_body) return;
     const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1), N = (int64_t)p.L.nx * p.L.ny;
@@ -281,6 +297,7 @@ __device__ __forceinline__ void body_grad(const P& p, const AdjArgs& a, int i, i
 // Bulk node, reverse mode by hand.  Forward: rho = sum g, u = j / rho, m = Pi / rho,
 // m' = (1 - w) m + w u u, fo_k = w_k rho A_k with A_k = 1 + 3 c.u + 4.5 m'_xx Hxx
 // + 4.5 m'_yy Hyy + 9 m'_xy Hxy.
+template <class P>
 __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int64_t t) {
     const int nx = p.L.nx, ny = p.L.ny;
     if (t >= (int64_t)nx * ny) return;
@@ -289,7 +306,7 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int64
     const int cls = node_class(p, i, j);
     if (cls >= 0) return;                                  // curved-wall node: adjoint_wall
     double g[Q], lam[Q];
-    gather(p, i, j, g);
+    gather_d(p, i, j, g);
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const int64_t at = p.L.at(i, j, k);
@@ -334,6 +351,7 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int64
 
 // Edge columns: thread (e, q), e over the 2 ny nodes of columns 1 and nx, q over 18 inputs:
 // own inputs 0..8; at the outlet the copied neighbour's inputs 9..17; at the inlet q = 9 is u_in(j).
+template <class P>
 __device__ __forceinline__ void adjoint_edge(const P& p, const AdjArgs& a, int e, int q, const double* lam) {
     if (e >= a.n_edge) return;
     const int ny = p.L.ny, nx = p.L.nx;
@@ -341,15 +359,15 @@ __device__ __forceinline__ void adjoint_edge(const P& p, const AdjArgs& a, int e
     const bool inlet = i == 1;
     if (inlet && q > 9) return;
     double g[Q], gn[Q];
-    gather(p, i, j, g);
-    if (!inlet) gather(p, nx - 1, j, gn);
+    gather_d(p, i, j, g);
+    if (!inlet) gather_d(p, nx - 1, j, gn);
     Dual f[Q], fn[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         f[k] = Dual(g[k], q == k ? 1.0 : 0.0);
         fn[k] = Dual(inlet ? 0.0 : gn[k], (!inlet && q == 9 + k) ? 1.0 : 0.0);
     }
-    const double u0 = p.u_in ? p.u_in[j - 1] : p.uinlet;
+    const double u0 = p.u_in ? (double)p.u_in[j - 1] : (double)p.uinlet;
     const Dual uin(u0, (inlet && q == 9) ? 1.0 : 0.0);
     Dual fo[Q];
     edge_map(p, i, f, fn, uin, fo);
@@ -366,6 +384,7 @@ __device__ __forceinline__ void adjoint_edge(const P& p, const AdjArgs& a, int e
 // its 8 stencil nodes) and the stencil quantities in shared memory; thread q < 81 then runs
 // the node's map with the derivative along input q (only its stencil node's quantities carry
 // a derivative) and scatters the contracted column.
+template <class P>
 __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l) {
     __shared__ double in[81], lam[Q], qd[4][8];
     __shared__ int slot[81];
@@ -381,7 +400,7 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
         }
         const SrcSlot sl = stream_source(p.L.nx, p.L.ny, ni, nj, k, p.xper, p.yper, p.freeslip);
         const int64_t at = p.L.at(sl.i, sl.j, sl.k);
-        in[q] = __ldg(p.src + at);
+        in[q] = to_f(p, k, __ldg(p.src + at));
         const bool ghost = sl.i < 1 || sl.i > p.L.nx || sl.j < 1 || sl.j > p.L.ny;
         slot[q] = ghost ? -1 : (int)at;
     } else if (q < 81 + Q) {
@@ -425,6 +444,7 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
 
 // One adjoint step in one launch of 128-thread blocks: [nb wall blocks][edge blocks, 7 nodes
 // x 18 inputs each][bulk blocks, 128 nodes each].
+template <class P>
 __global__ void __launch_bounds__(128) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
     const int b = (int)blockIdx.x;
     const int n_edge_blk = (a.n_edge + 6) / 7;

@@ -20,6 +20,8 @@ struct AdjArgs {
 // One adjoint step: p describes forward step n (src = F^{n-1}); lambda^{n-1} must be zero.
 // The step reads every in-domain slot of lambda^n exactly once and leaves it zero, so the two
 // adjoint buffers alternate without clearing.
+// FP32 handles: the forward states are FP32 deviations, the adjoint arithmetic is FP64.
 int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s);
+int launch_adjoint_step(const StepParams<float>& p, const adj::AdjArgs& a, cudaStream_t s);
 
 }  // namespace mrlbm

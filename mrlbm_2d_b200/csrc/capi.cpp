@@ -1067,15 +1067,16 @@ int mrlbm_get_launch_count(const mrlbm_handle* h, int64_t* n) {
 
 namespace {
 
-// One forward FP64 step from src into dst at iteration `iter` (drag record into rec if given).
-int adj_forward(mrlbm_handle* h, const double* src, double* dst, int iter, double* rec, bool ovr, int tile) {
-    StepParams<double> p{};
+// One forward step from src into dst at iteration `iter` (drag record into rec if given).
+template <class T>
+int adj_forward(mrlbm_handle* h, const void* src, void* dst, int iter, double* rec, bool ovr, int tile) {
+    StepParams<T> p{};
     fill_common(h, p);
     const mrlbm_config& c = h->cfg;
-    p.src = src;
-    p.dst = dst;
-    p.u_in = h->has_uin ? h->d_uin : nullptr;
-    p.body = h->has_body ? (const double*)h->d_body : nullptr;
+    p.src = (const T*)src;
+    p.dst = (T*)dst;
+    p.u_in = h->has_uin ? (const T*)h->d_uin : nullptr;
+    p.body = h->has_body ? (const T*)h->d_body : nullptr;
     p.ovr = ovr ? h->d_ovr : nullptr;
     p.n_ovr = ovr ? (int)h->ovr.size() : 0;
     p.zero_solid_u = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
@@ -1083,7 +1084,24 @@ int adj_forward(mrlbm_handle* h, const double* src, double* dst, int iter, doubl
     p.rec = rec;
     p.iter = iter;
     ++h->launches;
-    return launch_step_f64(p, tile, h->stream, 0);
+    if (sizeof(T) == 8) return launch_step_f64(reinterpret_cast<const StepParams<double>&>(p), tile, h->stream, 0);
+    return launch_step_f32(reinterpret_cast<const StepParams<float>&>(p), tile, h->stream, 0);
+}
+
+template <class T>
+int adj_backward(mrlbm_handle* h, const void* src, int iter, bool ovr, const adj::AdjArgs& a) {
+    StepParams<T> p{};
+    fill_common(h, p);
+    const mrlbm_config& c = h->cfg;
+    p.src = (const T*)src;
+    p.u_in = h->has_uin ? (const T*)h->d_uin : nullptr;
+    p.body = h->has_body ? (const T*)h->d_body : nullptr;
+    p.ovr = ovr ? h->d_ovr : nullptr;
+    p.n_ovr = ovr ? (int)h->ovr.size() : 0;
+    p.zero_solid_u = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
+    p.iter = iter;
+    h->launches += 1;
+    return launch_adjoint_step(p, a, h->stream);
 }
 
 }  // namespace
@@ -1093,7 +1111,6 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     if (!h || nsteps < 1 || window < 1 || window > nsteps || checkpoint_every < 1 || !J) return MRLBM_EINVAL;
     if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
     const mrlbm_config& c = h->cfg;
-    if (h->precision != MRLBM_FP64) return fail(h, MRLBM_EUNSUPPORTED, "the adjoint runs on FP64 handles");
     if (c.x_periodic || (c.wall_mode == MRLBM_WALL_REFERENCE && !c.y_periodic) || c.incomp_bc || c.incomp_bulk ||
         (h->geo.nb > 0 && (h->closure != CLOSURE_STRONG || !c.vel_interp || !c.mom_interp)))
         return fail(h, MRLBM_EUNSUPPORTED,
@@ -1103,19 +1120,22 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     if (rc != MRLBM_OK) return rc;
     const int N = nsteps, K = std::min(checkpoint_every, nsteps), T = window;
     const int ncp = (N + K - 1) / K;
-    const size_t LB = (size_t)h->L.total() * sizeof(double);
+    const size_t LB = (size_t)h->L.total() * h->elem;            // a population level
+    const size_t LAM = (size_t)h->L.total() * sizeof(double);     // an adjoint level (FP64)
+    const bool fp64 = h->precision == MRLBM_FP64;
     const int64_t nodes = (int64_t)h->L.nx * h->L.ny;
     const int tile = is_tma_cfg(h->tile_cfg) ? 1 : h->tile_cfg;
     const bool grads = grad_body || grad_uin;
-    std::vector<double*> cp(ncp, nullptr), seg(grads ? K : 0, nullptr);
-    double *work[2] = {nullptr, nullptr}, *lam[2] = {nullptr, nullptr}, *d_rec = nullptr, *gb = nullptr, *gu = nullptr;
+    std::vector<void*> cp(ncp, nullptr), seg(grads ? K : 0, nullptr);
+    void* work[2] = {nullptr, nullptr};
+    double *lam[2] = {nullptr, nullptr}, *d_rec = nullptr, *gb = nullptr, *gu = nullptr;
     auto release = [&]() {
-        for (double* q : cp) if (q) cudaFree(q);
+        for (void* q : cp) if (q) cudaFree(q);
         for (size_t q = 1; q < seg.size(); ++q) if (seg[q]) cudaFree(seg[q]);   // seg[0] borrows a checkpoint
-        for (double* q : {work[0], work[1], lam[0], lam[1], d_rec, gb, gu}) if (q) cudaFree(q);
+        for (void* q : {work[0], work[1], (void*)lam[0], (void*)lam[1], (void*)d_rec, (void*)gb, (void*)gu}) if (q) cudaFree(q);
     };
-    auto alloc_level = [&](double** q) {
-        if (cudaMalloc((void**)q, LB) != cudaSuccess) return false;
+    auto alloc_level = [&](void** q) {
+        if (cudaMalloc(q, LB) != cudaSuccess) return false;
         // every level carries the never-written ghost values of the current state
         return cudaMemcpyAsync(*q, h->buf[h->cur], LB, cudaMemcpyDeviceToDevice, h->stream) == cudaSuccess;
     };
@@ -1125,11 +1145,11 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     ok = ok && alloc_level(&work[0]) && alloc_level(&work[1]) &&
          cudaMalloc((void**)&d_rec, (size_t)N * REC_WORDS * sizeof(double)) == cudaSuccess;
     if (ok && grads)
-        ok = cudaMalloc((void**)&lam[0], LB) == cudaSuccess && cudaMalloc((void**)&lam[1], LB) == cudaSuccess &&
+        ok = cudaMalloc((void**)&lam[0], LAM) == cudaSuccess && cudaMalloc((void**)&lam[1], LAM) == cudaSuccess &&
              cudaMalloc((void**)&gb, (size_t)2 * nodes * sizeof(double)) == cudaSuccess &&
              cudaMalloc((void**)&gu, (size_t)h->L.ny * sizeof(double)) == cudaSuccess &&
-             cudaMemsetAsync(lam[0], 0, LB, h->stream) == cudaSuccess &&
-             cudaMemsetAsync(lam[1], 0, LB, h->stream) == cudaSuccess &&
+             cudaMemsetAsync(lam[0], 0, LAM, h->stream) == cudaSuccess &&
+             cudaMemsetAsync(lam[1], 0, LAM, h->stream) == cudaSuccess &&
              cudaMemsetAsync(gb, 0, (size_t)2 * nodes * sizeof(double), h->stream) == cudaSuccess &&
              cudaMemsetAsync(gu, 0, (size_t)h->L.ny * sizeof(double), h->stream) == cudaSuccess;
     if (!ok) {
@@ -1139,11 +1159,14 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     }
     const int it0 = h->iter;
     // forward pass: F^0 .. F^N, checkpoint F^{cK}, drag records of the window
-    const double* prev = cp[0];
+    auto fwd = [&](const void* a, void* b, int it, double* rec, bool ovr) {
+        return fp64 ? adj_forward<double>(h, a, b, it, rec, ovr, tile) : adj_forward<float>(h, a, b, it, rec, ovr, tile);
+    };
+    const void* prev = cp[0];
     for (int n = 1; n <= N && rc == MRLBM_OK; ++n) {
-        double* dst = work[n & 1];
+        void* dst = work[n & 1];
         double* rec = n > N - T ? d_rec + (size_t)(n - 1) * REC_WORDS : nullptr;
-        if (adj_forward(h, prev, dst, it0 + n, rec, n == 1 && h->ovr_live, tile) != 0) rc = MRLBM_ECUDA;
+        if (fwd(prev, dst, it0 + n, rec, n == 1 && h->ovr_live) != 0) rc = MRLBM_ECUDA;
         if (n % K == 0 && n / K < ncp && cudaMemcpyAsync(cp[n / K], dst, LB, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
             rc = MRLBM_ECUDA;
         prev = dst;
@@ -1164,19 +1187,9 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
         const int n0 = cseg * K, m = std::min(K, N - n0);
         seg[0] = cp[cseg];
         for (int t = 1; t < m && rc == MRLBM_OK; ++t)
-            if (adj_forward(h, seg[t - 1], seg[t], it0 + n0 + t, nullptr, n0 + t == 1 && h->ovr_live, tile) != 0) rc = MRLBM_ECUDA;
+            if (fwd(seg[t - 1], seg[t], it0 + n0 + t, nullptr, n0 + t == 1 && h->ovr_live) != 0) rc = MRLBM_ECUDA;
         for (int n = n0 + m; n > n0 && rc == MRLBM_OK; --n) {
             const int t = n - n0 - 1;                  // seg[t] = F^{n-1}
-            StepParams<double> p{};
-            fill_common(h, p);
-            p.src = seg[t];
-            p.u_in = h->has_uin ? h->d_uin : nullptr;
-            p.body = h->has_body ? (const double*)h->d_body : nullptr;
-            p.ovr = (n == 1 && h->ovr_live) ? h->d_ovr : nullptr;
-            p.n_ovr = p.ovr ? (int)h->ovr.size() : 0;
-            const int iter = it0 + n;
-            p.zero_solid_u = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
-            p.iter = iter;
             adj::AdjArgs a{};
             a.lam_in = lam[li];
             a.lam_out = lam[li ^ 1];
@@ -1184,8 +1197,9 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             a.grad_uin = gu;
             a.wJ = n > N - T ? 1.0 / T : 0.0;
             a.n_edge = 2 * h->L.ny;
-            h->launches += 3;
-            if (launch_adjoint_step(p, a, h->stream) != 0) rc = MRLBM_ECUDA;
+            const bool ovr = n == 1 && h->ovr_live;
+            if ((fp64 ? adj_backward<double>(h, seg[t], it0 + n, ovr, a) : adj_backward<float>(h, seg[t], it0 + n, ovr, a)) != 0)
+                rc = MRLBM_ECUDA;
             li ^= 1;
         }
     }

@@ -64,12 +64,16 @@ int batch_blocks_per_sm_f64(int tile_cfg) {
 }
 
 // Adjoint step (adjoint.cuh): one launch with wall, edge-column and bulk blocks.
-int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s) {
+template <class T>
+static int launch_adjoint(const StepParams<T>& p, const adj::AdjArgs& a, cudaStream_t s) {
     const int64_t nodes = (int64_t)p.L.nx * p.L.ny;
     const int64_t blocks = (int64_t)p.nb + (a.n_edge + 6) / 7 + (nodes + 127) / 128;
-    adj::adjoint_step<<<(unsigned)blocks, 128, 0, s>>>(p, a);
+    adj::adjoint_step<StepParams<T>><<<(unsigned)blocks, 128, 0, s>>>(p, a);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
+
+int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s) { return launch_adjoint(p, a, s); }
+int launch_adjoint_step(const StepParams<float>& p, const adj::AdjArgs& a, cudaStream_t s) { return launch_adjoint(p, a, s); }
 
 int launch_surface_f64(const StepParams<double>& p, const SurfaceTables& t, double* rec, double* prec, cudaStream_t s) {
     return surf::launch_surface(p, t, rec, prec, s);
