@@ -45,6 +45,8 @@ def parse():
                     help="bulk tile shape (default: chosen by the autotuner before timing)")
     ap.add_argument("--large-steps", type=int, default=30,
                     help="timed steps of the 16384 x 4096 roofline case at N=1 (0: skip)")
+    ap.add_argument("--fields", action="store_true",
+                    help="with --profile: accumulate the FP64 field statistics in every step")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps of the case (for ncu); prints nothing else")
     return ap.parse_args()
@@ -245,6 +247,8 @@ def run_profile(args):
     sim = m.Simulation(cfg, precision=args.precision or 32)
     if args.tile is not None:
         sim.tile_config = args.tile
+    if args.fields:
+        sim.field_stats_window(1, 10 ** 9)
     sim.step(args.warmup)
     sim.step(args.steps)
     st = sim.status()

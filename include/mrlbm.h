@@ -241,7 +241,9 @@ int mrlbm_get_tile_config(const mrlbm_handle* h, int32_t* cfg);
 
 /* Autotuner: time every tile shape for trial_steps steps on this handle's own case (after one
  * warm-up step each), keep the fastest, and restore the populations, the iteration counter
- * and the force history, so a simulation is unaffected.  Returns the chosen shape and its
+ * and the force history, so a simulation is unaffected.  Trial steps record no surface
+ * pressure; with a field-statistics window they accumulate like the run will (so the choice
+ * fits it) into sums that are saved beforehand and put back.  Returns the chosen shape and its
  * time per step in milliseconds. */
 int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, double* best_ms);
 

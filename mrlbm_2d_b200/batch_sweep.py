@@ -29,6 +29,7 @@ def main(argv=None):
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--trial-steps", type=int, default=50)
     ap.add_argument("--seed", type=int, default=4242)
+    ap.add_argument("--no-sequential", action="store_true", help="skip the one-case-at-a-time baseline")
     a = ap.parse_args(argv)
     import torch
     cfgs = sweep_cases(a.cases, seed=a.seed)
@@ -71,6 +72,9 @@ def main(argv=None):
     out["finite_forces_of_stable_cases"] = bool(np.all(np.isfinite(drag)))
     b.close()
 
+    if a.no_sequential:
+        print(json.dumps(out), flush=True)
+        return out
     seq_el = 0.0
     st = torch.cuda.Stream()
     for cfg in cfgs:

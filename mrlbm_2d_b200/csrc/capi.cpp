@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -1006,8 +1007,32 @@ int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, doub
     const int iter0 = h->iter, cur0 = h->cur, ring0 = h->ring_n;
     const bool ovr0 = h->ovr_live;
     const size_t hist0 = h->hist.size();
+    // trials record no surface pressure; with a field-statistics window the trials accumulate
+    // too (the choice fits that workload) into sums saved here and put back afterwards
+    const bool surf0 = h->surf_on;
+    const int32_t fsb0 = h->fstat_begin, fse0 = h->fstat_end;
+    const int64_t fsn0 = h->fstat_n;
+    const size_t fbytes = (size_t)6 * h->L.nx * h->L.ny * sizeof(double);
+    double* fsave = nullptr;
+    h->surf_on = false;
+    if (h->d_fstat) {
+        if (cudaMalloc((void**)&fsave, fbytes) != cudaSuccess ||
+            cudaMemcpyAsync(fsave, h->d_fstat, fbytes, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess) {
+            if (fsave) cudaFree(fsave);
+            fsave = nullptr;
+            h->fstat_begin = 1;                        // no room to save the sums: trials without them
+            h->fstat_end = 0;
+        } else {
+            h->fstat_begin = std::numeric_limits<int32_t>::min();
+            h->fstat_end = std::numeric_limits<int32_t>::max();
+        }
+    }
     for (int b = 0; b < 2; ++b)
         if (cudaMemcpyAsync(save[b], h->buf[b], bytes, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess) {
+            h->surf_on = surf0;
+            h->fstat_begin = fsb0;
+            h->fstat_end = fse0;
+            if (fsave) cudaFree(fsave);
             cleanup();
             return fail(h, MRLBM_ECUDA, "autotune save copy");
         }
@@ -1039,6 +1064,15 @@ int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, doub
         h->ring_n = ring0;
         h->ovr_live = ovr0;
         h->hist.resize(hist0);
+    }
+    h->surf_on = surf0;
+    h->fstat_begin = fsb0;
+    h->fstat_end = fse0;
+    h->fstat_n = fsn0;
+    if (fsave) {
+        cudaMemcpyAsync(h->d_fstat, fsave, fbytes, cudaMemcpyDeviceToDevice, h->stream);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(fsave);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -57,19 +57,39 @@ __device__ __forceinline__ void store_macro(const StepParams<T>& p, int i, int j
 // Field statistics: this step's post-closure u, v and p = rho cs2 (cs2 = 1/3, 2d_mrlbm.f90:153,
 // 237) added to FP64 running sums of x and x^2.  Explicit round-to-nearest operations keep the
 // sums free of contraction in every build, so they equal a host loop adding the same fields.
+// The six old sums of a node are loaded (read-only path; each slot belongs to one thread of
+// the launch) before the node's arithmetic, so their latency overlaps it.
+struct FieldPre { double v[6]; };
+
 template <class T>
-__device__ __forceinline__ void accumulate_fields(const StepParams<T>& p, int i, int j, double rho, double ux,
-                                                  double uy) {
+__device__ __forceinline__ void fields_load(const StepParams<T>& p, int i, int j, FieldPre& q) {
+    const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1);
+    const int64_t N = (int64_t)p.L.nx * p.L.ny;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) q.v[c] = __ldg(p.fstat + n + c * N);
+}
+
+template <class T>
+__device__ __forceinline__ void fields_store(const StepParams<T>& p, int i, int j, const FieldPre& q, double rho,
+                                             double ux, double uy) {
     const int64_t n = (int64_t)(i - 1) + (int64_t)p.L.nx * (j - 1);
     const int64_t N = (int64_t)p.L.nx * p.L.ny;
     const double pr = __dmul_rn(rho, 1.0 / 3.0);
     double* a = p.fstat + n;
-    a[0] = __dadd_rn(a[0], ux);
-    a[N] = __dadd_rn(a[N], uy);
-    a[2 * N] = __dadd_rn(a[2 * N], pr);
-    a[3 * N] = __dadd_rn(a[3 * N], __dmul_rn(ux, ux));
-    a[4 * N] = __dadd_rn(a[4 * N], __dmul_rn(uy, uy));
-    a[5 * N] = __dadd_rn(a[5 * N], __dmul_rn(pr, pr));
+    a[0] = __dadd_rn(q.v[0], ux);
+    a[N] = __dadd_rn(q.v[1], uy);
+    a[2 * N] = __dadd_rn(q.v[2], pr);
+    a[3 * N] = __dadd_rn(q.v[3], __dmul_rn(ux, ux));
+    a[4 * N] = __dadd_rn(q.v[4], __dmul_rn(uy, uy));
+    a[5 * N] = __dadd_rn(q.v[5], __dmul_rn(pr, pr));
+}
+
+template <class T>
+__device__ __forceinline__ void accumulate_fields(const StepParams<T>& p, int i, int j, double rho, double ux,
+                                                  double uy) {
+    FieldPre q;
+    fields_load(p, i, j, q);
+    fields_store(p, i, j, q, rho, ux, uy);
 }
 
 // Body force (an extension: the reference has no forcing term).  A first-order momentum

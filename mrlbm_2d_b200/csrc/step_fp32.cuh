@@ -279,11 +279,13 @@ __device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls)
 
 // Interior fluid or solid node: populations already gathered.
 __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const float g[Q], float go[Q]) {
+    FieldPre pre;
+    if (p.fstat) fields_load(p, i, j, pre);
     Mac m = moments(p, g);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
+    if (p.fstat) fields_store(p, i, j, pre, 1.0 + (double)m.drho, m.ux, m.uy);
     collide(p, m, go);
     if (p.body) add_body_force(p, i, j, go);
 }

@@ -407,11 +407,13 @@ __device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls)
 // Bulk node (fluid or solid).
 // Interior fluid or solid node: populations already gathered.
 __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const double f[Q], double fo[Q]) {
+    FieldPre pre;
+    if (p.fstat) fields_load(p, i, j, pre);
     Mac m = moments(f, p.hm, p.hp);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
     if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
+    if (p.fstat) fields_store(p, i, j, pre, m.rho, m.ux, m.uy);
     collide(p, m, fo);
     if (p.body) add_body_force(p, i, j, fo);
 }

@@ -84,3 +84,27 @@ def test_field_stats_window_rules(mrlbm):
     s.step(3)
     assert s.field_stats()["n"] == 3
     s.close()
+
+
+def test_autotune_keeps_field_sums_and_surface_records(mrlbm):
+    """The autotuner's trial steps leave the field sums, their count and the surface-pressure
+    records as they were: a tuned run equals an untuned one."""
+    cfg = CASES["freeslip_label15"]()
+    out = []
+    for tune in (False, True):
+        s = mrlbm.Simulation(cfg)
+        s.field_stats_window(3, 40)
+        s.surface_enable()
+        s.step(10)
+        if tune:
+            s.autotune(trial_steps=3)
+        s.step(20)
+        fs = s.field_stats()
+        it, ps, pf, pr = s.surface()
+        out.append((fs, it, ps))
+        s.close()
+    (f0, i0, p0), (f1, i1, p1) = out
+    assert f0["n"] == f1["n"] == 29
+    for k in ("mean_u", "rms_v", "mean_p", "rms_p"):
+        assert np.array_equal(f0[k], f1[k]), k
+    assert np.array_equal(i0, i1) and np.array_equal(p0, p1)
