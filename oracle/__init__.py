@@ -96,6 +96,13 @@ class Oracle:
         keys = ["nx", "ny", "nbct", "iter", "r_cyl", "nu", "omega", "x_c", "y_c", "r_c", "rho_inf_mean"]
         return dict(zip(keys, out.tolist()))
 
+    def surface(self):
+        """(p_surface (n, nbct), p_smooth (n, nbct), probes (n, 12)) of the stats steps so far."""
+        ps, pf, pr = self.get("p_surface"), self.get("p_surface_smooth"), self.get("probes")
+        n = pr.size // 12
+        nb = ps.size // n if n else 0
+        return ps.reshape(n, nb), pf.reshape(n, nb), pr.reshape(n, 12)
+
     def forces(self):
         n = lib().orc_forces(self._h, None, None, None, None, 0)
         it = np.zeros(n, np.int32)

@@ -95,6 +95,9 @@ struct Oracle {
     double rho_inf_mean = 0.0, rho_infty = 1.0;
     std::vector<int> h_iter;
     std::vector<double> h_fd, h_fl, h_rhoin;
+    std::vector<double> h_psurf, h_psmooth, h_probe;   // per stats step: nbct, nbct, 12 values
+    int i_probe[4] = {0, 0, 0, 0}, j_probe[4] = {0, 0, 0, 0};
+    void write_statistics_out();                       // 2d_mrlbm.f90:593-616 (records, no files)
     std::string err;
 
     inline size_t I(int i, int j) const { return (size_t)(i - 1) + (size_t)nx * (size_t)(j - 1); }
@@ -136,12 +139,25 @@ bool Oracle::setup(const mrlbm_config& c) {
         x_c = (double)(float)(nfront + (c.ncy / 2) + 1);            // 2d_mrlbm.f90:946-948
         y_c = (double)(float)(nbot + c.ncy / 2);
         r_c = (double)(float)(c.ncy / 2);
+        const int base = nfront + c.ncy + 1;                        // probes, 2d_mrlbm.f90:102-109
+        i_probe[0] = base + (c.ncy / 2); i_probe[1] = base + c.ncy;
+        i_probe[2] = base + (3 * c.ncy / 2); i_probe[3] = base + (2 * c.ncy);
+        for (int q = 0; q < 4; ++q) j_probe[q] = nbot + (c.ncy / 2) + 1;
     } else {
         nx = c.nx;
         ny = c.ny;
         x_c = c.x_c;
         y_c = c.y_c;
         r_c = c.r_c;
+        // extension: probes 1, 1.5, 2 and 2.5 diameters behind the centre, one row above it
+        for (int q = 0; q < 4; ++q) {
+            i_probe[q] = (int)std::floor(x_c + (1.0 + 0.5 * q) * 2.0 * r_c + 0.5);
+            j_probe[q] = (int)std::floor(y_c) + 1;
+        }
+    }
+    for (int q = 0; q < 4; ++q) {                                   // keep probe reads in range
+        i_probe[q] = std::min(std::max(i_probe[q], 1), nx);
+        j_probe[q] = std::min(std::max(j_probe[q], 1), ny);
     }
     if (nx < 4 || ny < 4) { err = "nx and ny must be >= 4"; return false; }
     const size_t N = (size_t)nx * ny;
@@ -960,6 +976,11 @@ void Oracle::step() {
         h_fd.push_back(fd);
         h_fl.push_back(fl);
         h_rhoin.push_back(rho_in_sum);
+        // probe records (2d_mrlbm.f90:470-475) and the surface pressure (2d_mrlbm.f90:478)
+        for (int q = 0; q < 4; ++q) h_probe.push_back(rho[I(i_probe[q], j_probe[q])] / 3.0);
+        for (int q = 0; q < 4; ++q) h_probe.push_back(ux[I(i_probe[q], j_probe[q])] / 3.0);
+        for (int q = 0; q < 4; ++q) h_probe.push_back(uy[I(i_probe[q], j_probe[q])] / 3.0);
+        write_statistics_out();
     } else if (in_stats) {
         h_iter.push_back(iter);
         h_fd.push_back(0.0);
@@ -1012,6 +1033,49 @@ void Oracle::step() {
 
 // ---------------------------------------------------------------------------------------
 // ctypes surface (test infrastructure)
+// write_statistics_out (2d_mrlbm.f90:593-616): extrapolate_var_on_cylinder on p
+// (2d_mrlbm.f90:619-672), quadratic_interpolation (2d_mrlbm.f90:742-766), reorder by theta,
+// gaussian_smoothing (2d_mrlbm.f90:718-740); the two unformatted records become history rows.
+void Oracle::write_statistics_out() {
+    std::vector<double> p_cy(nbct), ps(nbct), fit(nbct);
+    for (int k = 1; k <= nbct; ++k) {
+        double var[5];
+        for (int r = 2; r <= 4; ++r) {
+            const double xd = (x_ref[r][k - 1] - X(IP(r, 0, k))) / dx;
+            const double yd = (y_ref[r][k - 1] - Y(JP(r, 0, k))) / dy;
+            const double v0 = (1.0 - xd) * p[I(IP(r, 0, k), JP(r, 0, k))] + xd * p[I(IP(r, 1, k), JP(r, 1, k))];
+            const double v1 = (1.0 - xd) * p[I(IP(r, 2, k), JP(r, 2, k))] + xd * p[I(IP(r, 3, k), JP(r, 3, k))];
+            var[r] = (1.0 - yd) * v0 + yd * v1;
+        }
+        const double xs = x_ref[1][k - 1] - x_c, ys = y_ref[1][k - 1] - y_c;
+        const double x1 = x_ref[2][k - 1] - x_c, y1 = y_ref[2][k - 1] - y_c;
+        const double x2 = x_ref[3][k - 1] - x_c, y2 = y_ref[3][k - 1] - y_c;
+        const double x3 = x_ref[4][k - 1] - x_c, y3 = y_ref[4][k - 1] - y_c;
+        const double p1 = var[2], p2 = var[3], p3 = var[4];
+        const double r1 = std::sqrt((x1 * x1) + (y1 * y1)), r2 = std::sqrt((x2 * x2) + (y2 * y2));
+        const double r3 = std::sqrt((x3 * x3) + (y3 * y3)), rs = std::sqrt((xs * xs) + (ys * ys));
+        const double denom = (r1 - r2) * (r1 - r3) * (r2 - r3);
+        const double a0 = (r1 * r3 * p2 * (r3 - r1) + (r2 * r2) * (r3 * p1 - r1 * p3) + r2 * ((r1 * r1) * p3 - (r3 * r3) * p1)) / denom;
+        const double a1 = ((r3 * r3) * (p1 - p2) + (r1 * r1) * (p2 - p3) + (r2 * r2) * (p3 - p1)) / denom;
+        const double a2 = (r3 * (p2 - p1) + r2 * (p1 - p3) + r1 * (p3 - p2)) / denom;
+        p_cy[k - 1] = a0 + a1 * rs + a2 * (rs * rs);
+    }
+    for (int k = 1; k <= nbct; ++k) ps[k - 1] = p_cy[idx[k - 1] - 1];
+    const double sigma = 0.1;
+    for (int i = 1; i <= nbct; ++i) {
+        double sw = 0.0, sv = 0.0;
+        for (int j = 1; j <= nbct; ++j) {
+            const double d = thetas_cy[i - 1] - thetas_cy[j - 1];
+            const double wgt = std::exp(-(d * d) / (2.0 * (sigma * sigma)));
+            sw = sw + wgt;
+            sv = sv + wgt * ps[j - 1];
+        }
+        fit[i - 1] = sv / sw;
+    }
+    h_psurf.insert(h_psurf.end(), ps.begin(), ps.end());
+    h_psmooth.insert(h_psmooth.end(), fit.begin(), fit.end());
+}
+
 extern "C" {
 
 void* orc_create(const mrlbm_config* cfg, char* errbuf, int errlen) {
@@ -1057,7 +1121,8 @@ static const std::vector<double>* dvec(Oracle* o, const char* name) {
         {"theta_c", &o->theta_c}, {"thetas_cy", &o->thetas_cy}, {"x_ref1", &o->x_ref[1]}, {"y_ref1", &o->y_ref[1]},
         {"x_ref2", &o->x_ref[2]}, {"y_ref2", &o->y_ref[2]}, {"x_ref3", &o->x_ref[3]}, {"y_ref3", &o->y_ref[3]},
         {"x_ref4", &o->x_ref[4]}, {"y_ref4", &o->y_ref[4]}, {"F_drag", &o->F_drag}, {"F_lift", &o->F_lift},
-        {"uxp_b", &o->uxp_b}, {"uyp_b", &o->uyp_b},
+        {"uxp_b", &o->uxp_b}, {"uyp_b", &o->uyp_b}, {"p_surface", &o->h_psurf}, {"p_surface_smooth", &o->h_psmooth},
+        {"probes", &o->h_probe},
     };
     for (auto& e : t)
         if (std::strcmp(e.n, name) == 0) return e.v;

@@ -71,6 +71,13 @@ def test_oracle_matches_reference_execution(mrlbm, oracle_mod, tmp_path, name):
     ref = d["forces"]
     assert np.array_equal(its, ref[:, 0].astype(int))
     assert np.array_equal(fd, ref[:, 1]) and np.array_equal(fl, ref[:, 2])
+    # write_statistics_out and the probe records (2d_mrlbm.f90:468-478, 593-616)
+    ps, pf, pr = o.surface()
+    assert np.array_equal(ps, d["p_surface"][:, 1:]), "surface pressure"
+    assert np.array_equal(pf, d["p_surface_smooth"][:, 1:]), "smoothed surface pressure"
+    for q, key in enumerate(("probe_p", "probe_ux", "probe_uy")):
+        if d[key].size:
+            assert np.array_equal(pr[:, 4 * q:4 * q + 4], d[key][:, 1:]), key
 
 
 @pytest.mark.gpu
