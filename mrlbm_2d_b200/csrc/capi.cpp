@@ -1530,7 +1530,7 @@ int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h) {
 }
 
 int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch) {
-    if (!b || tile_cfg < VEC_CFG0 || tile_cfg >= N_ALL_CFGS || steps_per_launch < 1 || steps_per_launch > RING_CAP ||
+    if (!b || !is_vec_cfg(tile_cfg) || steps_per_launch < 1 || steps_per_launch > RING_CAP ||
         (schedule != MRLBM_BATCH_PERSISTENT && schedule != MRLBM_BATCH_GRAPH))
         return MRLBM_EINVAL;
     b->tile_cfg = tile_cfg;
@@ -1642,7 +1642,7 @@ int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_pe
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const int steps = std::min(trial_steps, RING_CAP);
-    for (int cfg = VEC_CFG0; cfg < N_ALL_CFGS && rc == MRLBM_OK; ++cfg) {
+    for (int cfg = VEC_CFG0; cfg < PIPE_CFG0 && rc == MRLBM_OK; ++cfg) {
         for (int sched = MRLBM_BATCH_PERSISTENT; sched <= MRLBM_BATCH_GRAPH && rc == MRLBM_OK; ++sched) {
             b->tile_cfg = cfg;
             b->schedule = sched;

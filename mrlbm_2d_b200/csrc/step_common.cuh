@@ -8,6 +8,7 @@
 //   static void stencil_node(...), boundary_close(...);               // curved-wall nodes
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include "step_params.h"
 
 namespace mrlbm {
@@ -460,6 +461,70 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
     const int tiles_y = (p.L.ny + WARPS * NJ - 1) / (WARPS * NJ);
     const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
     step_kernel_vec<Phys, WARPS, NJ, MINB><<<(unsigned)nblocks, nthr, 0, s>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// ---- persistent software-pipelined bulk path -------------------------------------------------
+// A fixed grid of resident blocks walks the row segments of the lattice (segment u: row
+// 1 + u / tiles_x, columns (u % tiles_x) * B + 1 ..) with a stride of the grid size.  Each
+// thread loads the populations of its next node before it collides and stores the current
+// one, so a load is always in flight behind the arithmetic and no block waits out a tail
+// wave.  Edge and wall nodes are skipped (edge and boundary blocks own them).
+template <class Phys, int B, int MINB>
+__global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constant__ typename Phys::P p) {
+    using T = typename Phys::T;
+    if (run_aux_block<Phys>(p)) return;
+    const int nx = p.L.nx, ny = p.L.ny, tiles_x = p.tiles_x;
+    const int units = tiles_x * ny;
+    const int G = (int)gridDim.x - p.nbblk - p.neblk;
+    auto fetch = [&](int u, T (&f)[Q], int& i, int& j) -> bool {
+        if (u >= units) return false;
+        j = 1 + u / tiles_x;
+        i = 1 + (u - (j - 1) * tiles_x) * B + (int)threadIdx.x;
+        if (!(i > 1 && i < nx && j > 1 && j < ny)) return false;
+        gather_interior(p, i, j, f);
+        return true;
+    };
+    int u = (int)blockIdx.x - p.nbblk - p.neblk;
+    T a[Q], b[Q];
+    int ia = 0, ja = 0, ib = 0, jb = 0;
+    bool va = fetch(u, a, ia, ja);
+    while (u < units) {
+        const int un = u + G;
+        const bool vb = fetch(un, b, ib, jb);
+        if (va) {
+            const int cls = node_class(p, ia, ja);
+            if (cls < 0) Phys::finish(p, ia, ja, cls, a);     // cls >= 0: curved-wall node
+        }
+#pragma unroll
+        for (int k = 0; k < Q; ++k) a[k] = b[k];
+        ia = ib;
+        ja = jb;
+        va = vb;
+        u = un;
+    }
+}
+
+template <class Phys, int B, int MINB>
+int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
+    static_assert(B % BLANES == 0 && B / BLANES <= BNODES, "boundary block size");
+    static int per_sm[64] = {0}, sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 64) return -1;
+    if (!per_sm[dev]) {
+        if (cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], step_kernel_pipe<Phys, B, MINB>, B, 0) !=
+                cudaSuccess || per_sm[dev] <= 0)
+            return -1;
+    }
+    const int bn = B / BLANES;
+    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
+    p.neblk = edge_blocks(p.L.nx, p.L.ny, B);
+    p.tiles_x = (p.L.nx + B - 1) / B;
+    const long long units = (long long)p.tiles_x * p.L.ny;
+    const long long G = std::min<long long>(units, (long long)sms[dev] * per_sm[dev]);
+    step_kernel_pipe<Phys, B, MINB><<<(unsigned)(p.nbblk + p.neblk + G), B, 0, s>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

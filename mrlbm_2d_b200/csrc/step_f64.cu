@@ -24,6 +24,10 @@ int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int
     case id: return launch_step_vec<Ph, w, nj, mb>(p, s);
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
+#define MRLBM_PIPE_CASE(id, b, mb) \
+    case id: return launch_step_pipe<Ph, b, mb>(p, s);
+        MRLBM_PIPE_LIST(MRLBM_PIPE_CASE)
+#undef MRLBM_PIPE_CASE
     default: return -1;
     }
 }

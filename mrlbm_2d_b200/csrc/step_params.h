@@ -132,8 +132,20 @@ struct VecCfg { int warps, nj, minb; };
 constexpr VecCfg VEC_CFGS[N_VEC_CFGS] = {MRLBM_VEC_LIST(MRLBM_VEC_ENTRY)};
 #undef MRLBM_VEC_ENTRY
 constexpr int VEC_CFG0 = TMA_CFG0 + N_TMA_CFGS;
-constexpr int N_ALL_CFGS = VEC_CFG0 + N_VEC_CFGS;
+
+// Persistent software-pipelined shapes of step_kernel_pipe (B threads per block, MINB
+// resident blocks per SM; the grid is the resident set).
+#define MRLBM_PIPE_LIST(X) \
+    X(22, 128, 8)          \
+    X(23, 256, 4)          \
+    X(24, 128, 6)          \
+    X(25, 256, 3)          \
+    X(26, 128, 4)
+constexpr int N_PIPE_CFGS = 5;
+constexpr int PIPE_CFG0 = VEC_CFG0 + N_VEC_CFGS;
+constexpr int N_ALL_CFGS = PIPE_CFG0 + N_PIPE_CFGS;
 inline bool is_tma_cfg(int c) { return c >= TMA_CFG0 && c < VEC_CFG0; }
+inline bool is_vec_cfg(int c) { return c >= VEC_CFG0 && c < PIPE_CFG0; }
 
 // Host-side launch entry points (step_f64.cu / step_f32.cu).  `workers` is the persistent
 // CTA count for TMA shapes (ignored otherwise).  Return 0, -1 on a launch error, -2 when the
