@@ -156,3 +156,24 @@ def test_adjoint_rejects_unsupported_cases(mrlbm):
     with pytest.raises(mrlbm.MrlbmError):
         s.adjoint_drag(10, 5, 5)
     s.close()
+
+
+def test_adjoint_y_periodic_case_matches_central_differences(mrlbm):
+    """Top and bottom y-periodic instead of free-slip (another streaming map for the edge
+    rows), inlet-profile direction only."""
+    cfg = cylinder_case(96, 40, 8, 24.0, 20.5, 100.0, 0.05, seed=13, noise=1e-2).replace(y_periodic=1)
+    s = mrlbm.Simulation(cfg)
+    _, uin = _params(s, 8)
+    s.set_inlet_profile(uin)
+    N, T, K = 150, 60, 50
+    J, gb, gu = s.adjoint_drag(N, T, K)
+    du = 1e-3 * np.random.default_rng(3).standard_normal(uin.shape)
+    eps = 1e-4
+    vals = []
+    for sgn in (1.0, -1.0):
+        s.set_inlet_profile(uin + sgn * eps * du)
+        vals.append(s.adjoint_drag(N, T, K, grads=False))
+    fd = (vals[0] - vals[1]) / (2 * eps)
+    ad = float((gu * du).sum())
+    assert abs(ad - fd) <= 1e-3 * abs(fd), (ad, fd)
+    s.close()

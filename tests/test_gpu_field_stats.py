@@ -108,3 +108,23 @@ def test_autotune_keeps_field_sums_and_surface_records(mrlbm):
     for k in ("mean_u", "rms_v", "mean_p", "rms_p"):
         assert np.array_equal(f0[k], f1[k]), k
     assert np.array_equal(i0, i1) and np.array_equal(p0, p1)
+
+
+def test_fp32_surface_pressure_tracks_fp64(mrlbm):
+    """Wall pressure, its smoothing and the probes from an FP32 handle (deviation storage read
+    back as w + g in FP64) against the FP64 handle, after 300 steps of the 400 x 100 case."""
+    cfg = CASES["benchmark_small_400x100"]()
+    out = {}
+    for prec in (64, 32):
+        s = mrlbm.Simulation(cfg, precision=prec)
+        s.surface_enable()
+        s.step(300)
+        out[prec] = s.surface()
+        assert s.probe_nodes() == [(100, 51), (110, 51), (120, 51), (130, 51)]
+        s.close()
+    it64, ps64, pf64, pr64 = out[64]
+    it32, ps32, pf32, pr32 = out[32]
+    assert np.array_equal(it32, it64) and len(it64) == 300
+    assert np.abs(ps32 - ps64).max() < 1e-6          # p ~ 1/3; deviations ~1e-4
+    assert np.abs(pf32 - pf64).max() < 1e-6
+    assert np.abs(pr32 - pr64).max() < 1e-6
