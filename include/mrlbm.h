@@ -232,11 +232,13 @@ int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32
  * (TMA_CFGS there); shapes 16..21 read and write 16 bytes per lane and plane, with the
  * neighbouring columns exchanged by warp shuffles (MRLBM_VEC_LIST there); shapes 22..26 are
  * resident grids that walk the rows with the next node's loads issued before the current
- * node's arithmetic (MRLBM_PIPE_LIST there).  Every shape computes the same bits.  The default is 1; MRLBM_TILE_CFG in
+ * node's arithmetic (MRLBM_PIPE_LIST there); shapes 27..30 are TMA shapes whose fully interior
+ * tiles are written back by tensor stores from a shared-memory output tile (MRLBM_TMAS_LIST).
+ * Every shape computes the same bits.  The default is 1; MRLBM_TILE_CFG in
  * the environment overrides it at creation.  A shape that does not fit the handle's precision
  * makes the next mrlbm_step return MRLBM_EUNSUPPORTED.  mrlbm_step_noalloc runs shape 1 when a
  * TMA shape is selected (its counters live in the handle). */
-#define MRLBM_N_TILE_CONFIGS 27
+#define MRLBM_N_TILE_CONFIGS 31
 int mrlbm_set_tile_config(mrlbm_handle* h, int32_t cfg);
 int mrlbm_get_tile_config(const mrlbm_handle* h, int32_t* cfg);
 

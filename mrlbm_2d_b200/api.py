@@ -21,7 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmrlbm.so")
 
 FP64, FP32 = 64, 32
-N_TILE_CONFIGS = 27   # MRLBM_N_TILE_CONFIGS: 0..9 tiles, 10..15 TMA-fed persistent, 16..21 128-bit vector, 22..26 pipelined
+N_TILE_CONFIGS = 31   # MRLBM_N_TILE_CONFIGS: 0..9 tiles, 10..15 TMA, 16..21 128-bit vector, 22..26 pipelined, 27..30 TMA + tensor stores
 STEP_MACRO = 1
 
 EXPORTED = [

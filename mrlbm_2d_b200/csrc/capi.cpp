@@ -88,6 +88,7 @@ struct mrlbm_handle {
     unsigned long long tile_base = 0;
     int tmap_cfg = -1;
     CUtensorMap tmap[2];
+    CUtensorMap tmap_st[2];                   // store maps (box BX x BY) of the TMA-store shapes
     int workers = 0;
     int num_sms = 0;
 };
@@ -304,6 +305,13 @@ int prepare_tma(mrlbm_handle* h, int cfg) {
                          2, h->buf[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return fail(h, MRLBM_EUNSUPPORTED, "tensor map encoding failed");
+        if (is_tma_store_cfg(cfg)) {
+            cuuint32_t sbox[2] = {(cuuint32_t)tma_cfg(cfg).bx, (cuuint32_t)bh};
+            r = enc(&h->tmap_st[b], h->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                    h->buf[b], dims, strides, sbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return fail(h, MRLBM_EUNSUPPORTED, "store tensor map encoding failed");
+        }
     }
     h->workers = h->num_sms * per_sm;
     h->tmap_cfg = cfg;
@@ -381,6 +389,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.fstat = fstat ? h->d_fstat : nullptr;
         if (tma) {
             p.tmap = h->tmap[h->cur];
+            p.tmap_st = h->tmap_st[1 - h->cur];
             p.tile_ctr = h->d_tile_ctr;
             p.tile_base = h->tile_base;
         }
@@ -402,6 +411,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         p.fstat = fstat ? h->d_fstat : nullptr;
         if (tma) {
             p.tmap = h->tmap[h->cur];
+            p.tmap_st = h->tmap_st[1 - h->cur];
             p.tile_ctr = h->d_tile_ctr;
             p.tile_base = h->tile_base;
         }
@@ -419,7 +429,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     if (tma) {
         int bw, bh, st;
         tma_box(h->precision, tc, &bw, &bh, &st);
-        h->tile_base += tma_claims_host(h->L.nx, h->L.ny, TMA_CFGS[tc - TMA_CFG0].bx, bh, st, h->workers);
+        h->tile_base += tma_claims_host(h->L.nx, h->L.ny, tma_cfg(tc).bx, bh, st, h->workers);
     }
     if (stats && h->surf_on) {
         int src = surface_step(h);
@@ -857,7 +867,10 @@ int mrlbm_step(mrlbm_handle* h, int32_t nsteps, int32_t flags) {
                           (c.channel_with_cylinder || c.channel_with_square);
         const bool macro = (flags & MRLBM_STEP_MACRO) && s == nsteps - 1;
         int rc = launch_one(h, stats, plot, macro);
-        if (rc != MRLBM_OK) return rc;
+        if (rc != MRLBM_OK) {
+            if (rc == MRLBM_EUNSUPPORTED) h->iter -= 1;      // nothing was launched
+            return rc;
+        }
         if (h->ring_n == RING_CAP) {
             rc = drain_ring(h);
             if (rc != MRLBM_OK) return rc;
@@ -1046,7 +1059,11 @@ int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, doub
     for (int c = 0; c < N_ALL_CFGS && rc == MRLBM_OK; ++c) {
         h->tile_cfg = c;
         rc = mrlbm_step(h, 1, 0);                       // warm-up (and instruction cache)
-        if (rc == MRLBM_EUNSUPPORTED) { rc = MRLBM_OK; continue; }   // shape does not fit
+        if (rc == MRLBM_EUNSUPPORTED) {                 // shape does not fit: nothing ran
+            rc = MRLBM_OK;
+            h->iter = iter0;
+            continue;
+        }
         if (rc != MRLBM_OK) break;
         cudaEventRecord(e0, h->stream);
         rc = mrlbm_step(h, trial_steps, 0);

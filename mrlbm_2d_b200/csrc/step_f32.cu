@@ -14,9 +14,13 @@ int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int 
         MRLBM_TILE_LIST(MRLBM_TILE_CASE)
 #undef MRLBM_TILE_CASE
 #define MRLBM_TMA_CASE(id, bx, by, st) \
-    case id: return launch_step_tma<Ph, bx, by, st>(p, s, workers);
+    case id: return launch_step_tma<Ph, bx, by, st, false>(p, s, workers);
         MRLBM_TMA_LIST(MRLBM_TMA_CASE)
 #undef MRLBM_TMA_CASE
+#define MRLBM_TMAS_CASE(id, bx, by, st) \
+    case id: return launch_step_tma<Ph, bx, by, st, true>(p, s, workers);
+        MRLBM_TMAS_LIST(MRLBM_TMAS_CASE)
+#undef MRLBM_TMAS_CASE
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
     case id: return launch_step_vec<Ph, w, nj, mb>(p, s);
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
@@ -33,9 +37,13 @@ int tma_ctas_per_sm_f32(int tile_cfg) {
     int n = 0;
     switch (tile_cfg) {
 #define MRLBM_TMA_OCC(id, bx, by, st) \
-    case id: n = tma_occupancy(step_kernel_tma<fp32::Physics, bx, by, st>, bx, st * TmaGeom<float, bx, by>::STAGE_BYTES + 128); break;
+    case id: n = tma_occupancy(step_kernel_tma<fp32::Physics, bx, by, st, false>, bx, tma_smem_bytes<float, bx, by, st, false>()); break;
         MRLBM_TMA_LIST(MRLBM_TMA_OCC)
 #undef MRLBM_TMA_OCC
+#define MRLBM_TMAS_OCC(id, bx, by, st) \
+    case id: n = tma_occupancy(step_kernel_tma<fp32::Physics, bx, by, st, true>, bx, tma_smem_bytes<float, bx, by, st, true>()); break;
+        MRLBM_TMAS_LIST(MRLBM_TMAS_OCC)
+#undef MRLBM_TMAS_OCC
     default: n = 0;
     }
     return n;
@@ -46,7 +54,7 @@ int tma_ctas_per_sm(int precision, int tile_cfg) {
 }
 
 void tma_box(int precision, int tile_cfg, int* box_w, int* box_h, int* stages) {
-    const TmaCfg c = TMA_CFGS[tile_cfg - TMA_CFG0];
+    const TmaCfg c = tma_cfg(tile_cfg);
     const int m = 16 / (precision == 64 ? 8 : 4);
     *box_w = c.bx + 2 * m;
     *box_h = c.by;

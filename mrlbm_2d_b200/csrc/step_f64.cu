@@ -17,9 +17,13 @@ int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int
         MRLBM_TILE_LIST(MRLBM_TILE_CASE)
 #undef MRLBM_TILE_CASE
 #define MRLBM_TMA_CASE(id, bx, by, st) \
-    case id: return launch_step_tma<Ph, bx, by, st>(p, s, workers);
+    case id: return launch_step_tma<Ph, bx, by, st, false>(p, s, workers);
         MRLBM_TMA_LIST(MRLBM_TMA_CASE)
 #undef MRLBM_TMA_CASE
+#define MRLBM_TMAS_CASE(id, bx, by, st) \
+    case id: return launch_step_tma<Ph, bx, by, st, true>(p, s, workers);
+        MRLBM_TMAS_LIST(MRLBM_TMAS_CASE)
+#undef MRLBM_TMAS_CASE
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
     case id: return launch_step_vec<Ph, w, nj, mb>(p, s);
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
@@ -36,9 +40,13 @@ int tma_ctas_per_sm_f64(int tile_cfg) {
     int n = 0;
     switch (tile_cfg) {
 #define MRLBM_TMA_OCC(id, bx, by, st) \
-    case id: n = tma_occupancy(step_kernel_tma<fp64::Physics, bx, by, st>, bx, st * TmaGeom<double, bx, by>::STAGE_BYTES + 128); break;
+    case id: n = tma_occupancy(step_kernel_tma<fp64::Physics, bx, by, st, false>, bx, tma_smem_bytes<double, bx, by, st, false>()); break;
         MRLBM_TMA_LIST(MRLBM_TMA_OCC)
 #undef MRLBM_TMA_OCC
+#define MRLBM_TMAS_OCC(id, bx, by, st) \
+    case id: n = tma_occupancy(step_kernel_tma<fp64::Physics, bx, by, st, true>, bx, tma_smem_bytes<double, bx, by, st, true>()); break;
+        MRLBM_TMAS_LIST(MRLBM_TMAS_OCC)
+#undef MRLBM_TMAS_OCC
     default: n = 0;
     }
     return n;

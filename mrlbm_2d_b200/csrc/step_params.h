@@ -41,6 +41,7 @@ struct OvrEntry { int i, j, k, pad; double v; };
 template <class T>
 struct alignas(64) StepParams {
     CUtensorMap tmap;             // 2-D map of src (rows = 9 planes x (ny+2)), TMA shapes only
+    CUtensorMap tmap_st;          // 2-D map of dst with the store box (BX x BY), TMA-store shapes only
     unsigned long long* tile_ctr; // tile claim counter of the TMA shapes
     unsigned long long tile_base; // counter value at the start of this step
     const T* __restrict__ src;    // fout of the previous step (+ ghost ring)
@@ -117,6 +118,18 @@ constexpr int TMA_CFG0 = N_TILE_CFGS;
 constexpr TmaCfg TMA_CFGS[N_TMA_CFGS] = {MRLBM_TMA_LIST(MRLBM_TMA_ENTRY)};
 #undef MRLBM_TMA_ENTRY
 
+// TMA shapes whose fully interior tiles are also written back by tensor stores from a
+// shared-memory output tile (ids after the pipelined shapes).
+#define MRLBM_TMAS_LIST(X) \
+    X(27, 224, 4, 2)       \
+    X(28, 128, 4, 3)       \
+    X(29, 224, 2, 3)       \
+    X(30, 128, 8, 2)
+constexpr int N_TMAS_CFGS = 4;
+#define MRLBM_TMA_ENTRY(id, bx, by, st) {bx, by, st},
+constexpr TmaCfg TMAS_CFGS[N_TMAS_CFGS] = {MRLBM_TMAS_LIST(MRLBM_TMA_ENTRY)};
+#undef MRLBM_TMA_ENTRY
+
 // 128-bit vector shapes of step_kernel_vec (WARPS warps per block, each lane 16 bytes of a
 // row; NJ rows per warp; MINB resident blocks per SM).
 #define MRLBM_VEC_LIST(X) \
@@ -143,8 +156,11 @@ constexpr int VEC_CFG0 = TMA_CFG0 + N_TMA_CFGS;
     X(26, 128, 4)
 constexpr int N_PIPE_CFGS = 5;
 constexpr int PIPE_CFG0 = VEC_CFG0 + N_VEC_CFGS;
-constexpr int N_ALL_CFGS = PIPE_CFG0 + N_PIPE_CFGS;
-inline bool is_tma_cfg(int c) { return c >= TMA_CFG0 && c < VEC_CFG0; }
+constexpr int TMAS_CFG0 = PIPE_CFG0 + N_PIPE_CFGS;
+constexpr int N_ALL_CFGS = TMAS_CFG0 + N_TMAS_CFGS;
+inline bool is_tma_store_cfg(int c) { return c >= TMAS_CFG0 && c < N_ALL_CFGS; }
+inline bool is_tma_cfg(int c) { return (c >= TMA_CFG0 && c < VEC_CFG0) || is_tma_store_cfg(c); }
+inline TmaCfg tma_cfg(int c) { return is_tma_store_cfg(c) ? TMAS_CFGS[c - TMAS_CFG0] : TMA_CFGS[c - TMA_CFG0]; }
 inline bool is_vec_cfg(int c) { return c >= VEC_CFG0 && c < PIPE_CFG0; }
 
 // Host-side launch entry points (step_f64.cu / step_f32.cu).  `workers` is the persistent

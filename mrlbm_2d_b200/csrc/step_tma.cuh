@@ -61,6 +61,17 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Tensor store shared -> global (bulk group), its commit and waits.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                     (unsigned long long)map),
+                 "r"(smem_u32(src)), "r"(x), "r"(y)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 template <class T, int BX, int BY>
 struct TmaGeom {
     static constexpr int M = 16 / (int)sizeof(T);           // columns of margin each side
@@ -69,6 +80,8 @@ struct TmaGeom {
     static constexpr int PLANE_BYTES = ((BY * ROW_BYTES + 127) / 128) * 128;
     static constexpr int STAGE_BYTES = Q * PLANE_BYTES;
     static constexpr unsigned TX_BYTES = (unsigned)(Q * BY * ROW_BYTES);
+    static constexpr int OUT_PLANE = ((BY * BX * (int)sizeof(T) + 127) / 128) * 128;
+    static constexpr int OUT_BYTES = Q * OUT_PLANE;       // output tile of the TMA-store shapes
     static_assert(W <= 256 && BY <= 256, "tensor copy box limit");
     static_assert((BX * (int)sizeof(T)) % 16 == 0, "box start must stay 16-byte aligned");
 };
@@ -96,7 +109,7 @@ __device__ __forceinline__ void tma_issue(const typename Phys::P& p, char* stage
         tma_load_2d(stage + k * G::PLANE_BYTES, &p.tmap, bar, x0, k * rows + j0 - ey(k));
 }
 
-template <class Phys, int BX, int BY, int STAGES>
+template <class Phys, int BX, int BY, int STAGES, bool STORE>
 __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
     using T = typename Phys::T;
     using G = TmaGeom<T, BX, BY>;
@@ -115,6 +128,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
     if (tid == 0)
         for (int s = 0; s < STAGES; ++s) tma_issue<Phys, BX, BY>(p, tma_smem + s * G::STAGE_BYTES, &bars[s], &tile_of[s], ntiles);
     const int nx = p.L.nx, ny = p.L.ny;
+    T* out = reinterpret_cast<T*>(tma_smem + STAGES * G::STAGE_BYTES);   // STORE shapes only
     for (int q = 0;; ++q) {
         const int s = q % STAGES;
         const unsigned parity = (unsigned)(q / STAGES) & 1u;
@@ -133,36 +147,69 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
         const T* st = reinterpret_cast<const T*>(tma_smem + s * G::STAGE_BYTES);
         const int tx = t % p.tiles_x, ty = t / p.tiles_x;
         const int i = 1 + tx * BX + tid;
+        // a tile with no edge, ghost or cylinder-box node goes back through tensor stores
+        const int i0 = 1 + tx * BX, j0 = 1 + ty * BY;
+        const bool full = STORE && i0 > 1 && i0 + BX - 1 < nx && j0 > 1 && j0 + BY - 1 < ny &&
+                          (i0 + BX - 1 < p.box_x0 || i0 >= p.box_x0 + p.box_w || j0 + BY - 1 < p.box_y0 ||
+                           j0 >= p.box_y0 + p.box_h);
+        if (full) {
+            if (tid == 0) bulk_wait_read_all();               // the previous tile's stores have read `out`
+            __syncthreads();
+        }
 #pragma unroll
         for (int r = 0; r < BY; ++r) {
-            const int j = 1 + ty * BY + r;
+            const int j = j0 + r;
             if (i > nx || j > ny) continue;
+            T f[Q];
+            if (full) {
+#pragma unroll
+                for (int k = 0; k < Q; ++k)
+                    f[k] = st[(k * G::PLANE_BYTES) / (int)sizeof(T) + r * G::W + tid + G::M - ex(k)];
+                T fo[Q];
+                Phys::compute(p, i, j, CLS_FLUID, f, fo);
+#pragma unroll
+                for (int k = 0; k < Q; ++k) out[(k * G::OUT_PLANE) / (int)sizeof(T) + r * BX + tid] = fo[k];
+                continue;
+            }
             const int cls = node_class(p, i, j);
             if (cls >= 0) continue;                           // curved-wall node
             if (i == 1 || i == nx || j == 1 || j == ny) continue;   // edge blocks
-            T f[Q];
 #pragma unroll
             for (int k = 0; k < Q; ++k)
                 f[k] = st[(k * G::PLANE_BYTES) / (int)sizeof(T) + r * G::W + tid + G::M - ex(k)];
             Phys::finish(p, i, j, cls, f);
         }
-        __syncthreads();                                      // stage s fully read
+        __syncthreads();                                      // stage s fully read (and `out` written)
         if (tid == 0) {
             fence_proxy_async();
+            if (full) {
+                const int rows = p.L.ny + 2;
+#pragma unroll
+                for (int k = 0; k < Q; ++k)
+                    tma_store_2d(&p.tmap_st, reinterpret_cast<const char*>(out) + k * G::OUT_PLANE, i0 + p.L.off,
+                                 k * rows + j0);
+                bulk_commit();
+            }
             tma_issue<Phys, BX, BY>(p, tma_smem + s * G::STAGE_BYTES, &bars[s], &tile_of[s], ntiles);
         }
     }
+    if (STORE && tid == 0) bulk_wait_all();                  // stores complete before the CTA exits
     // Every stage's last phase has completed: either its copies landed or it was issued with
     // no tile.  Nothing is in flight when the loop ends.
 }
 
-template <class Phys, int BX, int BY, int STAGES>
+template <class Phys, int BX, int BY, int STAGES, bool STORE>
 __global__ void __launch_bounds__(BX, 1) step_kernel_tma(const __grid_constant__ typename Phys::P p) {
     if (run_aux_block<Phys>(p)) return;
-    tma_bulk_worker<Phys, BX, BY, STAGES>(p);
+    tma_bulk_worker<Phys, BX, BY, STAGES, STORE>(p);
 }
 
-template <class Phys, int BX, int BY, int STAGES>
+template <class T, int BX, int BY, int STAGES, bool STORE>
+constexpr int tma_smem_bytes() {
+    return STAGES * TmaGeom<T, BX, BY>::STAGE_BYTES + (STORE ? TmaGeom<T, BX, BY>::OUT_BYTES : 0) + 128;
+}
+
+template <class Phys, int BX, int BY, int STAGES, bool STORE>
 int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
     if (workers <= 0) return -2;
     using T = typename Phys::T;
@@ -172,18 +219,18 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
     p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
     p.tiles_x = (p.L.nx + BX - 1) / BX;
-    const int smem = STAGES * G::STAGE_BYTES + 128;
+    const int smem = tma_smem_bytes<T, BX, BY, STAGES, STORE>();
     if (smem > 200 * 1024) return -2;                        // shape too large for this precision
     static unsigned long long attr_set = 0;                  // one bit per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 64 || !((attr_set >> dev) & 1ull)) {
-        if (cudaFuncSetAttribute(step_kernel_tma<Phys, BX, BY, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(step_kernel_tma<Phys, BX, BY, STAGES, STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem) != cudaSuccess)
             return -1;
         if (dev < 64) attr_set |= 1ull << dev;
     }
-    step_kernel_tma<Phys, BX, BY, STAGES><<<(unsigned)(p.nbblk + p.neblk + workers), nthr, smem, s>>>(p);
+    step_kernel_tma<Phys, BX, BY, STAGES, STORE><<<(unsigned)(p.nbblk + p.neblk + workers), nthr, smem, s>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
