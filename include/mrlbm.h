@@ -297,6 +297,31 @@ int mrlbm_set_body_force(mrlbm_handle* h, const double* g);
 int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t window, int32_t checkpoint_every, double* J,
                        double* grad_body, double* grad_uin);
 
+/* ---- x-slabs of one domain (no counterpart in the reference, which runs on one node) ----
+ * mrlbm_create_slab builds the handle of global columns gx0..gx1 (1-based, at least 4) of the
+ * domain cfg describes; its lattice is that slab, with column 0 / nx+1 holding the incoming
+ * populations of the left / right neighbour when gx0 > 1 / gx1 < global nx.  Geometry and
+ * initial state are the domain's, sliced; the cylinder and its bilinear stencils must lie
+ * strictly inside one slab.  After every step the neighbours exchange one halo column per face
+ * (3 x ny values: the populations crossing the face), either through mrlbm_slabs_step
+ * (slabs of one process, on one or several devices) or through mrlbm_halo_pack /
+ * mrlbm_halo_unpack around the caller's own transport (e.g. NCCL send/recv between ranks).
+ * Force records: the slab holding the cylinder has the drag and lift, the slab holding column
+ * 1 the inlet density; the others record zeros.  Every slab's populations equal the
+ * corresponding columns of the single-domain run bit for bit. */
+int mrlbm_create_slab(const mrlbm_config* cfg, int precision, int device, int32_t gx0, int32_t gx1,
+                      mrlbm_handle** out);
+/* Values per halo face (3 x ny) and the bytes per value (the handle's storage type). */
+int mrlbm_halo_size(const mrlbm_handle* h, int64_t* n_values, int32_t* elem_bytes);
+/* side 0 = left face, 1 = right face.  pack copies the outgoing populations of the current
+ * state into device buffer dst; unpack copies a neighbour's packed face into the ghost column
+ * (both ordered on the handle's stream). */
+int mrlbm_halo_pack(mrlbm_handle* h, int32_t side, void* dst);
+int mrlbm_halo_unpack(mrlbm_handle* h, int32_t side, const void* src);
+/* Advance adjacent slabs (given left to right) nsteps steps with the halo exchange between
+ * them (device-to-device copies; peer copies across devices).  Synchronises at the end. */
+int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps);
+
 /* ---- batched cases (no counterpart in the reference, which runs one case per process) ----
  * Many independent cases of one precision on one device advance together: one kernel covers
  * the work of every case, either as a persistent cooperative launch that loops over steps

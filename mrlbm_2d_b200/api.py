@@ -38,6 +38,7 @@ EXPORTED = [
     "mrlbm_batch_last_error", "mrlbm_batch_launch_count", "mrlbm_batch_get_stream",
     "mrlbm_set_body_force", "mrlbm_adjoint_drag",
     "mrlbm_surface_enable", "mrlbm_get_probe_nodes", "mrlbm_get_surface",
+    "mrlbm_create_slab", "mrlbm_halo_size", "mrlbm_halo_pack", "mrlbm_halo_unpack", "mrlbm_slabs_step",
 ]
 BATCH_PERSISTENT, BATCH_GRAPH = 0, 1
 
@@ -113,6 +114,11 @@ def load_library(path=None):
         "mrlbm_surface_enable": [vp, i32],
         "mrlbm_get_probe_nodes": [vp, vp, vp],
         "mrlbm_get_surface": [vp, vp, vp, vp, vp, i32, vp],
+        "mrlbm_create_slab": [vp, ctypes.c_int, ctypes.c_int, i32, i32, vp],
+        "mrlbm_halo_size": [vp, vp, vp],
+        "mrlbm_halo_pack": [vp, i32, vp],
+        "mrlbm_halo_unpack": [vp, i32, vp],
+        "mrlbm_slabs_step": [vp, i32, i32],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -184,10 +190,16 @@ def config_from_namelist(path):
 class Simulation:
     """One cylinder-flow case resident on one GPU."""
 
-    def __init__(self, cfg, precision=FP64, device=0):
+    def __init__(self, cfg, precision=FP64, device=0, slab=None):
+        """slab=(gx0, gx1): only global columns gx0..gx1 of the domain (mrlbm_create_slab)."""
         self._L = load_library()
         self._h = ctypes.c_void_p()
-        rc = self._L.mrlbm_create(ctypes.byref(cfg), int(precision), int(device), ctypes.byref(self._h))
+        self.slab = slab
+        if slab is None:
+            rc = self._L.mrlbm_create(ctypes.byref(cfg), int(precision), int(device), ctypes.byref(self._h))
+        else:
+            rc = self._L.mrlbm_create_slab(ctypes.byref(cfg), int(precision), int(device), int(slab[0]),
+                                           int(slab[1]), ctypes.byref(self._h))
         if rc != 0:
             buf = ctypes.create_string_buffer(1024)
             self._L.mrlbm_last_error(None, buf, 1024)
@@ -333,6 +345,20 @@ class Simulation:
         self._check(self._L.mrlbm_get_surface(self._h, _ptr(it), _ptr(ps), _ptr(pf), _ptr(pr), cap, ctypes.byref(n)))
         m = n.value
         return it[:m].copy(), ps[:m].copy(), pf[:m].copy(), pr[:m].copy()
+
+    def halo_size(self):
+        """(values per halo face, bytes per value)."""
+        n, e = ctypes.c_int64(), ctypes.c_int32()
+        self._check(self._L.mrlbm_halo_size(self._h, ctypes.byref(n), ctypes.byref(e)))
+        return n.value, e.value
+
+    def halo_pack(self, side, dst_ptr):
+        """Copy the outgoing populations of face `side` (0 left, 1 right) to device memory dst_ptr."""
+        self._check(self._L.mrlbm_halo_pack(self._h, int(side), ctypes.c_void_p(int(dst_ptr))))
+
+    def halo_unpack(self, side, src_ptr):
+        """Copy a neighbour's packed face from device memory src_ptr into this slab's ghost column."""
+        self._check(self._L.mrlbm_halo_unpack(self._h, int(side), ctypes.c_void_p(int(src_ptr))))
 
     def set_body_force(self, g):
         """Body force g of shape (2, nx, ny) (x and y components, [c, i-1, j-1]); None removes it."""
@@ -490,3 +516,19 @@ class Batch:
         p = ctypes.c_void_p()
         self._check(self._L.mrlbm_batch_get_stream(self._b, ctypes.byref(p)))
         return p.value or 0
+
+
+def slabs_step(sims, nsteps):
+    """Advance adjacent slab simulations (left to right) with their halo exchange."""
+    if not sims:
+        return
+    L = sims[0]._L
+    arr = (ctypes.c_void_p * len(sims))(*[s._h.value for s in sims])
+    rc = L.mrlbm_slabs_step(arr, len(sims), int(nsteps))
+    if rc != 0:
+        for s in sims:
+            buf = ctypes.create_string_buffer(1024)
+            L.mrlbm_last_error(s._h, buf, 1024)
+            if buf.value:
+                raise MrlbmError(rc, buf.value.decode())
+        raise MrlbmError(rc, "mrlbm_slabs_step failed")

@@ -73,6 +73,9 @@ struct mrlbm_handle {
     double* d_fstat_out = nullptr;            // 6 x N mean and rms
     int32_t fstat_begin = 0, fstat_end = -1;
     int64_t fstat_n = 0;
+    // x-slab of a larger domain (mrlbm_create_slab): global columns gx0 .. gx0 + nx - 1 of gnx
+    bool halo_l = false, halo_r = false;
+    int gx0 = 1, gnx = 0;
     int tile_cfg = 1;
     long long launches = 0;
     std::string err;
@@ -113,7 +116,7 @@ int fail(mrlbm_handle* h, int code, const std::string& msg) {
 inline int64_t slot_of(const mrlbm_handle* h, int i, int j, int k) {
     const mrlbm_config& c = h->cfg;
     SrcSlot s = stream_source(h->L.nx, h->L.ny, i, j, k, c.x_periodic != 0, c.y_periodic != 0,
-                              c.wall_mode == MRLBM_WALL_FREESLIP);
+                              c.wall_mode == MRLBM_WALL_FREESLIP, h->halo_l, h->halo_r);
     return h->L.at(s.i, s.j, s.k);
 }
 
@@ -191,7 +194,7 @@ int upload_state(mrlbm_handle* h, const double* f) {
     const mrlbm_config& c = h->cfg;
     CK(launch_scatter_state(h->precision, h->d_fstage, h->buf[0], h->buf[1], h->L, c.x_periodic != 0,
                             c.y_periodic != 0, c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic, h->lat.w,
-                            h->stream));
+                            h->stream, h->halo_l, h->halo_r));
     ++h->launches;
     h->cur = 0;
     h->ovr = slot_conflicts(h);
@@ -253,6 +256,8 @@ void fill_common(mrlbm_handle* h, StepParams<T>& p) {
     p.label15_allnine = c.label15_rule == MRLBM_LABEL15_ALLNINE;
     p.partials = h->d_partials;
     p.counter = h->d_counter;
+    p.halo_l = h->halo_l;
+    p.halo_r = h->halo_r;
     p.node_force = nullptr;
     p.errflag = h->d_err;
     p.dc = h->dc;
@@ -454,6 +459,58 @@ void free_all(mrlbm_handle* h) {
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
 }
 
+// Geometry of the x-slab gx0..gx1 of a built domain: node classes sliced, wall-node and
+// stencil column indices shifted; the wall-point coordinates, centre and angles stay global
+// so every derived value keeps its bits.  The cylinder with its bilinear stencils must lie
+// strictly inside one slab (or the slab holds none of it).
+int slice_geometry(const Geometry& g, int gx0, int gx1, Geometry& s, std::string& err) {
+    const int nxl = gx1 - gx0 + 1, ny = g.ny, sh = gx0 - 1;
+    s = g;
+    s.nx = nxl;
+    s.cls.assign((size_t)nxl * ny, 0);
+    bool any = false;
+    for (int j = 1; j <= ny; ++j)
+        for (int i = gx0; i <= gx1; ++i) {
+            const int8_t c = g.cls[(size_t)(i - 1) + (size_t)g.nx * (j - 1)];
+            s.cls[(size_t)(i - gx0) + (size_t)nxl * (j - 1)] = c;
+            any = any || c != 0;
+        }
+    if (!g.cylinder || g.nb == 0 || !any) {
+        // no part of the cylinder here: a plain channel slab (any cylinder node outside it)
+        for (int j = 1; j <= ny && g.cylinder; ++j)
+            for (int i = gx0 - 1; i <= gx1 + 1; ++i)
+                if (i >= 1 && i <= g.nx && g.cls[(size_t)(i - 1) + (size_t)g.nx * (j - 1)] != 0) {
+                    err = "the cylinder touches the slab's halo columns";
+                    return MRLBM_EGEOMETRY;
+                }
+        s.nb = 0;
+        s.bi.clear(); s.bj.clear(); s.label.clear(); s.delta.clear(); s.ref.clear(); s.sten.clear(); s.theta.clear();
+        s.tint.clear(); s.tgeo.clear(); s.boxmap.clear();
+        s.box_x0 = 1; s.box_y0 = 1; s.box_w = 0; s.box_h = 0;
+        s.cylinder = false;
+        return MRLBM_OK;
+    }
+    // every wall node, solid node and stencil node strictly inside the slab
+    auto inside = [&](int i) { return i > gx0 && i < gx1; };
+    if (!inside(g.box_x0) || !inside(g.box_x0 + g.box_w - 1)) {
+        err = "the cylinder is cut by a slab boundary";
+        return MRLBM_EGEOMETRY;
+    }
+    for (int l = 0; l < g.nb; ++l) {
+        for (int m = 0; m < 12; ++m)
+            if (!inside(g.sten[24 * (size_t)l + 8 * (m / 4) + (m % 4)])) {
+                err = "a bilinear stencil of the cylinder crosses a slab boundary";
+                return MRLBM_EGEOMETRY;
+            }
+        s.bi[l] = g.bi[l] - sh;
+        for (int m = 0; m < 12; ++m) s.sten[24 * (size_t)l + 8 * (m / 4) + (m % 4)] -= sh;
+        s.tint[(size_t)I_NODEI * g.nb + l] -= sh;
+        for (int m = 0; m < 12; ++m) s.tint[(size_t)(I_SI + m) * g.nb + l] -= sh;
+    }
+    s.box_x0 = g.box_x0 - sh;
+    return MRLBM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -484,7 +541,7 @@ int mrlbm_config_resolve_geometry(mrlbm_config* cfg) {
     return MRLBM_OK;
 }
 
-int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handle** out) {
+static int create_impl(const mrlbm_config* cfg, int precision, int device, int sx0, int sx1, mrlbm_handle** out) {
     if (!cfg || !out) return MRLBM_EINVAL;
     *out = nullptr;
     if (precision != MRLBM_FP64 && precision != MRLBM_FP32) {
@@ -516,6 +573,19 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
     std::string err;
     int grc = build_geometry(c, nx, ny, xc, yc, rc, h->geo, err);
     if (grc != MRLBM_OK) return bail(grc, err);
+    h->gnx = nx;
+    const int gnx = nx;
+    if (sx0 > 0) {                                   // one x-slab of the domain
+        if (c.x_periodic) return bail(MRLBM_EUNSUPPORTED, "x-slabs of an x-periodic domain");
+        if (sx0 < 1 || sx1 > nx || sx1 - sx0 + 1 < 4) return bail(MRLBM_EINVAL, "slab columns out of range");
+        Geometry full = h->geo;
+        grc = slice_geometry(full, sx0, sx1, h->geo, err);
+        if (grc != MRLBM_OK) return bail(grc, err);
+        h->gx0 = sx0;
+        h->halo_l = sx0 > 1;
+        h->halo_r = sx1 < nx;
+        nx = sx1 - sx0 + 1;
+    }
     h->lat = make_lattice();
     // viscosity and relaxation, 2d_mrlbm.f90:133-135
     h->nu = c.uo * (double)(ny - 1) / c.Re;
@@ -587,7 +657,15 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
     ok = ok && ck(cudaMemset(h->d_counter, 0, sizeof(unsigned)), "memset") && ck(cudaMemset(h->d_err, 0, sizeof(int)), "memset");
     if (!ok) { std::string m = g_create_error; return bail(MRLBM_ECUDA, m); }
     std::vector<double> f0;
-    initial_state(h->cfg, h->lat, nx, ny, f0);
+    initial_state(h->cfg, h->lat, gnx, ny, f0);
+    if (nx != gnx) {                                 // the slab's columns of the domain's start
+        std::vector<double> fs((size_t)nx * ny * Q);
+        for (int k = 0; k < Q; ++k)
+            for (int j = 1; j <= ny; ++j)
+                std::memcpy(&fs[(size_t)nx * ny * k + (size_t)nx * (j - 1)],
+                            &f0[(size_t)gnx * ny * k + (size_t)gnx * (j - 1) + (h->gx0 - 1)], nx * sizeof(double));
+        f0.swap(fs);
+    }
     int urc = upload_state(h, f0.data());
     if (urc != MRLBM_OK) { std::string m = h->err; return bail(urc, m); }
     // the main loop runs iter = restart_step+1, ... with restart_step initialised to 1
@@ -595,6 +673,115 @@ int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handl
     h->iter = 1;
     *out = h;
     return MRLBM_OK;
+}
+
+int mrlbm_create(const mrlbm_config* cfg, int precision, int device, mrlbm_handle** out) {
+    return create_impl(cfg, precision, device, 0, 0, out);
+}
+
+int mrlbm_create_slab(const mrlbm_config* cfg, int precision, int device, int32_t gx0, int32_t gx1,
+                      mrlbm_handle** out) {
+    if (gx0 < 1) return MRLBM_EINVAL;
+    return create_impl(cfg, precision, device, gx0, gx1, out);
+}
+
+// Halo columns: side 0 is the left face (the populations moving left, k = 3, 6, 7, of column 1
+// go out; the left neighbour's k = 1, 5, 8 come into column 0), side 1 the right face (k = 1,
+// 5, 8 of column nx out; k = 3, 6, 7 into column nx + 1).  3 x ny values of the handle's
+// storage type per face, k-major, rows 1..ny.
+static const int HALO_OUT[2][3] = {{3, 6, 7}, {1, 5, 8}};
+static const int HALO_IN[2][3] = {{1, 5, 8}, {3, 6, 7}};
+
+int mrlbm_halo_size(const mrlbm_handle* h, int64_t* n_values, int32_t* elem_bytes) {
+    if (!h || !n_values) return MRLBM_EINVAL;
+    *n_values = 3 * (int64_t)h->L.ny;
+    if (elem_bytes) *elem_bytes = h->elem;
+    return MRLBM_OK;
+}
+
+static int halo_copy(mrlbm_handle* h, int side, void* dev, bool pack, void* peer_dst, const mrlbm_handle* peer) {
+    if (!h || side < 0 || side > 1) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    CK(cudaSetDevice(h->device));
+    const int ny = h->L.ny;
+    const size_t e = h->elem, pitch_b = (size_t)h->L.pitch * e;
+    char* base = (char*)h->buf[h->cur];
+    for (int q = 0; q < 3; ++q) {
+        if (pack) {
+            const int i = side == 0 ? 1 : h->L.nx, k = HALO_OUT[side][q];
+            const char* src = base + (size_t)h->L.at(i, 1, k) * e;
+            if (peer) {                              // straight into the neighbour's ghost column
+                const int pi = side == 0 ? peer->L.nx + 1 : 0;
+                char* dst = (char*)peer_dst + (size_t)peer->L.at(pi, 1, k) * e;
+                CK(cudaMemcpy2DAsync(dst, (size_t)peer->L.pitch * e, src, pitch_b, e, ny, cudaMemcpyDefault, h->stream));
+            } else {
+                CK(cudaMemcpy2DAsync((char*)dev + (size_t)q * ny * e, e, src, pitch_b, e, ny, cudaMemcpyDefault, h->stream));
+            }
+        } else {
+            const int i = side == 0 ? 0 : h->L.nx + 1, k = HALO_IN[side][q];
+            char* dst = base + (size_t)h->L.at(i, 1, k) * e;
+            CK(cudaMemcpy2DAsync(dst, pitch_b, (const char*)dev + (size_t)q * ny * e, e, e, ny, cudaMemcpyDefault, h->stream));
+        }
+    }
+    return MRLBM_OK;
+}
+
+int mrlbm_halo_pack(mrlbm_handle* h, int32_t side, void* dst) {
+    if (!dst) return MRLBM_EINVAL;
+    return halo_copy(h, side, dst, true, nullptr, nullptr);
+}
+
+int mrlbm_halo_unpack(mrlbm_handle* h, int32_t side, const void* src) {
+    if (!src) return MRLBM_EINVAL;
+    return halo_copy(h, side, const_cast<void*>(src), false, nullptr, nullptr);
+}
+
+int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps) {
+    if (!hs || n < 1 || nsteps < 0) return MRLBM_EINVAL;
+    for (int s = 0; s < n; ++s) {
+        if (!hs[s] || hs[s]->host_only || hs[s]->precision != hs[0]->precision || hs[s]->L.ny != hs[0]->L.ny)
+            return MRLBM_EINVAL;
+        if (s > 0 && (!hs[s]->halo_l || !hs[s - 1]->halo_r || hs[s]->gx0 != hs[s - 1]->gx0 + hs[s - 1]->L.nx))
+            return fail(hs[s], MRLBM_EINVAL, "slabs must be given left to right, adjacent");
+    }
+    std::vector<cudaEvent_t> done(n), halo(n);
+    for (int s = 0; s < n; ++s) {
+        if (cudaSetDevice(hs[s]->device) != cudaSuccess) return fail(hs[s], MRLBM_ECUDA, "cudaSetDevice");
+        cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&halo[s], cudaEventDisableTiming);
+    }
+    int rc = MRLBM_OK;
+    for (int t = 0; t < nsteps && rc == MRLBM_OK; ++t) {
+        for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
+            cudaSetDevice(hs[s]->device);
+            if (t > 0 && s > 0) cudaStreamWaitEvent(hs[s]->stream, halo[s - 1], 0);     // right-going halo
+            if (t > 0 && s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, halo[s + 1], 0); // left-going halo
+            rc = mrlbm_step(hs[s], 1, 0);
+            cudaEventRecord(done[s], hs[s]->stream);
+        }
+        // each slab sends its faces once both it and the receiver have stepped
+        for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
+            cudaSetDevice(hs[s]->device);
+            if (s > 0) cudaStreamWaitEvent(hs[s]->stream, done[s - 1], 0);
+            if (s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, done[s + 1], 0);
+            if (s > 0) rc = halo_copy(hs[s], 0, nullptr, true, hs[s - 1]->buf[hs[s - 1]->cur], hs[s - 1]);
+            if (rc == MRLBM_OK && s + 1 < n) rc = halo_copy(hs[s], 1, nullptr, true, hs[s + 1]->buf[hs[s + 1]->cur], hs[s + 1]);
+            cudaEventRecord(halo[s], hs[s]->stream);
+        }
+    }
+    for (int s = 0; s < n; ++s) {
+        cudaSetDevice(hs[s]->device);
+        cudaStreamWaitEvent(hs[s]->stream, halo[s], 0);
+        if (s > 0) cudaStreamWaitEvent(hs[s]->stream, halo[s - 1], 0);
+        if (s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, halo[s + 1], 0);
+    }
+    for (int s = 0; s < n; ++s) {
+        cudaSetDevice(hs[s]->device);
+        cudaStreamSynchronize(hs[s]->stream);
+        cudaEventDestroy(done[s]);
+        cudaEventDestroy(halo[s]);
+    }
+    return rc;
 }
 
 int mrlbm_destroy(mrlbm_handle* h) {
@@ -693,7 +880,7 @@ int mrlbm_get_state(mrlbm_handle* h, double* f) {
     if (!h->d_fstage) CK(cudaMalloc((void**)&h->d_fstage, N * Q * sizeof(double)));
     const mrlbm_config& c = h->cfg;
     CK(launch_gather_state(h->precision, h->buf[h->cur], h->d_fstage, h->L, c.x_periodic != 0, c.y_periodic != 0,
-                           c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic, h->lat.w, h->stream));
+                           c.wall_mode == MRLBM_WALL_FREESLIP && !c.y_periodic, h->lat.w, h->stream, h->halo_l, h->halo_r));
     ++h->launches;
     CK(cudaMemcpyAsync(f, h->d_fstage, N * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -1315,7 +1502,7 @@ void batch_items(const mrlbm_handle* h, int cfg, int& aux, int& tiles, int& nbbl
     const int nthr = v.warps * 32, vw = 16 / h->elem;
     const int bn = nthr / 8;
     nbblk = h->geo.nb > 0 ? (h->geo.nb + bn - 1) / bn : 1;
-    neblk = (2 * h->L.nx + 2 * (h->L.ny - 2) + nthr - 1) / nthr;
+    neblk = (2 * h->L.nx + (h->halo_l ? 0 : h->L.ny - 2) + (h->halo_r ? 0 : h->L.ny - 2) + nthr - 1) / nthr;
     tiles_x = (h->L.nx + 32 * vw - 1) / (32 * vw);
     const int tiles_y = (h->L.ny + v.warps * v.nj - 1) / (v.warps * v.nj);
     aux = nbblk + neblk;

@@ -58,12 +58,15 @@ inline Layout make_layout(int nx, int ny, int align_elems) {
 // specularly to the same row (source column wrapped when xper), applied after the wraps.
 struct SrcSlot { int i, j, k; };
 
-MRLBM_HD SrcSlot stream_source(int nx, int ny, int i, int j, int k, bool xper, bool yper, bool freeslip) {
+// For an x-slab of a larger domain (hl / hr: the left / right neighbour's populations sit in
+// column 0 / nx+1), a reflection whose source column is that halo column reads it there.
+MRLBM_HD SrcSlot stream_source(int nx, int ny, int i, int j, int k, bool xper, bool yper, bool freeslip,
+                               bool hl = false, bool hr = false) {
     const int dx = ex(k), dy = ey(k);
     SrcSlot s{i - dx, j - dy, k};
     if (freeslip && !yper && ((j == ny && dy == -1) || (j == 1 && dy == 1))) {
         int ti = i - dx;
-        if (ti >= 1 && ti <= nx) { s.i = ti; s.j = j; s.k = mirror_y(k); }
+        if ((ti >= 1 || hl) && (ti <= nx || hr)) { s.i = ti; s.j = j; s.k = mirror_y(k); }
         else if (xper) { s.i = ti < 1 ? nx : 1; s.j = j; s.k = mirror_y(k); }
         return s;
     }

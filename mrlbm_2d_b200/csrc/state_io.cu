@@ -11,14 +11,14 @@ __device__ __forceinline__ double weight(int k, double w0, double w1, double w5)
 
 template <class T>
 __global__ void scatter_state(const double* __restrict__ f0, T* a, T* b, Layout L, int xper, int yper, int freeslip,
-                              double w0, double w1, double w5, int deviation) {
+                              double w0, double w1, double w5, int deviation, int hl, int hr) {
     const int64_t N = (int64_t)L.nx * L.ny;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= N * Q) return;
     const int k = (int)(t / N);
     const int64_t n = t - (int64_t)k * N;
     const int i = (int)(n % L.nx) + 1, j = (int)(n / L.nx) + 1;
-    const SrcSlot s = stream_source(L.nx, L.ny, i, j, k, xper != 0, yper != 0, freeslip != 0);
+    const SrcSlot s = stream_source(L.nx, L.ny, i, j, k, xper != 0, yper != 0, freeslip != 0, hl != 0, hr != 0);
     const int64_t slot = L.at(s.i, s.j, s.k);
     const T v = deviation ? (T)(f0[t] - weight(k, w0, w1, w5)) : (T)f0[t];
     a[slot] = v;
@@ -27,14 +27,14 @@ __global__ void scatter_state(const double* __restrict__ f0, T* a, T* b, Layout 
 
 template <class T>
 __global__ void gather_state(const T* __restrict__ src, double* f, Layout L, int xper, int yper, int freeslip,
-                             double w0, double w1, double w5, int deviation) {
+                             double w0, double w1, double w5, int deviation, int hl, int hr) {
     const int64_t N = (int64_t)L.nx * L.ny;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= N * Q) return;
     const int k = (int)(t / N);
     const int64_t n = t - (int64_t)k * N;
     const int i = (int)(n % L.nx) + 1, j = (int)(n / L.nx) + 1;
-    const SrcSlot s = stream_source(L.nx, L.ny, i, j, k, xper != 0, yper != 0, freeslip != 0);
+    const SrcSlot s = stream_source(L.nx, L.ny, i, j, k, xper != 0, yper != 0, freeslip != 0, hl != 0, hr != 0);
     const double v = (double)src[L.at(s.i, s.j, s.k)];
     f[t] = deviation ? weight(k, w0, w1, w5) + v : v;
 }
@@ -54,24 +54,24 @@ unsigned blocks_for(const Layout& L) { return (unsigned)(((int64_t)L.nx * L.ny *
 }  // namespace
 
 cudaError_t launch_scatter_state(int precision, const double* f0, void* a, void* b, const Layout& L, int xper,
-                                 int yper, int freeslip, const double* w, cudaStream_t s) {
+                                 int yper, int freeslip, const double* w, cudaStream_t s, int hl, int hr) {
     if (precision == 64)
         scatter_state<double><<<blocks_for(L), 256, 0, s>>>(f0, (double*)a, (double*)b, L, xper, yper, freeslip, w[0],
-                                                            w[1], w[5], 0);
+                                                            w[1], w[5], 0, hl, hr);
     else
         scatter_state<float><<<blocks_for(L), 256, 0, s>>>(f0, (float*)a, (float*)b, L, xper, yper, freeslip, w[0], w[1],
-                                                           w[5], 1);
+                                                           w[5], 1, hl, hr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gather_state(int precision, const void* src, double* f, const Layout& L, int xper, int yper,
-                                int freeslip, const double* w, cudaStream_t s) {
+                                int freeslip, const double* w, cudaStream_t s, int hl, int hr) {
     if (precision == 64)
         gather_state<double><<<blocks_for(L), 256, 0, s>>>((const double*)src, f, L, xper, yper, freeslip, w[0], w[1],
-                                                           w[5], 0);
+                                                           w[5], 0, hl, hr);
     else
         gather_state<float><<<blocks_for(L), 256, 0, s>>>((const float*)src, f, L, xper, yper, freeslip, w[0], w[1],
-                                                          w[5], 1);
+                                                          w[5], 1, hl, hr);
     return cudaGetLastError();
 }
 

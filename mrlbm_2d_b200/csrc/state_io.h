@@ -5,15 +5,16 @@
 
 namespace mrlbm {
 
+// hl / hr: the lattice is an x-slab whose column 0 / nx+1 holds a neighbour's populations.
 // f0 (Fortran order, FP64, device) -> both padded time levels a and b (FP64 values, or FP32
 // deviations f - w_k when precision == 32).  Population (i,j,k) goes to the slot its
 // next-step gather reads (stream_source).
 cudaError_t launch_scatter_state(int precision, const double* f0, void* a, void* b, const Layout& L, int xper,
-                                 int yper, int freeslip, const double* w, cudaStream_t s);
+                                 int yper, int freeslip, const double* w, cudaStream_t s, int hl = 0, int hr = 0);
 // padded time level src -> f (Fortran order, FP64, device): the populations the next
 // step's gather reads, i.e. the reference's post-streaming f.
 cudaError_t launch_gather_state(int precision, const void* src, double* f, const Layout& L, int xper, int yper,
-                                int freeslip, const double* w, cudaStream_t s);
+                                int freeslip, const double* w, cudaStream_t s, int hl = 0, int hr = 0);
 // override entries (destinations sharing a streaming slot) take their values from f0.
 cudaError_t launch_fill_overrides(int precision, const double* f0, OvrEntry* ovr, int n, int nx, int ny,
                                   const double* w, cudaStream_t s);

@@ -13,20 +13,31 @@
 
 namespace mrlbm {
 
+// Columns 1 and nx are domain edges unless the lattice is one x-slab of a larger domain and
+// the neighbouring slab supplies that side's incoming populations in column 0 / nx+1.
+template <class T>
+__device__ __forceinline__ bool col_interior(const StepParams<T>& p, int i) {
+    return (i > 1 || p.halo_l) && (i < p.L.nx || p.halo_r);
+}
+template <class T>
+__device__ __forceinline__ bool is_interior(const StepParams<T>& p, int i, int j) {
+    return col_interior(p, i) && j > 1 && j < p.L.ny;
+}
+
 // f(i,j,:) of this step = fout of the previous step at the streaming sources
 // (stream_source in lattice.h).  Interior nodes take the branch-free fast path.
 template <class T>
 __device__ __forceinline__ void gather(const StepParams<T>& p, int i, int j, T f[Q]) {
     const int nx = p.L.nx, ny = p.L.ny;
     const int pitch = p.L.pitch, plane = (int)p.L.plane;
-    if (i > 1 && i < nx && j > 1 && j < ny) {
+    if (is_interior(p, i, j)) {
         const T* s = p.src + ((int)(j * pitch + i + p.L.off));
 #pragma unroll
         for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
     } else {
 #pragma unroll
         for (int k = 0; k < Q; ++k) {
-            SrcSlot sl = stream_source(nx, ny, i, j, k, p.xper, p.yper, p.freeslip);
+            SrcSlot sl = stream_source(nx, ny, i, j, k, p.xper, p.yper, p.freeslip, p.halo_l, p.halo_r);
             f[k] = __ldg(p.src + p.L.at(sl.i, sl.j, sl.k));
         }
         for (int q = 0; q < p.n_ovr; ++q)
@@ -160,7 +171,7 @@ __device__ __forceinline__ void aux_tail(const typename Phys::P& p, unsigned cha
     // its lane 0 adds them in index order, so only the adds are serial.
     const int lane = tid & 31;
     for (int w = tid >> 5; w < 3; w += (int)(blockDim.x >> 5)) {   // 64-thread blocks: a warp does two
-        const int n = w < 2 ? p.nb : p.L.ny;
+        const int n = w < 2 ? p.nb : (p.halo_l ? 0 : p.L.ny);      // an x-slab without column 1 adds 0
         const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
         double* st = reinterpret_cast<double*>(smem) + w * AUX_CHUNK;
         double acc = 0.0;
@@ -255,14 +266,15 @@ template <class Phys>
 __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, unsigned char* smem) {
     const int nx = p.L.nx, ny = p.L.ny;
     const int e = eb * (int)blockDim.x + (int)threadIdx.x;
-    if (e < 2 * nx + 2 * (ny - 2)) {
+    const int nl = p.halo_l ? 0 : ny - 2, nr = p.halo_r ? 0 : ny - 2;   // edge columns of this lattice
+    if (e < 2 * nx + nl + nr) {
         int i, j;
         if (e < nx) { i = e + 1; j = 1; }
         else if (e < 2 * nx) { i = e - nx + 1; j = ny; }
-        else if (e < 2 * nx + ny - 2) { i = 1; j = e - 2 * nx + 2; }
-        else { i = nx; j = e - 2 * nx - (ny - 2) + 2; }
+        else if (e < 2 * nx + nl) { i = 1; j = e - 2 * nx + 2; }
+        else { i = nx; j = e - 2 * nx - nl + 2; }
         const double rho = Phys::edge_bulk_node(p, i, j, CLS_FLUID);
-        if (p.do_stats && i == 1) p.partials[2 * p.nb + j - 1] = rho;
+        if (p.do_stats && i == 1 && !p.halo_l) p.partials[2 * p.nb + j - 1] = rho;
     }
     aux_tail<Phys>(p, smem);
 }
@@ -294,7 +306,11 @@ __device__ __forceinline__ bool run_aux_block(const typename Phys::P& p) {
     return true;
 }
 
-inline int edge_blocks(int nx, int ny, int nthr) { return (2 * nx + 2 * (ny - 2) + nthr - 1) / nthr; }
+template <class P>
+inline int edge_blocks(const P& p, int nthr) {
+    const int n = 2 * p.L.nx + (p.halo_l ? 0 : p.L.ny - 2) + (p.halo_r ? 0 : p.L.ny - 2);
+    return (n + nthr - 1) / nthr;
+}
 
 // Interior populations (no wraps, no ghosts): the branch-free half of `gather`.
 template <class T>
@@ -328,7 +344,7 @@ __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_consta
         cls[r] = CLS_FLUID;
         if (j <= ny) {
             cls[r] = node_class(p, i, j);
-            if (cls[r] < 0 && i > 1 && i < nx && j > 1 && j < ny) {
+            if (cls[r] < 0 && is_interior(p, i, j)) {
                 gather_interior(p, i, j, f[r]);
                 interior |= 1u << r;
             }
@@ -345,8 +361,8 @@ __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_consta
 // Each lane owns VW consecutive nodes of a row (VW = 16 bytes / element: four FP32 or two FP64
 // nodes) and reads every direction plane with one aligned 16-byte load per plane.  A pull
 // source one column left (planes with e_kx = +1) or right (e_kx = -1) of the lane's group comes
-// from the neighbouring lane by a warp shuffle; the warp's two outermost lanes fetch that
-// column with one scalar load.  A group whose nodes are all interior bulk nodes is written
+// from the neighbouring lane by a warp shuffle; the warp's two outermost lanes (and, in an
+// x-slab, the lane ending at column nx) fetch that column with one scalar load.  A group whose nodes are all interior bulk nodes is written
 // back with one 16-byte store per plane; groups touching an edge or the cylinder box fall back
 // to per-node handling (edge nodes belong to the edge blocks, wall nodes to the boundary
 // blocks).  Columns read: i0-1 .. i0+VW of rows j-1 .. j+1, which the layout's row slack
@@ -406,13 +422,17 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
                 if (lane == 0 && act) side[k] = __ldg(a - 1);
             } else if (ex(k) < 0) {
                 side[k] = __shfl_down_sync(0xffffffffu, v[k][0], 1);
-                if (lane == 31 && i0 + VW <= nx) side[k] = __ldg(a + VW);
+                // the warp's last lane, and the lane whose group ends at node nx of an x-slab
+                // (its right neighbour's column nx+1 is the halo, which no lane loads)
+                if ((lane == 31 && i0 + VW <= nx) || (p.halo_r && act && i0 + VW - 1 == nx))
+                    side[k] = __ldg(a + VW);
             }
         }
         if (!act) continue;
         const bool row_int = j > 1 && j < ny;
         const bool in_box_row = box_cols && (unsigned)(j - p.box_y0) < (unsigned)p.box_h;
-        const bool all_int = row_int && i0 > 1 && i0 + VW - 1 < nx && !in_box_row;
+        const bool all_int = row_int && col_interior(p, i0) && i0 + VW - 1 <= nx && col_interior(p, i0 + VW - 1) &&
+                             !in_box_row;
         T out[Q][VW];
 #pragma unroll
         for (int n = 0; n < VW; ++n) {
@@ -429,7 +449,7 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
                 Phys::compute(p, i, j, CLS_FLUID, f, fo);
 #pragma unroll
                 for (int k = 0; k < Q; ++k) out[k][n] = fo[k];
-            } else if (row_int && i > 1 && i < nx) {          // edge nodes: edge blocks
+            } else if (row_int && i <= nx && col_interior(p, i)) {   // edge nodes: edge blocks
                 const int cls = in_box_row ? node_class(p, i, j) : CLS_FLUID;
                 if (cls < 0) Phys::finish(p, i, j, cls, f);   // cls >= 0: curved-wall node
             }
@@ -456,7 +476,7 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
     static_assert(WARPS * 32 % BLANES == 0 && WARPS * 32 / BLANES <= BNODES, "boundary block size");
     const int bn = nthr / BLANES;
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
+    p.neblk = edge_blocks(p, nthr);
     p.tiles_x = (p.L.nx + 32 * VW - 1) / (32 * VW);
     const int tiles_y = (p.L.ny + WARPS * NJ - 1) / (WARPS * NJ);
     const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
@@ -481,7 +501,7 @@ __global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constan
         if (u >= units) return false;
         j = 1 + u / tiles_x;
         i = 1 + (u - (j - 1) * tiles_x) * B + (int)threadIdx.x;
-        if (!(i > 1 && i < nx && j > 1 && j < ny)) return false;
+        if (!(i <= nx && is_interior(p, i, j))) return false;
         gather_interior(p, i, j, f);
         return true;
     };
@@ -520,7 +540,7 @@ int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
     }
     const int bn = B / BLANES;
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p.L.nx, p.L.ny, B);
+    p.neblk = edge_blocks(p, B);
     p.tiles_x = (p.L.nx + B - 1) / B;
     const long long units = (long long)p.tiles_x * p.L.ny;
     const long long G = std::min<long long>(units, (long long)sms[dev] * per_sm[dev]);
@@ -534,7 +554,7 @@ int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     static_assert(BX * BY % BLANES == 0 && BX * BY / BLANES <= BNODES, "boundary block size");
     const int bn = nthr / BLANES;
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
+    p.neblk = edge_blocks(p, nthr);
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
     const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;

@@ -72,8 +72,8 @@ constexpr int M_BOTTOM = (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | 
 // apply_bc_incomp (2d_mrlbm.f90:249-272, 1237-1494) in deviation form.
 __device__ __noinline__ void edge_node(const P& p, int i, int j, const float g[Q], Mac& m) {
     const int nx = p.L.nx, ny = p.L.ny;
-    const bool outlet = !p.xper && i == nx;
-    const bool inlet = !p.xper && i == 1;
+    const bool outlet = !p.xper && !p.halo_r && i == nx;
+    const bool inlet = !p.xper && !p.halo_l && i == 1;
     const bool top = p.walls_ref && j == ny;
     const bool bottom = p.walls_ref && j == 1;
     const DevConsts& c = p.dc;

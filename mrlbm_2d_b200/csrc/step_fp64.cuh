@@ -111,8 +111,8 @@ constexpr int M_BOTTOM = (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | 
 // reference applies last at this node (apply_bc / apply_bc_incomp, 2d_mrlbm.f90:313-351).
 __device__ __noinline__ void edge_node(const P& p, int i, int j, const double f[Q], Mac& m) {
     const int nx = p.L.nx, ny = p.L.ny;
-    const bool outlet = !p.xper && i == nx;
-    const bool inlet = !p.xper && i == 1;
+    const bool outlet = !p.xper && !p.halo_r && i == nx;
+    const bool inlet = !p.xper && !p.halo_l && i == 1;
     const bool top = p.walls_ref && j == ny;
     const bool bottom = p.walls_ref && j == 1;
     if (outlet) {
@@ -203,7 +203,7 @@ __device__ __forceinline__ void collide(const P& p, const Mac& m, double fo[Q]) 
 // Post-boundary-condition macroscopic values of a non-cylinder node.
 __device__ __forceinline__ Mac node_macro(const P& p, int i, int j, const double f[Q]) {
     Mac m = moments(f, p.hm, p.hp);
-    if (i == 1 || i == p.L.nx || j == 1 || j == p.L.ny) edge_node(p, i, j, f, m);
+    if (!is_interior(p, i, j)) edge_node(p, i, j, f, m);
     return m;
 }
 

@@ -61,6 +61,7 @@ struct alignas(64) StepParams {
     // curved wall
     int nb, nbblk;                // boundary nodes, boundary blocks at the start of the grid
     int neblk;                    // edge blocks (one thread per domain-edge node) after them
+    int halo_l, halo_r;           // x-slab of a larger domain: column 0 / nx+1 hold the neighbour's populations
     const int* __restrict__ bint; // IntField table [I_NFIELDS * nb]
     const T* __restrict__ bgeo;   // GeoField table [G_NFIELDS * nb]
     int closure, vel_interp, mom_interp;

@@ -149,7 +149,8 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
         const int i = 1 + tx * BX + tid;
         // a tile with no edge, ghost or cylinder-box node goes back through tensor stores
         const int i0 = 1 + tx * BX, j0 = 1 + ty * BY;
-        const bool full = STORE && i0 > 1 && i0 + BX - 1 < nx && j0 > 1 && j0 + BY - 1 < ny &&
+        const bool full = STORE && col_interior(p, i0) && i0 + BX - 1 <= nx && col_interior(p, i0 + BX - 1) &&
+                          j0 > 1 && j0 + BY - 1 < ny &&
                           (i0 + BX - 1 < p.box_x0 || i0 >= p.box_x0 + p.box_w || j0 + BY - 1 < p.box_y0 ||
                            j0 >= p.box_y0 + p.box_h);
         if (full) {
@@ -173,7 +174,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
             }
             const int cls = node_class(p, i, j);
             if (cls >= 0) continue;                           // curved-wall node
-            if (i == 1 || i == nx || j == 1 || j == ny) continue;   // edge blocks
+            if (!is_interior(p, i, j)) continue;            // edge blocks
 #pragma unroll
             for (int k = 0; k < Q; ++k)
                 f[k] = st[(k * G::PLANE_BYTES) / (int)sizeof(T) + r * G::W + tid + G::M - ex(k)];
@@ -217,7 +218,7 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
     const int nthr = BX;
     const int bn = nthr / BLANES;
     p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p.L.nx, p.L.ny, nthr);
+    p.neblk = edge_blocks(p, nthr);
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int smem = tma_smem_bytes<T, BX, BY, STAGES, STORE>();
     if (smem > 200 * 1024) return -2;                        // shape too large for this precision

@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) surface_a(const __grid_constant__ StepPar
         double f[Q];
         gather_f(p, i, j, f);
         double rho, ux, uy;
-        if (sizeof(T) == 8 && (i == 1 || i == p.L.nx || j == 1 || j == p.L.ny)) {
+        if (sizeof(T) == 8 && !is_interior(p, i, j)) {
             const fp64::Mac m = fp64::node_macro(reinterpret_cast<const StepParams<double>&>(p), i, j, f);
             rho = m.rho; ux = m.ux; uy = m.uy;
         } else {

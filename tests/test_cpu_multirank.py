@@ -72,3 +72,43 @@ def test_reference_arm_prints_on_rank_zero_only(tmp_path):
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
     assert outs[1].strip() == ""
+
+
+SLAB_WORKER = r"""
+import json, os, sys
+sys.path.insert(0, {root!r})
+import torch, torch.distributed as dist
+from mrlbm_2d_b200.slabs import SlabExchange
+dist.init_process_group("gloo")
+r, w = dist.get_rank(), dist.get_world_size()
+got = {{}}
+def pack(side, t):
+    t.fill_(100.0 * r + side)                  # this rank's face `side`
+def unpack(side, t):
+    got[side] = float(t[0])
+ex = SlabExchange(r, w, pack, unpack, 12, torch.float64, torch.device("cpu"))
+ex.exchange()
+print(json.dumps({{"rank": r, "got": got}}), flush=True)
+dist.destroy_process_group()
+"""
+
+
+def test_slab_halo_exchange_between_three_gloo_ranks():
+    """Each slab receives its left neighbour's right face into side 0 and its right neighbour's
+    left face into side 1; the end slabs have one neighbour."""
+    import json
+    outs = _launch(SLAB_WORKER.format(root=ROOT), world=3)
+    rows = {json.loads(o.strip().splitlines()[-1])["rank"]: json.loads(o.strip().splitlines()[-1])["got"] for o in outs}
+    assert rows[0] == {"1": 100.0}
+    assert rows[1] == {"0": 1.0, "1": 200.0}
+    assert rows[2] == {"0": 101.0}
+
+
+def test_partition_keeps_the_cylinder_whole():
+    from mrlbm_2d_b200.slabs import partition
+    assert partition(400, 3, (65, 95)) == [(1, 133), (134, 266), (267, 400)]
+    parts = partition(400, 4, (90, 110))
+    assert any(a < 90 and 110 < b for (a, b) in parts)          # strictly inside one slab
+    for (a, b), (c, d) in zip(parts, parts[1:]):
+        assert b + 1 == c
+    assert parts[0][0] == 1 and parts[-1][1] == 400

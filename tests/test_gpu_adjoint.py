@@ -124,7 +124,7 @@ def test_torch_autograd_bridge(mrlbm):
     J = mean_drag(s, b, u, 100, 40, 25)
     (2.0 * J).backward()
     J0, gb, gu = s.adjoint_drag(100, 40, 25)
-    assert float(J) == J0
+    assert float(J.detach()) == J0
     assert np.allclose(b.grad.numpy(), 2.0 * gb, rtol=1e-10, atol=1e-14 * np.abs(gb).max())
     assert np.allclose(u.grad.numpy(), 2.0 * gu, rtol=1e-10, atol=1e-14 * np.abs(gu).max())
     s.close()

@@ -1,0 +1,81 @@
+"""x-slabs of one domain: stepped together with their halo exchange, each slab's populations
+equal the matching columns of the single-domain run bit for bit, and the force records too."""
+import numpy as np
+import pytest
+
+from cases import CASES
+from mrlbm_2d_b200.slabs import cylinder_columns, partition
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(mrlbm, cfg, prec, steps):
+    s = mrlbm.Simulation(cfg, precision=prec)
+    s.step(steps)
+    out = (s.get_state(), s.forces())
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("parts,tiles", [(2, (1, 1)), (3, (18, 27, 22)), (4, (3, 16, 10, 0))])
+def test_slabs_match_single_domain(mrlbm, prec, parts, tiles):
+    cfg = CASES["benchmark_small_400x100"]()
+    bounds = partition(400, parts, cylinder_columns(cfg))
+    sims = [mrlbm.Simulation(cfg, precision=prec, slab=b) for b in bounds]
+    for s, t in zip(sims, tiles):
+        try:
+            s.tile_config = t
+        except mrlbm.MrlbmError:
+            pass
+    mrlbm.slabs_step(sims, 17)
+    mrlbm.slabs_step(sims, 23)
+    f_ref, (it, fd, fl, rin) = _single(mrlbm, cfg, prec, 40)
+    f = np.concatenate([s.get_state() for s in sims], axis=0)
+    assert f.shape == f_ref.shape
+    assert np.array_equal(f, f_ref)
+    recs = [s.forces() for s in sims]
+    for r in recs:
+        assert np.array_equal(r[0], it)
+    assert np.array_equal(sum(r[1] for r in recs), fd) and np.array_equal(sum(r[2] for r in recs), fl)
+    assert np.array_equal(sum(r[3] for r in recs), rin)
+    for s in sims:
+        assert s.status() == 0
+        s.close()
+
+
+def test_halo_pack_unpack_exchange_in_torch_buffers(mrlbm):
+    """The rank-to-rank path without the transport: pack each face into a torch tensor, hand it
+    to the neighbour, unpack; same bits as the single-domain run."""
+    import torch
+    cfg = CASES["freeslip_label15"]()
+    bounds = partition(cfg.nx, 2, cylinder_columns(cfg))
+    stream = torch.cuda.Stream()
+    sims = [mrlbm.Simulation(cfg, precision=64, slab=b) for b in bounds]
+    for s in sims:
+        s.set_stream(stream.cuda_stream)
+    n, e = sims[0].halo_size()
+    assert n == 3 * cfg.ny and e == 8
+    buf = {(r, side): torch.empty(n, dtype=torch.float64, device="cuda") for r in range(2) for side in range(2)}
+    with torch.cuda.stream(stream):
+        for _ in range(30):
+            for s in sims:
+                s.step(1)
+            sims[0].halo_pack(1, buf[(0, 1)].data_ptr())
+            sims[1].halo_pack(0, buf[(1, 0)].data_ptr())
+            sims[1].halo_unpack(0, buf[(0, 1)].data_ptr())
+            sims[0].halo_unpack(1, buf[(1, 0)].data_ptr())
+    torch.cuda.synchronize()
+    f_ref, _ = _single(mrlbm, cfg, 64, 30)
+    f = np.concatenate([s.get_state() for s in sims], axis=0)
+    assert np.array_equal(f, f_ref)
+    for s in sims:
+        s.close()
+
+
+def test_slab_cutting_the_cylinder_is_rejected(mrlbm):
+    cfg = CASES["benchmark_small_400x100"]()
+    lo, hi = cylinder_columns(cfg)
+    with pytest.raises(mrlbm.MrlbmError) as e:
+        mrlbm.Simulation(cfg, slab=(1, (lo + hi) // 2))
+    assert e.value.code == 3
