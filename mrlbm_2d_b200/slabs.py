@@ -6,7 +6,8 @@ after every step each slab sends the populations that cross its faces (3 x ny va
 to its neighbours, which is the one exchange the decomposition needs.  Within one process,
 `mrlbm_2d_b200.slabs_step` does this with device-to-device copies; across processes (one GPU
 per rank) `SlabExchange` packs the faces into tensors, swaps them with the neighbouring ranks
-(NCCL send/recv on GPUs; gloo in the host-logic tests) and unpacks them.
+(NCCL send/recv on GPUs; gloo through pinned host buffers where several ranks share one GPU,
+and on CPU for the host-logic tests) and unpacks them.
 
     run = DistributedSlabRun(cfg, precision=FP32)        # under torchrun, one rank per GPU
     run.step(1000)
@@ -55,10 +56,18 @@ def partition(nx, parts, keep=None, min_width=4):
     return [(edges[p], edges[p + 1] - 1) for p in range(parts)]
 
 
+def _host_transport(group):
+    import torch.distributed as dist
+    return dist.get_backend(group) == "gloo"
+
+
 class SlabExchange:
     """Halo swap of one slab with its left and right neighbours (ranks rank-1, rank+1) over
     torch.distributed.  pack(side, tensor) / unpack(side, tensor) move a face between the
-    slab's state and a flat tensor of n_values elements (side 0 left, 1 right)."""
+    slab's state and a flat tensor of n_values elements (side 0 left, 1 right).
+
+    With NCCL the faces travel device to device.  A gloo group moves host tensors only, so
+    device faces are staged through pinned host buffers (one copy each way per face)."""
 
     def __init__(self, rank, world, pack, unpack, n_values, dtype, device, group=None):
         import torch
@@ -67,25 +76,39 @@ class SlabExchange:
         self.right = rank + 1 if rank + 1 < world else None
         self.pack, self.unpack = pack, unpack
         self.group = group
+        device = torch.device(device)
         mk = lambda: torch.empty(n_values, dtype=dtype, device=device)
         self.send = {0: mk(), 1: mk()}
         self.recv = {0: mk(), 1: mk()}
+        self.staged = device.type == "cuda" and _host_transport(group)
+        if self.staged:
+            mh = lambda: torch.empty(n_values, dtype=dtype, pin_memory=True)
+            self.send_h = {0: mh(), 1: mh()}
+            self.recv_h = {0: mh(), 1: mh()}
 
     def exchange(self):
+        import torch
         import torch.distributed as dist
-        ops = []
-        for side, peer in ((0, self.left), (1, self.right)):
-            if peer is None:
-                continue
+        sides = [(side, peer) for side, peer in ((0, self.left), (1, self.right)) if peer is not None]
+        for side, _ in sides:
             self.pack(side, self.send[side])
-            ops.append(dist.P2POp(dist.isend, self.send[side], peer, self.group))
-            ops.append(dist.P2POp(dist.irecv, self.recv[side], peer, self.group))
+        send, recv = self.send, self.recv
+        if self.staged:
+            for side, _ in sides:
+                self.send_h[side].copy_(self.send[side])      # ordered after the pack on this stream
+            torch.cuda.current_stream().synchronize()
+            send, recv = self.send_h, self.recv_h
+        ops = []
+        for side, peer in sides:
+            ops.append(dist.P2POp(dist.isend, send[side], peer, self.group))
+            ops.append(dist.P2POp(dist.irecv, recv[side], peer, self.group))
         if ops:
             for r in dist.batch_isend_irecv(ops):
                 r.wait()
-        for side, peer in ((0, self.left), (1, self.right)):
-            if peer is not None:
-                self.unpack(side, self.recv[side])
+        for side, _ in sides:
+            if self.staged:
+                self.recv[side].copy_(self.recv_h[side])
+            self.unpack(side, self.recv[side])
 
 
 class DistributedSlabRun:
@@ -122,7 +145,11 @@ class DistributedSlabRun:
         import torch
         import torch.distributed as dist
         it, fd, fl, rin = self.sim.forces()
-        t = torch.tensor(np.stack([fd, fl, rin]), dtype=torch.float64, device="cuda")
+        dev = "cpu" if _host_transport(None) else "cuda"
+        t = torch.tensor(np.stack([fd, fl, rin]), dtype=torch.float64, device=dev)
         dist.all_reduce(t)
         a = t.cpu().numpy()
         return it, a[0], a[1], a[2]
+
+    def close(self):
+        self.sim.close()

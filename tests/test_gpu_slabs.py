@@ -79,3 +79,45 @@ def test_slab_cutting_the_cylinder_is_rejected(mrlbm):
     with pytest.raises(mrlbm.MrlbmError) as e:
         mrlbm.Simulation(cfg, slab=(1, (lo + hi) // 2))
     assert e.value.code == 3
+
+
+RANK_WORKER = r"""
+import json, os, sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {tests!r})
+import datetime
+import numpy as np
+import torch, torch.distributed as dist
+from cases import CASES
+from mrlbm_2d_b200.slabs import DistributedSlabRun
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+torch.cuda.set_device(0)
+run = DistributedSlabRun(CASES["benchmark_small_400x100"](), precision={prec}, device=0)
+run.step(25)
+it, fd, fl, rin = run.forces()
+np.save(os.path.join({out!r}, "f%d.npy" % run.rank), run.sim.get_state())
+if run.rank == 0:
+    np.save(os.path.join({out!r}, "forces.npy"), np.stack([fd, fl, rin]))
+print(json.dumps({{"rank": run.rank, "bounds": run.bounds[run.rank], "status": run.sim.status()}}), flush=True)
+run.close()
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_distributed_slab_run_two_ranks_on_one_gpu(mrlbm, prec, tmp_path):
+    """DistributedSlabRun end to end: two processes, one slab each, sharing the GPU, with the
+    faces swapped over a gloo group through pinned host buffers (the kernels of the two ranks
+    never wait on each other; the host does).  Same bits as the single-domain run."""
+    import json
+    import os
+    from test_cpu_multirank import _launch
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = RANK_WORKER.format(root=os.path.dirname(here), tests=here, prec=prec, out=str(tmp_path))
+    outs = _launch(code, world=2, timeout=300)
+    recs = sorted((json.loads(o.strip().splitlines()[-1]) for o in outs), key=lambda r: r["rank"])
+    assert [r["status"] for r in recs] == [0, 0]
+    f = np.concatenate([np.load(tmp_path / f"f{r}.npy") for r in range(2)], axis=0)
+    f_ref, (it, fd, fl, rin) = _single(mrlbm, CASES["benchmark_small_400x100"](), prec, 25)
+    assert np.array_equal(f, f_ref)
+    got = np.load(tmp_path / "forces.npy")
+    assert np.array_equal(got[0], fd) and np.array_equal(got[1], fl) and np.array_equal(got[2], rin)
