@@ -637,7 +637,7 @@ static int create_impl(const mrlbm_config* cfg, int precision, int device, int s
     ok = ok && ck(cudaMalloc((void**)&h->d_boxmap, nbox * sizeof(int)), "cudaMalloc boxmap");
     const size_t nscratch = 2 * (size_t)nb + (size_t)ny + 8;
     ok = ok && ck(cudaMalloc((void**)&h->d_partials, nscratch * sizeof(double)), "cudaMalloc partials") &&
-         ck(cudaMalloc((void**)&h->d_counter, sizeof(unsigned)), "cudaMalloc counter") &&
+         ck(cudaMalloc((void**)&h->d_counter, 2 * sizeof(unsigned)), "cudaMalloc counter") &&
          ck(cudaMalloc((void**)&h->d_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMalloc ring") &&
          ck(cudaMalloc((void**)&h->d_err, sizeof(int)), "cudaMalloc err") &&
          ck(cudaMallocHost((void**)&h->h_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMallocHost ring");
@@ -654,7 +654,7 @@ static int create_impl(const mrlbm_config* cfg, int precision, int device, int s
     if (!h->geo.boxmap.empty())
         ok = ok && ck(cudaMemcpy(h->d_boxmap, h->geo.boxmap.data(), h->geo.boxmap.size() * sizeof(int),
                                  cudaMemcpyHostToDevice), "upload boxmap");
-    ok = ok && ck(cudaMemset(h->d_counter, 0, sizeof(unsigned)), "memset") && ck(cudaMemset(h->d_err, 0, sizeof(int)), "memset");
+    ok = ok && ck(cudaMemset(h->d_counter, 0, 2 * sizeof(unsigned)), "memset") && ck(cudaMemset(h->d_err, 0, sizeof(int)), "memset");
     if (!ok) { std::string m = g_create_error; return bail(MRLBM_ECUDA, m); }
     std::vector<double> f0;
     initial_state(h->cfg, h->lat, gnx, ny, f0);

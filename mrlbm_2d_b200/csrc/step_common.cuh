@@ -151,50 +151,101 @@ struct BTab {
     __device__ __forceinline__ int gi(int field, int li) const { return i[field * n + li]; }
 };
 
-// The last boundary or edge block to finish sums the per-node forces and the inlet column in
-// index order, as the reference's sum() does (2d_mrlbm.f90:359, 488-489): the result does not
-// depend on the launch shape and equals the reference's sums bit for bit.
-template <class Phys>
-__device__ __forceinline__ void aux_tail(const typename Phys::P& p, unsigned char* smem) {
-    if (!p.do_stats) return;
+// The per-step sums of the force record (Fx and Fy over the wall nodes, rho over the inlet
+// column) are taken in index order, as the reference's sum() does (2d_mrlbm.f90:359,
+// 488-489): the result does not depend on the launch shape and equals the reference's sums
+// bit for bit.  Two tails do them, each in the last block of its group to finish: the last
+// boundary block sums the forces (arrival counter 0), the last of the edge blocks that hold
+// the inlet column sums rho (counter 1), so neither waits for the other group.
+
+// True in the last of n blocks to arrive at counter c (block-uniform).
+__device__ __forceinline__ bool last_to_arrive(unsigned* c, int n) {
     __shared__ unsigned ticket;
-    __shared__ double sm[3];
-    const int tid = threadIdx.x;
     __threadfence();
     __syncthreads();
-    if (tid == 0) ticket = atomicAdd(p.counter, 1u);
+    if (threadIdx.x == 0) ticket = atomicAdd(c, 1u);
     __syncthreads();
-    if (ticket != (unsigned)(p.nbblk + p.neblk - 1)) return;
-    __threadfence();
-    // Three sequential sums (Fx over nodes, Fy over nodes, rho over the inlet column), one per
-    // warp: the warp stages AUX_CHUNK terms at a time in shared memory with parallel loads and
-    // its lane 0 adds them in index order, so only the adds are serial.
-    const int lane = tid & 31;
-    for (int w = tid >> 5; w < 3; w += (int)(blockDim.x >> 5)) {   // 64-thread blocks: a warp does two
-        const int n = w < 2 ? p.nb : (p.halo_l ? 0 : p.L.ny);      // an x-slab without column 1 adds 0
-        const double* v = p.partials + (w == 0 ? 0 : (w == 1 ? p.nb : 2 * p.nb));
-        double* st = reinterpret_cast<double*>(smem) + w * AUX_CHUNK;
-        double acc = 0.0;
-        for (int q0 = 0; q0 < n; q0 += AUX_CHUNK) {
-            const int m = min(AUX_CHUNK, n - q0);
+    const bool last = ticket == (unsigned)(n - 1);
+    if (last) __threadfence();
+    return last;
+}
+
+// ((0 + v[0]) + v[1]) + ... + v[n-1] by one warp, returned in lane 0.  The warp stages
+// AUX_CHUNK terms per round in shared memory (st) with parallel loads and issues the next
+// round's loads before lane 0 adds the current round, so only the adds are serial.
+__device__ __forceinline__ double warp_ordered_sum(const double* v, int n, double* st, int lane) {
+    constexpr int R = AUX_CHUNK / 32;
+    double r[R];
 #pragma unroll
-            for (int r = 0; r < AUX_CHUNK / 32; ++r) {
-                const int q = r * 32 + lane;
-                if (q < m) st[q] = __ldcg(v + q0 + q);
+    for (int u = 0; u < R; ++u) {
+        const int q = u * 32 + lane;
+        r[u] = q < n ? __ldcg(v + q) : 0.0;
+    }
+    double acc = 0.0;
+    for (int q0 = 0; q0 < n; q0 += AUX_CHUNK) {
+        const int m = min(AUX_CHUNK, n - q0);
+#pragma unroll
+        for (int u = 0; u < R; ++u) st[u * 32 + lane] = r[u];
+        __syncwarp();
+        const int q1 = q0 + AUX_CHUNK;
+        if (q1 < n) {
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const int q = q1 + u * 32 + lane;
+                r[u] = q < n ? __ldcg(v + q) : 0.0;
             }
-            __syncwarp();
-            if (lane == 0) {
-#pragma unroll 16
-                for (int q = 0; q < m; ++q) acc = acc + st[q];
-            }
-            __syncwarp();
         }
-        if (lane == 0) sm[w] = acc;
+        if (lane == 0) {
+#pragma unroll 16
+            for (int q = 0; q < m; ++q) acc = acc + st[q];
+        }
+        __syncwarp();
+    }
+    return acc;
+}
+
+// Force tail, called by every boundary block once its nodes' forces are in p.partials.
+template <class Phys>
+__device__ __forceinline__ void force_tail(const typename Phys::P& p, unsigned char* smem) {
+    if (!p.do_stats) return;
+    if (!last_to_arrive(p.counter, p.nbblk)) return;
+    __shared__ double sm[2];
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int w = tid >> 5; w < 2; w += (int)(blockDim.x >> 5)) {     // Fx by warp 0, Fy by warp 1
+        const double sum = warp_ordered_sum(p.partials + w * p.nb, p.nb, reinterpret_cast<double*>(smem) + w * AUX_CHUNK, lane);
+        if (lane == 0) sm[w] = sum;
     }
     __syncthreads();
     if (tid == 0) {
-        if (p.rec) { p.rec[0] = (double)p.iter; p.rec[1] = sm[0]; p.rec[2] = sm[1]; p.rec[3] = sm[2]; }
-        *p.counter = 0u;
+        if (p.rec) {
+            p.rec[0] = (double)p.iter;
+            p.rec[1] = sm[0];
+            p.rec[2] = sm[1];
+            if (p.halo_l) p.rec[3] = 0.0;                   // an x-slab without column 1 adds 0
+        }
+        p.counter[0] = 0u;
+    }
+}
+
+// Edge blocks [0, inlet_blocks) hold the inlet column (it comes first in their enumeration).
+__device__ __forceinline__ int inlet_blocks(int ny, int halo_l) {
+    return halo_l ? 0 : (ny + (int)blockDim.x - 1) / (int)blockDim.x;
+}
+
+// Inlet tail, called by every edge block once its inlet nodes' rho are in p.partials.
+template <class Phys>
+__device__ __forceinline__ void inlet_tail(const typename Phys::P& p, unsigned char* smem, int eb) {
+    if (!p.do_stats) return;
+    const int nin = inlet_blocks(p.L.ny, p.halo_l);
+    if (eb >= nin) return;
+    if (!last_to_arrive(p.counter + 1, nin)) return;
+    const int tid = threadIdx.x;
+    if (tid < 32) {
+        const double sum = warp_ordered_sum(p.partials + 2 * p.nb, p.L.ny, reinterpret_cast<double*>(smem), tid);
+        if (tid == 0) {
+            if (p.rec) p.rec[3] = sum;
+            p.counter[1] = 0u;
+        }
     }
 }
 
@@ -254,29 +305,33 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
         Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
         if (p.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
     }
-    aux_tail<Phys>(p, smem);
+    force_tail<Phys>(p, smem);
 }
 
-// Edge blocks: one thread per domain-edge node (rows 1 and ny, then columns 1 and nx without
-// the corners), so the edge closures (outlet neighbour gather, inlet/outlet/wall closures,
-// 2d_mrlbm.f90:249-272, 313-351) run side by side instead of serially inside bulk tiles.  The
-// thread of node (1,j) also records rho(1,j) after the closures for the inlet running mean
-// (2d_mrlbm.f90:359).
+// Edge blocks: one thread per domain-edge node, so the edge closures (outlet neighbour gather,
+// inlet/outlet/wall closures, 2d_mrlbm.f90:249-272, 313-351) run side by side instead of
+// serially inside bulk tiles.  Order: column 1 (j = 1..ny), column nx, then rows 1 and ny
+// without the corners; an x-slab's halo faces are not edges.  The thread of node (1,j) also
+// records rho(1,j) after the closures for the inlet running mean (2d_mrlbm.f90:359).
 template <class Phys>
 __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, unsigned char* smem) {
     const int nx = p.L.nx, ny = p.L.ny;
     const int e = eb * (int)blockDim.x + (int)threadIdx.x;
-    const int nl = p.halo_l ? 0 : ny - 2, nr = p.halo_r ? 0 : ny - 2;   // edge columns of this lattice
-    if (e < 2 * nx + nl + nr) {
+    const int cl = p.halo_l ? 0 : 1, cr = p.halo_r ? 0 : 1;         // edge columns of this lattice
+    const int nl = cl * ny, nr = cr * ny, nrow = nx - cl - cr;
+    if (e < nl + nr + 2 * nrow) {
         int i, j;
-        if (e < nx) { i = e + 1; j = 1; }
-        else if (e < 2 * nx) { i = e - nx + 1; j = ny; }
-        else if (e < 2 * nx + nl) { i = 1; j = e - 2 * nx + 2; }
-        else { i = nx; j = e - 2 * nx - nl + 2; }
+        if (e < nl) { i = 1; j = e + 1; }
+        else if (e < nl + nr) { i = nx; j = e - nl + 1; }
+        else {
+            const int q = e - nl - nr;
+            i = cl + 1 + (q < nrow ? q : q - nrow);
+            j = q < nrow ? 1 : ny;
+        }
         const double rho = Phys::edge_bulk_node(p, i, j, CLS_FLUID);
         if (p.do_stats && i == 1 && !p.halo_l) p.partials[2 * p.nb + j - 1] = rho;
     }
-    aux_tail<Phys>(p, smem);
+    inlet_tail<Phys>(p, smem, eb);
 }
 
 // Shared memory of an auxiliary block: the boundary tables and, afterwards, the tail's

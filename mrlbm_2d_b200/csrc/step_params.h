@@ -70,7 +70,7 @@ struct alignas(64) StepParams {
     int label15_allnine;
     // reduction scratch and output
     double* partials;             // per-step scratch: Fx[nb], Fy[nb], rho(1,j)[ny]
-    unsigned* counter;            // arrival counter of boundary blocks (reset by the last)
+    unsigned* counter;            // [0] arrivals of boundary blocks, [1] of inlet edge blocks (reset by the last)
     double* rec;                  // REC_WORDS doubles for this step, or null
     double* node_force;           // optional per-boundary-node (Fx, Fy) [2 * nb], or null
     int iter;
