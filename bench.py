@@ -8,8 +8,9 @@ grid, forces reduced every step.  Synthetic, seeded inputs only.
                   [--precision 32|64] [--case mid|large|small]
 
 `value` is the aggregate MLUPS of the headline precision (FP32 deviation form unless
---precision 64), each timed step preceded by an L2 flush (a 256 MiB write) outside its CUDA
-event pair; `e2e` is the same metric through the public C ABI with host buffers: upload the
+--precision 64), each timed step preceded by an L2 flush outside its CUDA event pair (a
+256 MiB write, then a read of the same buffer, so L2 holds none of the state and the flush's
+own dirty lines are written back before the step starts); `e2e` is the same metric through the public C ABI with host buffers: upload the
 initial populations, K steps, drain the force history every 100 steps, read the last step's
 rho/ux/uy back.  Under torchrun every rank runs an independent replica (its own seed) on its
 own GPU: weak scaling, no collective on the data path; times are max over ranks.
@@ -283,6 +284,13 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    flush_words = flush.view(torch.int64)
+
+    def flush_l2():
+        # 256 MiB (twice the L2) written, then read: every line of the state is evicted, and
+        # the dirty lines the write leaves are cleaned here rather than inside the timed step
+        flush.zero_()
+        flush_words.sum()
 
     def barrier():
         ranks.barrier()
@@ -317,7 +325,7 @@ def main():
         barrier()
         t_wall0 = time.time()
         for s in range(K):
-            flush.zero_()
+            flush_l2()
             starts[s].record(stream)
             sim.step(1)
             ends[s].record(stream)
@@ -410,7 +418,7 @@ def main():
         "metric": "D2Q9 MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if head == 32 else "f64", "data": "synthetic (seeded noise init)",
-        "config": dict(case_desc(args.case, cfg), precision=f"fp{head}", l2="flushed before every timed step",
+        "config": dict(case_desc(args.case, cfg), precision=f"fp{head}", l2="flushed before every timed step (256 MiB written, then read)",
                        parallelism=f"replicas{world}", tile_shape=tile),
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -431,7 +439,7 @@ def main():
     if large:
         lcfg = make_case("large", 1234)
         rl = {"workload": case_desc("large", lcfg)["workload"], "steps": args.large_steps,
-              "l2": "flushed before every timed step (working set 4.8 GB FP32 / 9.7 GB FP64)", "peak": peak,
+              "l2": "flushed before every timed step, 256 MiB written then read (working set 4.8 GB FP32 / 9.7 GB FP64)", "peak": peak,
               "peak_kind": peak_kind, "unit": "GB/s", "bound": "hbm"}
         for prec, v in large.items():
             v = dict(v)

@@ -40,8 +40,15 @@ __device__ __forceinline__ void gather(const StepParams<T>& p, int i, int j, T f
             SrcSlot sl = stream_source(nx, ny, i, j, k, p.xper, p.yper, p.freeslip, p.halo_l, p.halo_r);
             f[k] = __ldg(p.src + p.L.at(sl.i, sl.j, sl.k));
         }
+        // overrides by a select over the nine slots: an index known only at run time would put
+        // f in local memory, and each load would then wait for the one before to be stored
         for (int q = 0; q < p.n_ovr; ++q)
-            if (p.ovr[q].i == i && p.ovr[q].j == j) f[p.ovr[q].k] = (T)p.ovr[q].v;
+            if (p.ovr[q].i == i && p.ovr[q].j == j) {
+                const int kq = p.ovr[q].k;
+                const T v = (T)p.ovr[q].v;
+#pragma unroll
+                for (int k = 0; k < Q; ++k) f[k] = k == kq ? v : f[k];
+            }
     }
 }
 

@@ -70,7 +70,7 @@ constexpr int M_BOTTOM = (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | 
 
 // Edge nodes: Dirichlet values and the regularized edge closures of apply_bc /
 // apply_bc_incomp (2d_mrlbm.f90:249-272, 1237-1494) in deviation form.
-__device__ __noinline__ void edge_node(const P& p, int i, int j, const float g[Q], Mac& m) {
+__device__ __forceinline__ void edge_node(const P& p, int i, int j, const float g[Q], Mac& m) {
     const int nx = p.L.nx, ny = p.L.ny;
     const bool outlet = !p.xper && !p.halo_r && i == nx;
     const bool inlet = !p.xper && !p.halo_l && i == 1;
@@ -260,8 +260,9 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<float>& tb, i
     if (p.node_force) { p.node_force[2 * l] = Fx; p.node_force[2 * l + 1] = Fy; }
 }
 
-// Edge nodes: own gather, Dirichlet values and closures (out of line, see the FP64 step).
-__device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
+// Edge nodes: own gather, Dirichlet values and closures.  Inline, so the populations stay in
+// registers and the gathers of a node overlap.
+__device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
     float g[Q];
     gather(p, i, j, g);
     Mac m = moments(p, g);

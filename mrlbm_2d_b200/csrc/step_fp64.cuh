@@ -109,7 +109,7 @@ constexpr int M_BOTTOM = (1 << 0) | (1 << 1) | (1 << 3) | (1 << 4) | (1 << 7) | 
 
 // Edge nodes: Dirichlet values (2d_mrlbm.f90:249-272) then the regularized closure the
 // reference applies last at this node (apply_bc / apply_bc_incomp, 2d_mrlbm.f90:313-351).
-__device__ __noinline__ void edge_node(const P& p, int i, int j, const double f[Q], Mac& m) {
+__device__ __forceinline__ void edge_node(const P& p, int i, int j, const double f[Q], Mac& m) {
     const int nx = p.L.nx, ny = p.L.ny;
     const bool outlet = !p.xper && !p.halo_r && i == nx;
     const bool inlet = !p.xper && !p.halo_l && i == 1;
@@ -386,9 +386,10 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
     if (p.node_force) { p.node_force[2 * l] = Fx; p.node_force[2 * l + 1] = Fy; }
 }
 
-// Edge nodes (first/last row or column): own gather, Dirichlet values and closures.  Out
-// of line so the interior path keeps its populations in registers.
-__device__ __noinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
+// Edge nodes (first/last row or column): own gather, Dirichlet values and closures.  Inline,
+// so the populations stay in registers and the gathers of a node overlap (edge blocks are a
+// branch of their own, so the bulk path's registers are not affected).
+__device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
     double f[Q];
     gather(p, i, j, f);
     Mac m = moments(f, p.hm, p.hp);
