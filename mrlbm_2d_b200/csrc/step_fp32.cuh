@@ -182,7 +182,7 @@ __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, float c
 // cancel exactly:  rho_I = W + G,  G' = W + (a1 + omega e2),  D_xy = SW_xy + d1, so
 //   R_xy = d1 - SG_xy - S_xy (a1 + omega e2 - G) / rho_I,
 //   den  = W + dden,  dden = a1 + (1-omega)(M'.B') + omega e2,  drho = (G - dden) / den.
-__device__ __noinline__ void closure_strong(const P& p, const BTab<float>& tb, int li, const float g[Q], float uxp,
+__device__ __forceinline__ void closure_strong(const P& p, const BTab<float>& tb, int li, const float g[Q], float uxp,
                                             float uyp, float Mxx, float Myy, Mac& m) {
     const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     const int label = tb.gi(I_LABEL, li);
@@ -226,7 +226,7 @@ __device__ __noinline__ void closure_strong(const P& p, const BTab<float>& tb, i
 
 // Lane 0 of a boundary node: extrapolation (wall value 0), closure, collision, store and
 // the momentum-exchange force accumulated in FP64 from w_k + g_k (2d_mrlbm.f90:558-591).
-__device__ __noinline__ void boundary_close(const P& p, const BTab<float>& tb, int li, int l, float ux2, float uy2,
+__device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb, int li, int l, float ux2, float uy2,
                                             float mx2, float my2, float ux3, float uy3, float mx3, float my3,
                                             double& Fx, double& Fy) {
     const int i = tb.gi(I_NODEI, li), j = tb.gi(I_NODEJ, li);
