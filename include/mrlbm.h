@@ -318,8 +318,20 @@ int mrlbm_halo_size(const mrlbm_handle* h, int64_t* n_values, int32_t* elem_byte
  * (both ordered on the handle's stream). */
 int mrlbm_halo_pack(mrlbm_handle* h, int32_t side, void* dst);
 int mrlbm_halo_unpack(mrlbm_handle* h, int32_t side, const void* src);
+/* Exchange overlapped with the step.  mrlbm_step_faces computes the halo-face columns (1 on a
+ * left halo face, nx on a right one) of the next step into the next time level, on the
+ * handle's stream; mrlbm_step then computes the whole slab and writes the same bits again.
+ * Between the two, mrlbm_halo_pack_next / mrlbm_halo_unpack_next (same layout as pack /
+ * unpack, on the handle's stream) can move the faces of that next level while the step runs
+ * elsewhere: per step, step_faces; on a second stream ordered after it, pack_next, the
+ * transport and the neighbour's unpack_next into its next level; mrlbm_step; the next
+ * step_faces waits for the second stream. */
+int mrlbm_step_faces(mrlbm_handle* h);
+int mrlbm_halo_pack_next(mrlbm_handle* h, int32_t side, void* dst);
+int mrlbm_halo_unpack_next(mrlbm_handle* h, int32_t side, const void* src);
 /* Advance adjacent slabs (given left to right) nsteps steps with the halo exchange between
- * them (device-to-device copies; peer copies across devices).  Synchronises at the end. */
+ * them (device-to-device copies; peer copies across devices), each slab's faces computed
+ * first and copied on a second stream while its step kernel runs.  Synchronises at the end. */
 int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps);
 
 /* ---- batched cases (no counterpart in the reference, which runs one case per process) ----

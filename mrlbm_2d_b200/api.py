@@ -39,6 +39,7 @@ EXPORTED = [
     "mrlbm_set_body_force", "mrlbm_adjoint_drag",
     "mrlbm_surface_enable", "mrlbm_get_probe_nodes", "mrlbm_get_surface",
     "mrlbm_create_slab", "mrlbm_halo_size", "mrlbm_halo_pack", "mrlbm_halo_unpack", "mrlbm_slabs_step",
+    "mrlbm_step_faces", "mrlbm_halo_pack_next", "mrlbm_halo_unpack_next",
 ]
 BATCH_PERSISTENT, BATCH_GRAPH = 0, 1
 
@@ -118,6 +119,9 @@ def load_library(path=None):
         "mrlbm_halo_size": [vp, vp, vp],
         "mrlbm_halo_pack": [vp, i32, vp],
         "mrlbm_halo_unpack": [vp, i32, vp],
+        "mrlbm_step_faces": [vp],
+        "mrlbm_halo_pack_next": [vp, i32, vp],
+        "mrlbm_halo_unpack_next": [vp, i32, vp],
         "mrlbm_slabs_step": [vp, i32, i32],
     }
     for name, args in sig.items():
@@ -359,6 +363,19 @@ class Simulation:
     def halo_unpack(self, side, src_ptr):
         """Copy a neighbour's packed face from device memory src_ptr into this slab's ghost column."""
         self._check(self._L.mrlbm_halo_unpack(self._h, int(side), ctypes.c_void_p(int(src_ptr))))
+
+    def step_faces(self):
+        """Compute the halo-face columns of the next step into the next time level (ahead of
+        step(1), which writes the same bits), so the faces can travel while the step runs."""
+        self._check(self._L.mrlbm_step_faces(self._h))
+
+    def halo_pack_next(self, side, dst_ptr):
+        """halo_pack from the time level the next step writes (after step_faces)."""
+        self._check(self._L.mrlbm_halo_pack_next(self._h, int(side), ctypes.c_void_p(int(dst_ptr))))
+
+    def halo_unpack_next(self, side, src_ptr):
+        """halo_unpack into the ghost column of the time level the next step writes."""
+        self._check(self._L.mrlbm_halo_unpack_next(self._h, int(side), ctypes.c_void_p(int(src_ptr))))
 
     def set_body_force(self, g):
         """Body force g of shape (2, nx, ny) (x and y components, [c, i-1, j-1]); None removes it."""

@@ -699,13 +699,18 @@ int mrlbm_halo_size(const mrlbm_handle* h, int64_t* n_values, int32_t* elem_byte
     return MRLBM_OK;
 }
 
-static int halo_copy(mrlbm_handle* h, int side, void* dev, bool pack, void* peer_dst, const mrlbm_handle* peer) {
+// One halo face between a slab's time level (next = false: the current state, true: the
+// level the next step writes) and a flat device buffer, or straight into a neighbour's
+// buffer peer_dst (same time level) on the handle's stream (or on `on`, if given).
+static int halo_copy(mrlbm_handle* h, int side, void* dev, bool pack, void* peer_dst, const mrlbm_handle* peer,
+                     bool next = false, cudaStream_t on = nullptr) {
     if (!h || side < 0 || side > 1) return MRLBM_EINVAL;
     if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
     CK(cudaSetDevice(h->device));
     const int ny = h->L.ny;
     const size_t e = h->elem, pitch_b = (size_t)h->L.pitch * e;
-    char* base = (char*)h->buf[h->cur];
+    char* base = (char*)h->buf[next ? 1 - h->cur : h->cur];
+    cudaStream_t st = on ? on : h->stream;
     for (int q = 0; q < 3; ++q) {
         if (pack) {
             const int i = side == 0 ? 1 : h->L.nx, k = HALO_OUT[side][q];
@@ -713,14 +718,14 @@ static int halo_copy(mrlbm_handle* h, int side, void* dev, bool pack, void* peer
             if (peer) {                              // straight into the neighbour's ghost column
                 const int pi = side == 0 ? peer->L.nx + 1 : 0;
                 char* dst = (char*)peer_dst + (size_t)peer->L.at(pi, 1, k) * e;
-                CK(cudaMemcpy2DAsync(dst, (size_t)peer->L.pitch * e, src, pitch_b, e, ny, cudaMemcpyDefault, h->stream));
+                CK(cudaMemcpy2DAsync(dst, (size_t)peer->L.pitch * e, src, pitch_b, e, ny, cudaMemcpyDefault, st));
             } else {
-                CK(cudaMemcpy2DAsync((char*)dev + (size_t)q * ny * e, e, src, pitch_b, e, ny, cudaMemcpyDefault, h->stream));
+                CK(cudaMemcpy2DAsync((char*)dev + (size_t)q * ny * e, e, src, pitch_b, e, ny, cudaMemcpyDefault, st));
             }
         } else {
             const int i = side == 0 ? 0 : h->L.nx + 1, k = HALO_IN[side][q];
             char* dst = base + (size_t)h->L.at(i, 1, k) * e;
-            CK(cudaMemcpy2DAsync(dst, pitch_b, (const char*)dev + (size_t)q * ny * e, e, e, ny, cudaMemcpyDefault, h->stream));
+            CK(cudaMemcpy2DAsync(dst, pitch_b, (const char*)dev + (size_t)q * ny * e, e, e, ny, cudaMemcpyDefault, st));
         }
     }
     return MRLBM_OK;
@@ -736,6 +741,57 @@ int mrlbm_halo_unpack(mrlbm_handle* h, int32_t side, const void* src) {
     return halo_copy(h, side, const_cast<void*>(src), false, nullptr, nullptr);
 }
 
+int mrlbm_halo_pack_next(mrlbm_handle* h, int32_t side, void* dst) {
+    if (!dst) return MRLBM_EINVAL;
+    return halo_copy(h, side, dst, true, nullptr, nullptr, true);
+}
+
+int mrlbm_halo_unpack_next(mrlbm_handle* h, int32_t side, const void* src) {
+    if (!src) return MRLBM_EINVAL;
+    return halo_copy(h, side, const_cast<void*>(src), false, nullptr, nullptr, true);
+}
+
+// Halo-face columns of the next step into the next time level (face_kernel), with the
+// parameters the step will use, minus its statistics, field sums and macroscopic output.
+int mrlbm_step_faces(mrlbm_handle* h) {
+    if (!h) return MRLBM_EINVAL;
+    if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
+    if (!h->halo_l && !h->halo_r) return MRLBM_OK;
+    CK(cudaSetDevice(h->device));
+    const mrlbm_config& c = h->cfg;
+    const int iter = h->iter + 1;
+    const bool plot = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
+    int rc;
+    if (h->precision == MRLBM_FP64) {
+        StepParams<double> p{};
+        fill_common(h, p);
+        p.src = (const double*)h->buf[h->cur];
+        p.dst = (double*)h->buf[1 - h->cur];
+        p.u_in = h->has_uin ? h->d_uin : nullptr;
+        p.body = h->has_body ? (const double*)h->d_body : nullptr;
+        p.ovr = h->ovr_live ? h->d_ovr : nullptr;
+        p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
+        p.zero_solid_u = plot;
+        p.iter = iter;
+        rc = launch_face_f64(p, h->stream);
+    } else {
+        StepParams<float> p{};
+        fill_common(h, p);
+        p.src = (const float*)h->buf[h->cur];
+        p.dst = (float*)h->buf[1 - h->cur];
+        p.u_in = h->has_uin ? (const float*)h->d_uin : nullptr;
+        p.body = h->has_body ? (const float*)h->d_body : nullptr;
+        p.ovr = h->ovr_live ? h->d_ovr : nullptr;
+        p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
+        p.zero_solid_u = plot;
+        p.iter = iter;
+        rc = launch_face_f32(p, h->stream);
+    }
+    ++h->launches;
+    if (rc != 0) return fail(h, MRLBM_ECUDA, std::string("face kernel launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    return MRLBM_OK;
+}
+
 int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps) {
     if (!hs || n < 1 || nsteps < 0) return MRLBM_EINVAL;
     for (int s = 0; s < n; ++s) {
@@ -744,40 +800,66 @@ int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps) {
         if (s > 0 && (!hs[s]->halo_l || !hs[s - 1]->halo_r || hs[s]->gx0 != hs[s - 1]->gx0 + hs[s - 1]->L.nx))
             return fail(hs[s], MRLBM_EINVAL, "slabs must be given left to right, adjacent");
     }
-    std::vector<cudaEvent_t> done(n), halo(n);
-    for (int s = 0; s < n; ++s) {
-        if (cudaSetDevice(hs[s]->device) != cudaSuccess) return fail(hs[s], MRLBM_ECUDA, "cudaSetDevice");
-        cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&halo[s], cudaEventDisableTiming);
-    }
+    // Per step and slab: the face kernel writes the halo-face columns of the next level
+    // (event face), the step kernel then computes the whole slab on the slab's stream while a
+    // side stream copies the faces into the neighbours' next levels.  A copy into a neighbour's
+    // level waits for the neighbour's previous step, which read that level; a slab's next face
+    // kernel waits for the copies into its level.
+    std::vector<cudaEvent_t> face(n), done(n), halo(n);
+    std::vector<cudaStream_t> side(n, nullptr);
     int rc = MRLBM_OK;
-    for (int t = 0; t < nsteps && rc == MRLBM_OK; ++t) {
-        for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
-            cudaSetDevice(hs[s]->device);
-            if (t > 0 && s > 0) cudaStreamWaitEvent(hs[s]->stream, halo[s - 1], 0);     // right-going halo
-            if (t > 0 && s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, halo[s + 1], 0); // left-going halo
-            rc = mrlbm_step(hs[s], 1, 0);
-            cudaEventRecord(done[s], hs[s]->stream);
-        }
-        // each slab sends its faces once both it and the receiver have stepped
-        for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
-            cudaSetDevice(hs[s]->device);
-            if (s > 0) cudaStreamWaitEvent(hs[s]->stream, done[s - 1], 0);
-            if (s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, done[s + 1], 0);
-            if (s > 0) rc = halo_copy(hs[s], 0, nullptr, true, hs[s - 1]->buf[hs[s - 1]->cur], hs[s - 1]);
-            if (rc == MRLBM_OK && s + 1 < n) rc = halo_copy(hs[s], 1, nullptr, true, hs[s + 1]->buf[hs[s + 1]->cur], hs[s + 1]);
+    for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
+        if (cudaSetDevice(hs[s]->device) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&side[s], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&face[s], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&halo[s], cudaEventDisableTiming) != cudaSuccess)
+            rc = fail(hs[s], MRLBM_ECUDA, "stream or event creation");
+        else {
+            cudaEventRecord(done[s], hs[s]->stream);         // "previous step" of the first step
             cudaEventRecord(halo[s], hs[s]->stream);
         }
     }
+    for (int t = 0; t < nsteps && rc == MRLBM_OK; ++t) {
+        for (int s = 0; s < n; ++s) {                          // copies of step t wait for the
+            cudaSetDevice(hs[s]->device);                      // neighbours' step t-1
+            if (s > 0) cudaStreamWaitEvent(side[s], done[s - 1], 0);
+            if (s + 1 < n) cudaStreamWaitEvent(side[s], done[s + 1], 0);
+        }
+        for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
+            cudaSetDevice(hs[s]->device);
+            if (s > 0) cudaStreamWaitEvent(hs[s]->stream, halo[s - 1], 0);      // right-going halo of t-1
+            if (s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, halo[s + 1], 0);  // left-going halo of t-1
+            rc = mrlbm_step_faces(hs[s]);
+            if (rc != MRLBM_OK) break;
+            cudaEventRecord(face[s], hs[s]->stream);
+            rc = mrlbm_step(hs[s], 1, 0);
+            cudaEventRecord(done[s], hs[s]->stream);
+        }
+        for (int s = 0; s < n && rc == MRLBM_OK; ++s) {
+            cudaSetDevice(hs[s]->device);
+            cudaStreamWaitEvent(side[s], face[s], 0);
+            // after mrlbm_step the handles' current level is the one step t writes
+            if (s > 0) rc = halo_copy(hs[s], 0, nullptr, true, hs[s - 1]->buf[hs[s - 1]->cur], hs[s - 1], false, side[s]);
+            if (rc == MRLBM_OK && s + 1 < n)
+                rc = halo_copy(hs[s], 1, nullptr, true, hs[s + 1]->buf[hs[s + 1]->cur], hs[s + 1], false, side[s]);
+            cudaEventRecord(halo[s], side[s]);
+        }
+    }
     for (int s = 0; s < n; ++s) {
+        if (!side[s]) continue;
         cudaSetDevice(hs[s]->device);
         cudaStreamWaitEvent(hs[s]->stream, halo[s], 0);
         if (s > 0) cudaStreamWaitEvent(hs[s]->stream, halo[s - 1], 0);
         if (s + 1 < n) cudaStreamWaitEvent(hs[s]->stream, halo[s + 1], 0);
     }
     for (int s = 0; s < n; ++s) {
+        if (!side[s]) continue;
         cudaSetDevice(hs[s]->device);
         cudaStreamSynchronize(hs[s]->stream);
+        cudaStreamSynchronize(side[s]);
+        cudaStreamDestroy(side[s]);
+        cudaEventDestroy(face[s]);
         cudaEventDestroy(done[s]);
         cudaEventDestroy(halo[s]);
     }

@@ -610,6 +610,40 @@ int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// Halo faces of an x-slab, ahead of the step: one thread per node of column 1 (left halo
+// face) and column nx (right halo face), computing the node exactly as the step kernel does
+// and writing it into the next time level.  The step kernel then writes the same bits again;
+// in between, the populations that cross the faces can already travel to the neighbours
+// while the rest of the slab is computed.  The caller clears fstat and macro (the step
+// kernel accumulates them) and do_stats.  A face never holds a wall node: the partition
+// keeps the cylinder and its stencils inside one slab.
+template <class Phys>
+__global__ void __launch_bounds__(128) face_kernel(const __grid_constant__ typename Phys::P p) {
+    using T = typename Phys::T;
+    const int ny = p.L.ny;
+    const int n = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (n >= 2 * ny) return;
+    const int side = n / ny, j = 1 + (n - side * ny);
+    if (side == 0 ? !p.halo_l : !p.halo_r) return;
+    const int i = side == 0 ? 1 : p.L.nx;
+    if (j == 1 || j == ny) {                          // rows 1 and ny: edge nodes
+        Phys::edge_bulk_node(p, i, j, CLS_FLUID);
+        return;
+    }
+    const int cls = node_class(p, i, j);
+    if (cls >= 0) return;
+    T f[Q];
+    gather(p, i, j, f);
+    Phys::finish(p, i, j, cls, f);
+}
+
+template <class Phys>
+int launch_face(const typename Phys::P& p, cudaStream_t s) {
+    const int n = 2 * p.L.ny;
+    face_kernel<Phys><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 template <class Phys, int BX, int BY, int NJ, int MINB>
 int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     const int nthr = BX * BY;

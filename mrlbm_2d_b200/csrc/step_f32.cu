@@ -5,6 +5,10 @@
 
 namespace mrlbm {
 
+int launch_face_f32(const StepParams<float>& p, void* stream) {
+    return launch_face<fp32::Physics>(p, (cudaStream_t)stream);
+}
+
 int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers) {
     cudaStream_t s = (cudaStream_t)stream;
     using Ph = fp32::Physics;

@@ -8,6 +8,10 @@
 
 namespace mrlbm {
 
+int launch_face_f64(const StepParams<double>& p, void* stream) {
+    return launch_face<fp64::Physics>(p, (cudaStream_t)stream);
+}
+
 int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers) {
     cudaStream_t s = (cudaStream_t)stream;
     using Ph = fp64::Physics;

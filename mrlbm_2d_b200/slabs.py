@@ -112,7 +112,11 @@ class SlabExchange:
 
 
 class DistributedSlabRun:
-    """One x-slab of `cfg` per rank (torch.distributed initialised, one GPU per rank)."""
+    """One x-slab of `cfg` per rank (torch.distributed initialised, one GPU per rank).
+
+    Each step overlaps the exchange with the step: the face kernel writes the halo-face
+    columns of the next level, a second stream sends them (and receives the neighbours') while
+    the step kernel computes the whole slab, and the next step waits for that stream."""
 
     def __init__(self, cfg, precision=api.FP32, bounds=None, device=None):
         import torch
@@ -127,18 +131,31 @@ class DistributedSlabRun:
         self.bounds = bounds
         self.sim = api.Simulation(cfg, precision=precision, device=dev, slab=bounds[self.rank])
         self.stream = torch.cuda.current_stream(dev)
+        self.side = torch.cuda.Stream(dev)
         self.sim.set_stream(self.stream.cuda_stream)
         n, e = self.sim.halo_size()
         dtype = torch.float64 if e == 8 else torch.float32
-        self.ex = SlabExchange(self.rank, self.world,
-                               lambda side, t: self.sim.halo_pack(side, t.data_ptr()),
-                               lambda side, t: self.sim.halo_unpack(side, t.data_ptr()),
-                               n, dtype, torch.device("cuda", dev))
+        # the side stream packs and unpacks: point the handle at it around those copies
+        def on_side(fn):
+            def run(side, t):
+                self.sim.set_stream(self.side.cuda_stream)
+                try:
+                    fn(side, t.data_ptr())
+                finally:
+                    self.sim.set_stream(self.stream.cuda_stream)
+            return run
+        self.ex = SlabExchange(self.rank, self.world, on_side(self.sim.halo_pack_next),
+                               on_side(self.sim.halo_unpack_next), n, dtype, torch.device("cuda", dev))
 
     def step(self, n=1):
+        import torch
         for _ in range(int(n)):
+            self.sim.step_faces()
+            self.side.wait_stream(self.stream)            # faces written; previous step done
+            with torch.cuda.stream(self.side):
+                self.ex.exchange()
             self.sim.step(1)
-            self.ex.exchange()
+            self.stream.wait_stream(self.side)            # ghost columns in before the next step
 
     def forces(self):
         """Force history summed over the slabs (iter, F_drag, F_lift, sum rho(1,:))."""

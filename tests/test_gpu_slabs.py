@@ -73,6 +73,53 @@ def test_halo_pack_unpack_exchange_in_torch_buffers(mrlbm):
         s.close()
 
 
+@pytest.mark.parametrize("prec", [64, 32])
+def test_faces_first_exchange_overlapping_the_step(mrlbm, prec):
+    """The overlapped order through torch buffers: face kernels, then on a second stream the
+    faces of the next level packed and unpacked into the neighbour's next level, while the
+    step kernels run on the first stream.  Same bits as the single-domain run."""
+    import torch
+    cfg = CASES["benchmark_small_400x100"]()
+    bounds = partition(cfg.nx, 2, cylinder_columns(cfg))
+    main, side = torch.cuda.Stream(), torch.cuda.Stream()
+    sims = [mrlbm.Simulation(cfg, precision=prec, slab=b) for b in bounds]
+    for s in sims:
+        s.set_stream(main.cuda_stream)
+    n, e = sims[0].halo_size()
+    dt = torch.float64 if e == 8 else torch.float32
+    buf = {(r, side_): torch.empty(n, dtype=dt, device="cuda") for r in range(2) for side_ in range(2)}
+    for _ in range(30):
+        for s in sims:
+            s.step_faces()
+        side.wait_stream(main)
+        for s in sims:
+            s.set_stream(side.cuda_stream)
+        sims[0].halo_pack_next(1, buf[(0, 1)].data_ptr())
+        sims[1].halo_pack_next(0, buf[(1, 0)].data_ptr())
+        sims[1].halo_unpack_next(0, buf[(0, 1)].data_ptr())
+        sims[0].halo_unpack_next(1, buf[(1, 0)].data_ptr())
+        for s in sims:
+            s.set_stream(main.cuda_stream)
+            s.step(1)
+        main.wait_stream(side)
+    torch.cuda.synchronize()
+    f_ref, _ = _single(mrlbm, cfg, prec, 30)
+    f = np.concatenate([s.get_state() for s in sims], axis=0)
+    assert np.array_equal(f, f_ref)
+    for s in sims:
+        assert s.status() == 0
+        s.close()
+
+
+def test_step_faces_is_a_no_op_without_halo(mrlbm):
+    cfg = CASES["benchmark_small_400x100"]()
+    s = mrlbm.Simulation(cfg, precision=64)
+    f0, it0 = s.get_state(), s.iter
+    s.step_faces()
+    assert np.array_equal(s.get_state(), f0) and s.iter == it0
+    s.close()
+
+
 def test_slab_cutting_the_cylinder_is_rejected(mrlbm):
     cfg = CASES["benchmark_small_400x100"]()
     lo, hi = cylinder_columns(cfg)
