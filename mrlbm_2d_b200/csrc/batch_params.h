@@ -40,6 +40,7 @@ struct BatchArgs {
     int step0;                     // index of this launch's first step within the call
     int call_steps;                // steps of the whole call (macro output on the last)
     int want_macro;
+    int full;                      // some case has field statistics, macroscopic output or a body force
 };
 
 // Host-side launch entry points (step_f64.cu / step_f32.cu).  tile_cfg is a vector shape

@@ -761,6 +761,8 @@ int mrlbm_step_faces(mrlbm_handle* h) {
     const mrlbm_config& c = h->cfg;
     const int iter = h->iter + 1;
     const bool plot = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
+    // the kernel instantiation the step will use when it asks for no macroscopic output
+    const bool full = h->has_body || (h->d_fstat && iter >= h->fstat_begin && iter <= h->fstat_end);
     int rc;
     if (h->precision == MRLBM_FP64) {
         StepParams<double> p{};
@@ -773,7 +775,7 @@ int mrlbm_step_faces(mrlbm_handle* h) {
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         p.zero_solid_u = plot;
         p.iter = iter;
-        rc = launch_face_f64(p, h->stream);
+        rc = launch_face_f64(p, full, h->stream);
     } else {
         StepParams<float> p{};
         fill_common(h, p);
@@ -785,7 +787,7 @@ int mrlbm_step_faces(mrlbm_handle* h) {
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         p.zero_solid_u = plot;
         p.iter = iter;
-        rc = launch_face_f32(p, h->stream);
+        rc = launch_face_f32(p, full, h->stream);
     }
     ++h->launches;
     if (rc != 0) return fail(h, MRLBM_ECUDA, std::string("face kernel launch failed: ") + cudaGetErrorString(cudaGetLastError()));
@@ -1556,7 +1558,7 @@ struct mrlbm_batch {
     int stage_i = 0;
     size_t stage_bytes = 0;
     cudaGraphExec_t graph = nullptr;
-    int graph_cfg = -1, graph_steps = 0, graph_macro = -1;
+    int graph_cfg = -1, graph_steps = 0, graph_macro = -1, graph_full = -1;
 };
 
 namespace {
@@ -1671,6 +1673,13 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
     const int* off = reinterpret_cast<const int*>(b->h_stage[si] + pb + cb);
     const int items = off[n] + off[2 * n + 1];
 
+    // the full kernel instantiation when any case has field statistics or a body force in this
+    // call, or macroscopic output is asked for; the lean one otherwise
+    int full = want_macro ? 1 : 0;
+    for (mrlbm_handle* h : b->h) {
+        if (h->has_body) full = 1;
+        if (h->d_fstat && std::max(h->iter + 1, h->fstat_begin) <= std::min(h->iter + steps, h->fstat_end)) full = 1;
+    }
     BatchArgs<double> a64{};
     BatchArgs<float> a32{};
     auto setup = [&](auto& a, auto* params) {
@@ -1682,6 +1691,7 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
         a.ncases = n;
         a.call_steps = steps;
         a.want_macro = want_macro;
+        a.full = full;
     };
     setup(a64, (const StepParams<double>*)b->d_params);
     setup(a32, (const StepParams<float>*)b->d_params);
@@ -1699,7 +1709,8 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
             return bfail(b, MRLBM_ECUDA, std::string("batch launch: ") + cudaGetErrorString(cudaGetLastError()));
         ++b->launches;
     } else {
-        if (!b->graph || b->graph_cfg != b->tile_cfg || b->graph_steps != steps || b->graph_macro != want_macro) {
+        if (!b->graph || b->graph_cfg != b->tile_cfg || b->graph_steps != steps || b->graph_macro != want_macro ||
+            b->graph_full != full) {
             if (b->graph) cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
             BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -1718,6 +1729,7 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
             b->graph_cfg = b->tile_cfg;
             b->graph_steps = steps;
             b->graph_macro = want_macro;
+            b->graph_full = full;
         }
         BCK(cudaGraphLaunch(b->graph, b->stream));
         b->launches += steps;

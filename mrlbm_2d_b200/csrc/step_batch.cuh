@@ -72,8 +72,8 @@ __device__ __forceinline__ bool batch_barrier(BatchBarrier* bar) {
     return ok != 0;
 }
 
-template <class Phys, int WARPS, int NJ>
-__global__ void __launch_bounds__(WARPS * 32) step_kernel_batch(const __grid_constant__ BatchArgs<typename Phys::T> a) {
+template <class Phys, int WARPS, int NJ, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __grid_constant__ BatchArgs<typename Phys::T> a) {
     using T = typename Phys::T;
     using P = typename Phys::P;
     __shared__ __align__(64) unsigned char sp_raw[sizeof(P)];
@@ -122,10 +122,11 @@ __global__ void __launch_bounds__(WARPS * 32) step_kernel_batch(const __grid_con
     }
 }
 
-// Block sizes of the batch kernels: the vector shapes' warps per block.
-template <class Phys, int WARPS, int NJ>
+// Block sizes and register budgets of the batch kernels: the vector shapes' (warps per block,
+// resident blocks per SM).
+template <class Phys, int WARPS, int NJ, int MINB>
 int launch_step_batch(const BatchArgs<typename Phys::T>& a, int grid, bool cooperative, cudaStream_t s) {
-    auto k = step_kernel_batch<Phys, WARPS, NJ>;
+    auto k = step_kernel_batch<Phys, WARPS, NJ, MINB>;
     if (!cooperative) {
         k<<<(unsigned)grid, WARPS * 32, 0, s>>>(a);
         return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -137,10 +138,10 @@ int launch_step_batch(const BatchArgs<typename Phys::T>& a, int grid, bool coope
                : -1;
 }
 
-template <class Phys, int WARPS, int NJ>
+template <class Phys, int WARPS, int NJ, int MINB>
 int batch_blocks_per_sm() {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_batch<Phys, WARPS, NJ>, WARPS * 32, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_batch<Phys, WARPS, NJ, MINB>, WARPS * 32, 0) !=
         cudaSuccess)
         return 0;
     return n;

@@ -52,6 +52,14 @@ __device__ __forceinline__ void gather(const StepParams<T>& p, int i, int j, T f
     }
 }
 
+// Non-positive (or NaN) density at a node: set the handle's error flag.  The flag is read
+// first, so a case that has gone unstable costs one atomic per SM until the flag is visible,
+// not one per node and step on a single address.
+template <class T>
+__device__ __forceinline__ void flag_bad_density(const StepParams<T>& p) {
+    if (__ldcg(p.errflag) == 0) atomicOr(p.errflag, 1);
+}
+
 template <class T>
 __device__ __forceinline__ void store(const StepParams<T>& p, int i, int j, const T fo[Q]) {
     T* d = p.dst + ((int)(j * p.L.pitch + i + p.L.off));

@@ -5,13 +5,13 @@
 
 namespace mrlbm {
 
-int launch_face_f32(const StepParams<float>& p, void* stream) {
-    return launch_face<fp32::Physics>(p, (cudaStream_t)stream);
+int launch_face_f32(const StepParams<float>& p, bool full, void* stream) {
+    return full ? launch_face<fp32::Physics>(p, (cudaStream_t)stream)
+                : launch_face<fp32::PhysicsLean>(p, (cudaStream_t)stream);
 }
 
-int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers) {
-    cudaStream_t s = (cudaStream_t)stream;
-    using Ph = fp32::Physics;
+template <class Ph>
+static int launch_step_impl(const StepParams<float>& p, int tile_cfg, cudaStream_t s, int workers) {
     switch (tile_cfg) {
 #define MRLBM_TILE_CASE(id, bx, by, nj, mb) \
     case id: return launch_step_tiles<Ph, bx, by, nj, mb>(p, s);
@@ -35,6 +35,13 @@ int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int 
 #undef MRLBM_PIPE_CASE
     default: return -1;
     }
+}
+
+// The lean instantiation when the step has no field statistics, macroscopic output or body force.
+int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers) {
+    cudaStream_t s = (cudaStream_t)stream;
+    return (p.fstat || p.macro || p.body) ? launch_step_impl<fp32::Physics>(p, tile_cfg, s, workers)
+                                          : launch_step_impl<fp32::PhysicsLean>(p, tile_cfg, s, workers);
 }
 
 int tma_ctas_per_sm_f32(int tile_cfg) {
@@ -65,23 +72,28 @@ void tma_box(int precision, int tile_cfg, int* box_w, int* box_h, int* stages) {
     *stages = c.stages;
 }
 
-int launch_batch_f32(const BatchArgs<float>& a, int tile_cfg, int grid, bool cooperative, void* stream) {
-    cudaStream_t s = (cudaStream_t)stream;
-    using Ph = fp32::Physics;
+template <class Ph>
+static int launch_batch_impl(const BatchArgs<float>& a, int tile_cfg, int grid, bool cooperative, cudaStream_t s) {
     switch (tile_cfg) {
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
-    case id: return launch_step_batch<Ph, w, nj>(a, grid, cooperative, s);
+    case id: return launch_step_batch<Ph, w, nj, mb>(a, grid, cooperative, s);
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
     default: return -2;
     }
 }
 
+int launch_batch_f32(const BatchArgs<float>& a, int tile_cfg, int grid, bool cooperative, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    return a.full ? launch_batch_impl<fp32::Physics>(a, tile_cfg, grid, cooperative, s)
+                  : launch_batch_impl<fp32::PhysicsLean>(a, tile_cfg, grid, cooperative, s);
+}
+
 int batch_blocks_per_sm_f32(int tile_cfg) {
     using Ph = fp32::Physics;
     switch (tile_cfg) {
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
-    case id: return batch_blocks_per_sm<Ph, w, nj>();
+    case id: return batch_blocks_per_sm<Ph, w, nj, mb>();
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
     default: return 0;

@@ -8,13 +8,13 @@
 
 namespace mrlbm {
 
-int launch_face_f64(const StepParams<double>& p, void* stream) {
-    return launch_face<fp64::Physics>(p, (cudaStream_t)stream);
+int launch_face_f64(const StepParams<double>& p, bool full, void* stream) {
+    return full ? launch_face<fp64::Physics>(p, (cudaStream_t)stream)
+                : launch_face<fp64::PhysicsLean>(p, (cudaStream_t)stream);
 }
 
-int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers) {
-    cudaStream_t s = (cudaStream_t)stream;
-    using Ph = fp64::Physics;
+template <class Ph>
+static int launch_step_impl(const StepParams<double>& p, int tile_cfg, cudaStream_t s, int workers) {
     switch (tile_cfg) {
 #define MRLBM_TILE_CASE(id, bx, by, nj, mb) \
     case id: return launch_step_tiles<Ph, bx, by, nj, mb>(p, s);
@@ -40,6 +40,13 @@ int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int
     }
 }
 
+// The lean instantiation when the step has no field statistics, macroscopic output or body force.
+int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers) {
+    cudaStream_t s = (cudaStream_t)stream;
+    return (p.fstat || p.macro || p.body) ? launch_step_impl<fp64::Physics>(p, tile_cfg, s, workers)
+                                          : launch_step_impl<fp64::PhysicsLean>(p, tile_cfg, s, workers);
+}
+
 int tma_ctas_per_sm_f64(int tile_cfg) {
     int n = 0;
     switch (tile_cfg) {
@@ -56,23 +63,28 @@ int tma_ctas_per_sm_f64(int tile_cfg) {
     return n;
 }
 
-int launch_batch_f64(const BatchArgs<double>& a, int tile_cfg, int grid, bool cooperative, void* stream) {
-    cudaStream_t s = (cudaStream_t)stream;
-    using Ph = fp64::Physics;
+template <class Ph>
+static int launch_batch_impl(const BatchArgs<double>& a, int tile_cfg, int grid, bool cooperative, cudaStream_t s) {
     switch (tile_cfg) {
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
-    case id: return launch_step_batch<Ph, w, nj>(a, grid, cooperative, s);
+    case id: return launch_step_batch<Ph, w, nj, mb>(a, grid, cooperative, s);
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
     default: return -2;
     }
 }
 
+int launch_batch_f64(const BatchArgs<double>& a, int tile_cfg, int grid, bool cooperative, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    return a.full ? launch_batch_impl<fp64::Physics>(a, tile_cfg, grid, cooperative, s)
+                  : launch_batch_impl<fp64::PhysicsLean>(a, tile_cfg, grid, cooperative, s);
+}
+
 int batch_blocks_per_sm_f64(int tile_cfg) {
     using Ph = fp64::Physics;
     switch (tile_cfg) {
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
-    case id: return batch_blocks_per_sm<Ph, w, nj>();
+    case id: return batch_blocks_per_sm<Ph, w, nj, mb>();
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
     default: return 0;

@@ -226,6 +226,7 @@ __device__ __forceinline__ void closure_strong(const P& p, const BTab<float>& tb
 
 // Lane 0 of a boundary node: extrapolation (wall value 0), closure, collision, store and
 // the momentum-exchange force accumulated in FP64 from w_k + g_k (2d_mrlbm.f90:558-591).
+template <bool FULL>
 __device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb, int li, int l, float ux2, float uy2,
                                             float mx2, float my2, float ux3, float uy3, float mx3, float my3,
                                             double& Fx, double& Fy) {
@@ -241,9 +242,9 @@ __device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb
         const float c = tb.gf(G_CTH, li), s = tb.gf(G_STH, li);
         closure_strong(p, tb, li, g, m.ux * c + m.uy * s, m.uy * c - m.ux * s, mxxp, myyp, m);
     }
-    if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
+    if (!(m.rho > 0.0f)) flag_bad_density(p);
+    if (FULL && p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (FULL && p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     float go[Q];
     collide(p, m, go);
     store(p, i, j, go);
@@ -262,52 +263,60 @@ __device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb
 
 // Edge nodes: own gather, Dirichlet values and closures.  Inline, so the populations stay in
 // registers and the gathers of a node overlap.
+template <bool FULL>
 __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
     float g[Q];
     gather(p, i, j, g);
     Mac m = moments(p, g);
     edge_node(p, i, j, g, m);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
-    if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
+    if (!(m.rho > 0.0f)) flag_bad_density(p);
+    if (FULL && p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (FULL && p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
     float go[Q];
     collide(p, m, go);
-    if (p.body) add_body_force(p, i, j, go);
+    if (FULL && p.body) add_body_force(p, i, j, go);
     store(p, i, j, go);
     return 1.0 + (double)m.drho;
 }
 
 // Interior fluid or solid node: populations already gathered.
+template <bool FULL>
 __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const float g[Q], float go[Q]) {
     FieldPre pre;
-    if (p.fstat) fields_load(p, i, j, pre);
+    if (FULL && p.fstat) fields_load(p, i, j, pre);
     Mac m = moments(p, g);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
-    if (!(m.rho > 0.0f)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) fields_store(p, i, j, pre, 1.0 + (double)m.drho, m.ux, m.uy);
+    if (!(m.rho > 0.0f)) flag_bad_density(p);
+    if (FULL && p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (FULL && p.fstat) fields_store(p, i, j, pre, 1.0 + (double)m.drho, m.ux, m.uy);
     collide(p, m, go);
-    if (p.body) add_body_force(p, i, j, go);
+    if (FULL && p.body) add_body_force(p, i, j, go);
 }
 
+template <bool FULL>
 __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const float g[Q]) {
     float go[Q];
-    compute(p, i, j, cls, g, go);
+    compute<FULL>(p, i, j, cls, g, go);
     store(p, i, j, go);
 }
 
-struct Physics {
+// FULL: the node paths include the optional per-node work (field statistics, macroscopic
+// output, body force), each behind its run-time switch.  The lean instantiation leaves it
+// out; the launchers pick it when all three are off, which keeps the registers and the
+// branches of that work out of the common step.
+template <bool FULL>
+struct PhysicsT {
     using P = StepParams<float>;
     using T = float;
     static __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const T f[Q], T fo[Q]) {
-        fp32::compute(p, i, j, cls, f, fo);
+        fp32::compute<FULL>(p, i, j, cls, f, fo);
     }
     static __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const T g[Q]) {
-        fp32::finish(p, i, j, cls, g);
+        fp32::finish<FULL>(p, i, j, cls, g);
     }
     static __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
-        return fp32::edge_bulk_node(p, i, j, cls);
+        return fp32::edge_bulk_node<FULL>(p, i, j, cls);
     }
     static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
                                                         T& mx, T& my) {
@@ -316,9 +325,11 @@ struct Physics {
     static __device__ __forceinline__ void boundary_close(const P& p, const BTab<T>& tb, int li, int l, T ux2, T uy2,
                                                           T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
                                                           double& Fy) {
-        fp32::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
+        fp32::boundary_close<FULL>(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
 };
+using Physics = PhysicsT<true>;
+using PhysicsLean = PhysicsT<false>;
 
 }  // namespace fp32
 }  // namespace mrlbm

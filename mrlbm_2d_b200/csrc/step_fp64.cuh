@@ -340,6 +340,7 @@ __device__ __noinline__ void closure_unrotated(const P& p, const BTab<double>& t
 // Lane 0 of a boundary node: extrapolated velocity / rotated moments from the reference
 // points (the wall value is 0; 2d_mrlbm.f90:809-814, 919-924), closure, collision, store,
 // momentum-exchange force (evaluate_forces, 2d_mrlbm.f90:558-591).
+template <bool FULL>
 __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, int li, int l, double ux2, double uy2,
                                             double mx2, double my2, double ux3, double uy3, double mx3, double my3,
                                             double& Fx, double& Fy) {
@@ -368,9 +369,9 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
     } else {
         closure_unrotated(p, tb, li, f, m.ux, m.uy, m);
     }
-    if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
+    if (!(m.rho > 0.0)) flag_bad_density(p);
+    if (FULL && p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (FULL && p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     double fo[Q];
     collide(p, m, fo);
     store(p, i, j, fo);
@@ -389,53 +390,61 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
 // Edge nodes (first/last row or column): own gather, Dirichlet values and closures.  Inline,
 // so the populations stay in registers and the gathers of a node overlap (edge blocks are a
 // branch of their own, so the bulk path's registers are not affected).
+template <bool FULL>
 __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
     double f[Q];
     gather(p, i, j, f);
     Mac m = moments(f, p.hm, p.hp);
     edge_node(p, i, j, f, m);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
-    if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
+    if (!(m.rho > 0.0)) flag_bad_density(p);
+    if (FULL && p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (FULL && p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
     double fo[Q];
     collide(p, m, fo);
-    if (p.body) add_body_force(p, i, j, fo);
+    if (FULL && p.body) add_body_force(p, i, j, fo);
     store(p, i, j, fo);
     return m.rho;
 }
 
 // Bulk node (fluid or solid).
 // Interior fluid or solid node: populations already gathered.
+template <bool FULL>
 __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const double f[Q], double fo[Q]) {
     FieldPre pre;
-    if (p.fstat) fields_load(p, i, j, pre);
+    if (FULL && p.fstat) fields_load(p, i, j, pre);
     Mac m = moments(f, p.hm, p.hp);
     if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
-    if (!(m.rho > 0.0)) atomicOr(p.errflag, 1);
-    if (p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
-    if (p.fstat) fields_store(p, i, j, pre, m.rho, m.ux, m.uy);
+    if (!(m.rho > 0.0)) flag_bad_density(p);
+    if (FULL && p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
+    if (FULL && p.fstat) fields_store(p, i, j, pre, m.rho, m.ux, m.uy);
     collide(p, m, fo);
-    if (p.body) add_body_force(p, i, j, fo);
+    if (FULL && p.body) add_body_force(p, i, j, fo);
 }
 
+template <bool FULL>
 __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const double f[Q]) {
     double fo[Q];
-    compute(p, i, j, cls, f, fo);
+    compute<FULL>(p, i, j, cls, f, fo);
     store(p, i, j, fo);
 }
 
-struct Physics {
+// FULL: the node paths include the optional per-node work (field statistics, macroscopic
+// output, body force), each behind its run-time switch.  The lean instantiation leaves it
+// out; the launchers pick it when all three are off, which keeps the registers and the
+// branches of that work out of the common step.
+template <bool FULL>
+struct PhysicsT {
     using P = StepParams<double>;
     using T = double;
     static __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const T f[Q], T fo[Q]) {
-        fp64::compute(p, i, j, cls, f, fo);
+        fp64::compute<FULL>(p, i, j, cls, f, fo);
     }
     static __device__ __forceinline__ void finish(const P& p, int i, int j, int cls, const T f[Q]) {
-        fp64::finish(p, i, j, cls, f);
+        fp64::finish<FULL>(p, i, j, cls, f);
     }
     static __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int cls) {
-        return fp64::edge_bulk_node(p, i, j, cls);
+        return fp64::edge_bulk_node<FULL>(p, i, j, cls);
     }
     static __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, T cc, T ss, T s2, T& ux, T& uy,
                                                         T& mx, T& my) {
@@ -444,9 +453,11 @@ struct Physics {
     static __device__ __forceinline__ void boundary_close(const P& p, const BTab<T>& tb, int li, int l, T ux2, T uy2,
                                                           T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
                                                           double& Fy) {
-        fp64::boundary_close(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
+        fp64::boundary_close<FULL>(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
 };
+using Physics = PhysicsT<true>;
+using PhysicsLean = PhysicsT<false>;
 
 }  // namespace fp64
 }  // namespace mrlbm

@@ -170,8 +170,8 @@ inline bool is_vec_cfg(int c) { return c >= VEC_CFG0 && c < PIPE_CFG0; }
 int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers);
 int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers);
 // Halo-face columns of an x-slab ahead of its step (face_kernel, step_common.cuh).
-int launch_face_f64(const StepParams<double>& p, void* stream);
-int launch_face_f32(const StepParams<float>& p, void* stream);
+int launch_face_f64(const StepParams<double>& p, bool full, void* stream);
+int launch_face_f32(const StepParams<float>& p, bool full, void* stream);
 // Persistent CTAs one SM holds for a TMA shape (0 when the shape does not fit).
 int tma_ctas_per_sm(int precision, int tile_cfg);
 // Bytes of one tensor-map box row and rows per box for a TMA shape.

@@ -128,3 +128,27 @@ def test_fp32_surface_pressure_tracks_fp64(mrlbm):
     assert np.abs(ps32 - ps64).max() < 1e-6          # p ~ 1/3; deviations ~1e-4
     assert np.abs(pf32 - pf64).max() < 1e-6
     assert np.abs(pr32 - pr64).max() < 1e-6
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("tile", [0, 17, 22, 27])
+def test_optional_outputs_leave_the_populations_unchanged(mrlbm, prec, tile):
+    """With field statistics and macroscopic output the kernels run their full instantiation,
+    without them the lean one; the populations must not depend on which ran."""
+    cfg = CASES["benchmark_small_400x100"]()
+    runs = []
+    for extras in (False, True):
+        s = mrlbm.Simulation(cfg, precision=prec)
+        try:
+            s.tile_config = tile
+        except mrlbm.MrlbmError:
+            s.close()
+            pytest.skip("shape does not fit this precision")
+        if extras:
+            s.field_stats_window(1, 10 ** 6)
+        for _ in range(5):
+            s.step(4, macro=extras)
+        runs.append(s.get_state())
+        assert s.status() == 0
+        s.close()
+    assert np.array_equal(runs[0], runs[1])
