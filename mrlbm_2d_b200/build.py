@@ -60,20 +60,24 @@ def build(force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc)), "include")
-    objs = []
+    # every translation unit is compiled in its own process, all at once
+    objs, cmds = [], []
     for src, extra in CU_UNITS.items():
         obj = os.path.join(BUILD, src + ".o")
         cmd = [nvcc] + NVCC_COMMON + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
     for src in CPP_UNITS:
         obj = os.path.join(BUILD, src + ".o")
-        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
-               "-I" + cuda_inc, "-c", os.path.join(CSRC, src), "-o", obj]
-        subprocess.run(cmd, check=True)
+        cmds.append(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+                     "-I" + cuda_inc, "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    procs = [subprocess.Popen(c) for c in cmds]
+    failed = [c for c, pr in zip(cmds, procs) if pr.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     tmp = OUT + ".tmp"
     subprocess.run([nvcc] + ARCH + ["-shared", "-o", tmp] + objs, check=True)
     os.replace(tmp, OUT)
