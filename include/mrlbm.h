@@ -61,7 +61,8 @@ extern "C" {
  * Run configuration.  The first block mirrors the reference namelists
  * DomainSize, Cylinder, Numbers, Parallel, Controls and LogicalControls
  * (2d_mrlbm.f90:2227-2233, input.dat:1-45); the last block holds the extensions
- * a BASELINE-style case needs.  Field order is part of the ABI.
+ * the benchmark-suite cylinder cases need (explicit centre, free-slip walls, seeded noise
+ * start).  Field order is part of the ABI.
  */
 typedef struct mrlbm_config {
     double   x_c, y_c, r_c;          /* cylinder centre / classification radius (lattice units, node (i,j) sits at (i,j)) */

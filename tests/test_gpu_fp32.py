@@ -1,7 +1,7 @@
 """FP32 deviation-form step against the FP64 step (same case, same seeded start).
 
 Short horizons only (the long-horizon Cd / Cl_rms / St comparison is
-`python -m mrlbm_2d_b200.precision_study`, reported in DESIGN.md).  Tolerances: the FP32
+`python -m mrlbm_2d_b200.precision_study`).  Tolerances: the FP32
 form keeps only small quantities in FP32, so after 2000 steps of the 400 x 100 benchmark case
 the velocity field agrees to 5e-5 U (max), density and populations to 1e-5 absolute
 (observed 2e-6) and the per-step drag to 1e-5 relative."""
