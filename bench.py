@@ -329,10 +329,12 @@ def main():
         sim.tile_config = best
         return best
 
-    def time_device(precision, K, W, case_cfg=None, soak_s=1.0):
+    def time_device(precision, K, W, case_cfg=None, soak_s=1.0, fields=False):
         c = case_cfg or cfg
         sim = m.Simulation(c, precision=precision, device=dev)
         sim.set_stream(stream.cuda_stream)
+        if fields:                           # FP64 mean/rms sums of u, v, p in every step
+            sim.field_stats_window(1, 2 ** 30)
         sim.step(W)
         tile = pick_tile(sim, flushed=case_cfg is None)
         # untimed soak so clock samples see the steady state
@@ -426,6 +428,15 @@ def main():
             large[prec] = {"ms_per_step": ms, "mlups": lnodes / (ms * 1e-3) / 1e6, "tile_shape": ltile,
                            "hbm_gbs_alg": BYTES_PER_LU[prec] * lnodes / (ms * 1e-3) / 1e9,
                            "ms_per_step_unflushed": nf, "window": lwin}
+            # the same with the field statistics on: six FP64 running sums read and written per
+            # node and step on top of the populations (+96 B per lattice update)
+            t, _, _, nf, lwin, ltile = time_device(prec, args.large_steps, 3, case_cfg=lcfg, soak_s=0.3, fields=True)
+            ms = t / args.large_steps
+            bpl = BYTES_PER_LU[prec] + 96
+            large[prec]["with_field_statistics"] = {
+                "ms_per_step": ms, "mlups": lnodes / (ms * 1e-3) / 1e6, "tile_shape": ltile,
+                "bytes_per_lu": bpl, "hbm_gbs_alg": bpl * lnodes / (ms * 1e-3) / 1e9,
+                "ms_per_step_unflushed": nf, "window": lwin}
     if sampler:
         time.sleep(0.3)
         sampler.stop()
@@ -469,12 +480,17 @@ def main():
             v = dict(v)
             v.pop("window")
             v["frac"] = v["hbm_gbs_alg"] / peak
+            fs = dict(v.pop("with_field_statistics"))
+            fs.pop("window")
+            fs["frac"] = fs["hbm_gbs_alg"] / peak
+            v["with_field_statistics"] = fs
             rl[f"fp{prec}"] = v
         if 32 in large and 64 in large:
             rl["fp32_over_fp64"] = large[64]["ms_per_step"] / large[32]["ms_per_step"]
         line["roofline_large"] = rl
     if sampler:
-        wins = [r[4] for r in results.values()] + [v["window"] for v in large.values()]
+        wins = [r[4] for r in results.values()] + [v["window"] for v in large.values()] + \
+               [v["with_field_statistics"]["window"] for v in large.values()]
         t0 = min(w[0] for w in wins) - 1.2
         t1 = max(w[1] for w in wins)
         line["clocks"] = sampler.summary(t0, t1)
