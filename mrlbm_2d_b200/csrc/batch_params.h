@@ -34,6 +34,7 @@ struct BatchArgs {
     const BatchCase* cases;
     const int* aux_off;            // [ncases + 1] prefix sums of aux items
     const int* tile_off;           // [ncases + 1] prefix sums of bulk tiles
+    const int* item_case;          // [aux items + bulk tiles] case of each work item
     BatchBarrier* bar;
     int ncases;
     int nsteps;                    // steps this launch advances (persistent schedule)

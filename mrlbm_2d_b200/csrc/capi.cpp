@@ -1552,6 +1552,9 @@ struct mrlbm_batch {
     void* d_params = nullptr;          // ncases x StepParams<T>
     BatchCase* d_cases = nullptr;
     int* d_off = nullptr;              // aux_off[n + 1], tile_off[n + 1]
+    int* d_item_case = nullptr;        // case of each work item, for tile shape item_case_cfg
+    size_t item_case_cap = 0;
+    int item_case_cfg = -1;
     BatchBarrier* d_bar = nullptr;
     unsigned char* h_stage[2] = {nullptr, nullptr};   // pinned upload staging, double-buffered
     cudaEvent_t staged[2] = {nullptr, nullptr};
@@ -1672,6 +1675,23 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
     b->stage_i ^= 1;
     const int* off = reinterpret_cast<const int*>(b->h_stage[si] + pb + cb);
     const int items = off[n] + off[2 * n + 1];
+    if (b->item_case_cfg != b->tile_cfg) {             // the item -> case table of this shape
+        std::vector<int> tab((size_t)items);
+        for (int c = 0; c < n; ++c) {
+            for (int k = off[c]; k < off[c + 1]; ++k) tab[(size_t)k] = c;
+            for (int k = off[n + 1 + c]; k < off[n + 2 + c]; ++k) tab[(size_t)(off[n] + k)] = c;
+        }
+        BCK(cudaStreamSynchronize(b->stream));
+        if (b->item_case_cap < (size_t)items) {
+            if (b->d_item_case) cudaFree(b->d_item_case);
+            b->d_item_case = nullptr;
+            b->item_case_cap = 0;
+            BCK(cudaMalloc((void**)&b->d_item_case, sizeof(int) * (size_t)items));
+            b->item_case_cap = (size_t)items;
+        }
+        BCK(cudaMemcpy(b->d_item_case, tab.data(), sizeof(int) * (size_t)items, cudaMemcpyHostToDevice));
+        b->item_case_cfg = b->tile_cfg;
+    }
 
     // the full kernel instantiation when any case has field statistics or a body force in this
     // call, or macroscopic output is asked for; the lean one otherwise
@@ -1687,6 +1707,7 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
         a.cases = b->d_cases;
         a.aux_off = b->d_off;
         a.tile_off = b->d_off + n + 1;
+        a.item_case = b->d_item_case;
         a.bar = b->d_bar;
         a.ncases = n;
         a.call_steps = steps;
@@ -1756,7 +1777,7 @@ void batch_free(mrlbm_batch* b) {
         free_all(h);
         delete h;
     }
-    for (void* q : {(void*)b->d_params, (void*)b->d_cases, (void*)b->d_off, (void*)b->d_bar})
+    for (void* q : {(void*)b->d_params, (void*)b->d_cases, (void*)b->d_off, (void*)b->d_bar, (void*)b->d_item_case})
         if (q) cudaFree(q);
     for (int i = 0; i < 2; ++i) {
         if (b->h_stage[i]) cudaFreeHost(b->h_stage[i]);

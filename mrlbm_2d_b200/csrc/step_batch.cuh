@@ -1,7 +1,8 @@
 // step_batch.cuh -- many independent cylinder cases advanced by one kernel.
 //
 // Work items of one step, over all cases: first every case's boundary and edge blocks
-// (aux items), then every case's bulk tiles of the 128-bit vector shape (step_common.cuh).
+// (aux items), then every case's bulk tiles of the 128-bit vector shape (step_common.cuh); a
+// table gives the case of each item.
 // A block copies the item's case parameters to shared memory, sets the per-step fields
 // (time level, iteration, statistics flags, force-record slot) and runs the same device
 // functions as the single-case kernels, so each case steps exactly as it would alone.
@@ -22,16 +23,6 @@
 namespace mrlbm {
 
 constexpr unsigned BAR_SPIN_LIMIT = 1u << 24;
-
-__device__ __forceinline__ int batch_find(const int* off, int n, int item) {
-    int lo = 0, hi = n;                                  // off[lo] <= item < off[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= item) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
 
 // Stats steps (post_process and statsbegin <= it <= statsend) among iterations a..b.
 __device__ __forceinline__ int batch_stats_count(const BatchCase& c, int a, int b) {
@@ -85,15 +76,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
         const int cs = a.step0 + s;                     // step index within the call
         for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
             const bool aux = item < n_aux;
-            const int c = aux ? batch_find(a.aux_off, a.ncases, item) : batch_find(a.tile_off, a.ncases, item - n_aux);
+            const int c = __ldg(a.item_case + item);
+            const int local = aux ? item - __ldg(a.aux_off + c) : item - n_aux - __ldg(a.tile_off + c);
             {   // case parameters -> shared memory, 16 bytes per thread
                 const uint4* src = reinterpret_cast<const uint4*>(a.params + c);
                 uint4* dst = reinterpret_cast<uint4*>(sp_raw);
                 for (int q = threadIdx.x; q < (int)(sizeof(P) / 16); q += blockDim.x) dst[q] = src[q];
             }
+            BatchCase bc;                                   // thread 0: loaded alongside the copy
+            if (threadIdx.x == 0) bc = a.cases[c];
             __syncthreads();
             if (threadIdx.x == 0) {
-                const BatchCase& bc = a.cases[c];
                 const int iter = bc.iter0 + cs + 1;
                 if (cs & 1) {                           // params hold the call's first time level
                     const T* t = sp.src;
@@ -114,8 +107,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
                 }
             }
             __syncthreads();
-            if (aux) aux_item<Phys>(sp, smem, item - __ldg(a.aux_off + c));
-            else vec_tile<Phys, WARPS, NJ>(sp, item - n_aux - __ldg(a.tile_off + c));
+            if (aux) aux_item<Phys>(sp, smem, local);
+            else vec_tile<Phys, WARPS, NJ>(sp, local);
             __syncthreads();
         }
         if (a.nsteps > 1 && !batch_barrier(a.bar)) return;
