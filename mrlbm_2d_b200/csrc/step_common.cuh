@@ -13,6 +13,33 @@
 
 namespace mrlbm {
 
+// Programmatic dependent launch.  The step kernels are launched with programmatic stream
+// serialization.  Each block first waits for the previous kernel on the stream to complete
+// and its writes to be visible (griddepcontrol.wait; at once when there is none), then allows
+// the next kernel to launch (griddepcontrol.launch_dependents): once every block of this grid
+// is running, the next step's blocks are dispatched onto the SM slots this grid frees and
+// wait there, so its launch overlaps this step's tail.  Nothing a step reads or writes is
+// touched before the wait.
+__device__ __forceinline__ void wait_prior_grid() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class K, class P>
+inline cudaError_t launch_after_prior(K kernel, unsigned grid, unsigned block, size_t smem, cudaStream_t s, const P& p) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, p);
+}
+
 // Columns 1 and nx are domain edges unless the lattice is one x-slab of a larger domain and
 // the neighbouring slab supplies that side's incoming populations in column 0 / nx+1.
 template <class T>
@@ -398,6 +425,7 @@ __device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, i
 template <class Phys, int BX, int BY, int NJ, int MINB>
 __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
+    wait_prior_grid();
     if (run_aux_block<Phys>(p)) return;
     const int t = blockIdx.x - p.nbblk - p.neblk;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
@@ -534,6 +562,7 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
 
 template <class Phys, int WARPS, int NJ, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
+    wait_prior_grid();
     if (run_aux_block<Phys>(p)) return;
     vec_tile<Phys, WARPS, NJ>(p, (int)blockIdx.x - p.nbblk - p.neblk);
 }
@@ -550,8 +579,8 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
     p.tiles_x = (p.L.nx + 32 * VW - 1) / (32 * VW);
     const int tiles_y = (p.L.ny + WARPS * NJ - 1) / (WARPS * NJ);
     const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
-    step_kernel_vec<Phys, WARPS, NJ, MINB><<<(unsigned)nblocks, nthr, 0, s>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_after_prior(step_kernel_vec<Phys, WARPS, NJ, MINB>, (unsigned)nblocks, nthr, 0, s, p) == cudaSuccess ? 0
+                                                                                                            : -1;
 }
 
 // ---- persistent software-pipelined bulk path -------------------------------------------------
@@ -563,6 +592,7 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
 template <class Phys, int B, int MINB>
 __global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
+    wait_prior_grid();
     if (run_aux_block<Phys>(p)) return;
     const int nx = p.L.nx, ny = p.L.ny, tiles_x = p.tiles_x;
     const int units = tiles_x * ny;
@@ -614,8 +644,9 @@ int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
     p.tiles_x = (p.L.nx + B - 1) / B;
     const long long units = (long long)p.tiles_x * p.L.ny;
     const long long G = std::min<long long>(units, (long long)sms[dev] * per_sm[dev]);
-    step_kernel_pipe<Phys, B, MINB><<<(unsigned)(p.nbblk + p.neblk + G), B, 0, s>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_after_prior(step_kernel_pipe<Phys, B, MINB>, (unsigned)(p.nbblk + p.neblk + G), B, 0, s, p) == cudaSuccess
+               ? 0
+               : -1;
 }
 
 // Halo faces of an x-slab, ahead of the step: one thread per node of column 1 (left halo
@@ -628,6 +659,7 @@ int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
 template <class Phys>
 __global__ void __launch_bounds__(128) face_kernel(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
+    wait_prior_grid();
     const int ny = p.L.ny;
     const int n = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     if (n >= 2 * ny) return;
@@ -648,8 +680,7 @@ __global__ void __launch_bounds__(128) face_kernel(const __grid_constant__ typen
 template <class Phys>
 int launch_face(const typename Phys::P& p, cudaStream_t s) {
     const int n = 2 * p.L.ny;
-    face_kernel<Phys><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_after_prior(face_kernel<Phys>, (unsigned)((n + 127) / 128), 128, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 
 template <class Phys, int BX, int BY, int NJ, int MINB>
@@ -662,8 +693,7 @@ int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
     const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
-    step_kernel<Phys, BX, BY, NJ, MINB><<<(unsigned)nblocks, nthr, 0, s>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_after_prior(step_kernel<Phys, BX, BY, NJ, MINB>, (unsigned)nblocks, nthr, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace mrlbm

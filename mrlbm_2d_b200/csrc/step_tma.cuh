@@ -201,6 +201,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
 
 template <class Phys, int BX, int BY, int STAGES, bool STORE>
 __global__ void __launch_bounds__(BX, 1) step_kernel_tma(const __grid_constant__ typename Phys::P p) {
+    wait_prior_grid();
     if (run_aux_block<Phys>(p)) return;
     tma_bulk_worker<Phys, BX, BY, STAGES, STORE>(p);
 }
@@ -231,8 +232,10 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
             return -1;
         if (dev < 64) attr_set |= 1ull << dev;
     }
-    step_kernel_tma<Phys, BX, BY, STAGES, STORE><<<(unsigned)(p.nbblk + p.neblk + workers), nthr, smem, s>>>(p);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_after_prior(step_kernel_tma<Phys, BX, BY, STAGES, STORE>, (unsigned)(p.nbblk + p.neblk + workers),
+                              nthr, (size_t)smem, s, p) == cudaSuccess
+               ? 0
+               : -1;
 }
 
 // Resident CTAs per SM of a TMA kernel with `smem` dynamic bytes: 0 when the shape does not
