@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
     __shared__ __align__(64) unsigned char sp_raw[sizeof(P)];
     __shared__ __align__(16) unsigned char smem[aux_smem_bytes<T>()];
     P& sp = *reinterpret_cast<P*>(sp_raw);
+    wait_prior_grid();                                   // per-step launches: see step_common.cuh
     const int n_aux = __ldg(a.aux_off + a.ncases);
     const int n_items = n_aux + __ldg(a.tile_off + a.ncases);
     for (int s = 0; s < a.nsteps; ++s) {
@@ -120,10 +121,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
 template <class Phys, int WARPS, int NJ, int MINB>
 int launch_step_batch(const BatchArgs<typename Phys::T>& a, int grid, bool cooperative, cudaStream_t s) {
     auto k = step_kernel_batch<Phys, WARPS, NJ, MINB>;
-    if (!cooperative) {
-        k<<<(unsigned)grid, WARPS * 32, 0, s>>>(a);
-        return cudaGetLastError() == cudaSuccess ? 0 : -1;
-    }
+    if (!cooperative) return launch_after_prior(k, (unsigned)grid, WARPS * 32, 0, s, a) == cudaSuccess ? 0 : -1;
     void* args[] = {(void*)&a};
     return cudaLaunchCooperativeKernel((const void*)k, dim3((unsigned)grid), dim3(WARPS * 32), args, 0, s) ==
                    cudaSuccess
