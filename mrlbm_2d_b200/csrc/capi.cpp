@@ -203,9 +203,8 @@ int upload_state(mrlbm_handle* h, const double* f) {
         const double v = f[(size_t)(e.i - 1) + (size_t)h->L.nx * (e.j - 1) + N * e.k];
         e.v = h->precision == MRLBM_FP64 ? v : (double)(float)(v - h->lat.w[e.k]);
     }
-    if (!h->ovr.empty()) {
-        if (h->d_ovr) cudaFree(h->d_ovr);
-        CK(cudaMalloc((void**)&h->d_ovr, h->ovr.size() * sizeof(OvrEntry)));
+    if (!h->ovr.empty()) {                // at most the 4 x 9 corner slots; allocated once
+        if (!h->d_ovr) CK(cudaMalloc((void**)&h->d_ovr, 4 * Q * sizeof(OvrEntry)));
         CK(cudaMemcpyAsync(h->d_ovr, h->ovr.data(), h->ovr.size() * sizeof(OvrEntry), cudaMemcpyHostToDevice,
                            h->stream));
     }
