@@ -307,6 +307,9 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
         const int f = idx / bn, n = idx - f * bn;
         sgi[idx] = (l0 + n < p.nb) ? p.bint[f * p.nb + l0 + n] : 0;
     }
+    // The tables are written once, when the handle is created, so the staging above may run
+    // while the previous step finishes; everything below reads or writes what steps change.
+    wait_prior_grid();
     __syncthreads();
     const BTab<T> tb{sg, sgi, bn};
     const int li = tid / BLANES, lane = tid % BLANES;
@@ -425,7 +428,7 @@ __device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, i
 template <class Phys, int BX, int BY, int NJ, int MINB>
 __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
-    wait_prior_grid();
+    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
     if (run_aux_block<Phys>(p)) return;
     const int t = blockIdx.x - p.nbblk - p.neblk;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
@@ -562,7 +565,7 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
 
 template <class Phys, int WARPS, int NJ, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
-    wait_prior_grid();
+    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
     if (run_aux_block<Phys>(p)) return;
     vec_tile<Phys, WARPS, NJ>(p, (int)blockIdx.x - p.nbblk - p.neblk);
 }
@@ -592,7 +595,7 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
 template <class Phys, int B, int MINB>
 __global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
-    wait_prior_grid();
+    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
     if (run_aux_block<Phys>(p)) return;
     const int nx = p.L.nx, ny = p.L.ny, tiles_x = p.tiles_x;
     const int units = tiles_x * ny;

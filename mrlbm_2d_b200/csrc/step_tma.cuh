@@ -201,7 +201,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
 
 template <class Phys, int BX, int BY, int STAGES, bool STORE>
 __global__ void __launch_bounds__(BX, 1) step_kernel_tma(const __grid_constant__ typename Phys::P p) {
-    wait_prior_grid();
+    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
     if (run_aux_block<Phys>(p)) return;
     tma_bulk_worker<Phys, BX, BY, STAGES, STORE>(p);
 }
