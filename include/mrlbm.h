@@ -294,7 +294,11 @@ int mrlbm_set_body_force(mrlbm_handle* h, const double* g);
  * the adjoint kernels step by step.  Either gradient pointer may be NULL; both NULL computes J
  * only.  Handles with inlet/outlet columns, free-slip or y-periodic walls and the rotated strong
  * closure (the defaults); MRLBM_EUNSUPPORTED otherwise.  On an FP32 handle the trajectory is the
- * FP32 step's (checkpoints in FP32) and the adjoint arithmetic is FP64. */
+ * FP32 step's (checkpoints in FP32) and the adjoint arithmetic is FP64.  The device workspace
+ * (nsteps / checkpoint_every + 2 x checkpoint_every population levels, two FP64 adjoint levels)
+ * is allocated by the first call, grown when a later call needs more, and kept until
+ * mrlbm_destroy; the backward pass recomputes the next segment on a second stream while the
+ * adjoint kernels sweep the current one. */
 int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t window, int32_t checkpoint_every, double* J,
                        double* grad_body, double* grad_uin);
 

@@ -193,9 +193,16 @@ __device__ __forceinline__ void stencil_quad(const P& p, int l, int s, const S f
 // interpolation at reference points 2 and 3, extrapolation to the node, rotated strong
 // closure, collision (2d_mrlbm.f90:294-311, 768-928, 1635-1765, 407-457) and the node's drag
 // term (2d_mrlbm.f90:558-591).
+// The eight stencil nodes' u, v and rotated moments come as plain values (qd[kind][t]); the
+// one stencil node s whose inputs carry the derivative (s < 0: none) comes as duals.  Each
+// operand is formed where it is used, so no per-thread array of stencil duals exists.
 template <class P, class S>
-__device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const S su[8], const S sv[8], const S smx[8],
-                                         const S smy[8], S fo[Q], S& drag) {
+__device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const double (*qd)[8], int s, S us, S vs,
+                                         S mxs, S mys, S fo[Q], S& drag) {
+    auto val = [&](int kind, int t) -> S {
+        if (t == s) return kind == 0 ? us : kind == 1 ? vs : kind == 2 ? mxs : mys;
+        return S(qd[kind][t]);
+    };
     S u[2], v[2], mx[2], my[2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
@@ -204,10 +211,10 @@ __device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const 
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr) {
             const int s0 = 4 * r + 2 * rr;
-            row_u[rr] = (1.0 - xd) * su[s0] + xd * su[s0 + 1];
-            row_v[rr] = (1.0 - xd) * sv[s0] + xd * sv[s0 + 1];
-            row_mx[rr] = (1.0 - xd) * smx[s0] + xd * smx[s0 + 1];
-            row_my[rr] = (1.0 - xd) * smy[s0] + xd * smy[s0 + 1];
+            row_u[rr] = (1.0 - xd) * val(0, s0) + xd * val(0, s0 + 1);
+            row_v[rr] = (1.0 - xd) * val(1, s0) + xd * val(1, s0 + 1);
+            row_mx[rr] = (1.0 - xd) * val(2, s0) + xd * val(2, s0 + 1);
+            row_my[rr] = (1.0 - xd) * val(3, s0) + xd * val(3, s0 + 1);
         }
         u[r] = (1.0 - yd) * row_u[0] + yd * row_u[1];
         v[r] = (1.0 - yd) * row_v[0] + yd * row_v[1];
@@ -418,24 +425,21 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
     }
     __syncthreads();
     if (q >= 81) return;
-    Dual f[Q], su[8], sv[8], smx[8], smy[8];
+    Dual f[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) f[k] = Dual(in[k], q == k ? 1.0 : 0.0);
-#pragma unroll
-    for (int s = 0; s < 8; ++s) { su[s] = qd[0][s]; sv[s] = qd[1][s]; smx[s] = qd[2][s]; smy[s] = qd[3][s]; }
+    int s = -1;                                          // the stencil node input q belongs to
+    Dual us(0.0), vs(0.0), mxs(0.0), mys(0.0);
     if (q >= 9) {
-        const int s = (q - 9) / Q, kk = (q - 9) % Q;
+        s = (q - 9) / Q;
+        const int kk = (q - 9) % Q;
         Dual g[Q];
 #pragma unroll
         for (int k = 0; k < Q; ++k) g[k] = Dual(in[9 + Q * s + k], k == kk ? 1.0 : 0.0);
-        Dual u, v, mx, my;
-        stencil_quad(p, l, s, g, u, v, mx, my);
-        // only stencil s depends on input q
-        for (int t = 0; t < 8; ++t)
-            if (t == s) { su[t] = u; sv[t] = v; smx[t] = mx; smy[t] = my; }
+        stencil_quad(p, l, s, g, us, vs, mxs, mys);    // only stencil s depends on input q
     }
     Dual fo[Q], drag;
-    wall_map(p, l, f, su, sv, smx, smy, fo, drag);
+    wall_map(p, l, f, qd, s, us, vs, mxs, mys, fo, drag);
     double c = a.wJ * drag.d;
 #pragma unroll
     for (int k = 0; k < Q; ++k) c += lam[k] * fo[k].d;
@@ -445,7 +449,8 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
 // One adjoint step in one launch of 128-thread blocks: [nb wall blocks][edge blocks, 7 nodes
 // x 18 inputs each][bulk blocks, 128 nodes each].
 template <class P>
-__global__ void __launch_bounds__(128) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(128, 4) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    wait_prior_grid();                                  // launched like the step kernels (step_common.cuh)
     const int b = (int)blockIdx.x;
     const int n_edge_blk = (a.n_edge + 6) / 7;
     if (b < p.nb) {

@@ -85,6 +85,8 @@ struct mrlbm_handle {
     std::vector<OvrEntry> ovr;                // loaded-state overrides (see OvrEntry)
     bool ovr_live = false;                    // true until the first step after a load
     OvrEntry* d_ovr = nullptr;
+    void* adj_ws = nullptr;                   // adjoint workspace, kept between mrlbm_adjoint_drag calls
+    size_t adj_ws_bytes = 0;
     double* d_fstage = nullptr;               // f(nx,ny,0:8) staging for state transfers
     // TMA shapes: tensor maps of both time levels, tile-claim counter, persistent CTAs
     unsigned long long* d_tile_ctr = nullptr;
@@ -450,7 +452,7 @@ void free_all(mrlbm_handle* h) {
     if (h->host_only) return;
     cudaSetDevice(h->device);
     for (void* p : {h->buf[0], h->buf[1], h->d_bgeo, (void*)h->d_bint, (void*)h->d_boxmap, (void*)h->d_partials,
-                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, h->d_body, (void*)h->d_ovr, (void*)h->d_fstage,
+                    (void*)h->d_counter, (void*)h->d_ring, (void*)h->d_err, (void*)h->d_macro, (void*)h->d_uin, h->d_body, (void*)h->d_ovr, h->adj_ws, (void*)h->d_fstage,
                     (void*)h->d_tile_ctr, (void*)h->d_fstat, (void*)h->d_fstat_out, (void*)h->d_quad, (void*)h->d_W,
                     (void*)h->d_sumw, (void*)h->d_sring, (void*)h->d_pring, (void*)h->d_sidx})
         if (p) cudaFree(p);
@@ -1390,7 +1392,7 @@ namespace {
 
 // One forward step from src into dst at iteration `iter` (drag record into rec if given).
 template <class T>
-int adj_forward(mrlbm_handle* h, const void* src, void* dst, int iter, double* rec, bool ovr, int tile) {
+int adj_forward(mrlbm_handle* h, const void* src, void* dst, int iter, double* rec, bool ovr, int tile, cudaStream_t st) {
     StepParams<T> p{};
     fill_common(h, p);
     const mrlbm_config& c = h->cfg;
@@ -1405,8 +1407,8 @@ int adj_forward(mrlbm_handle* h, const void* src, void* dst, int iter, double* r
     p.rec = rec;
     p.iter = iter;
     ++h->launches;
-    if (sizeof(T) == 8) return launch_step_f64(reinterpret_cast<const StepParams<double>&>(p), tile, h->stream, 0);
-    return launch_step_f32(reinterpret_cast<const StepParams<float>&>(p), tile, h->stream, 0);
+    if (sizeof(T) == 8) return launch_step_f64(reinterpret_cast<const StepParams<double>&>(p), tile, st, 0);
+    return launch_step_f32(reinterpret_cast<const StepParams<float>&>(p), tile, st, 0);
 }
 
 template <class T>
@@ -1447,47 +1449,63 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     const int64_t nodes = (int64_t)h->L.nx * h->L.ny;
     const int tile = is_tma_cfg(h->tile_cfg) ? 1 : h->tile_cfg;
     const bool grads = grad_body || grad_uin;
-    std::vector<void*> cp(ncp, nullptr), seg(grads ? K : 0, nullptr);
+    std::vector<void*> cp(ncp, nullptr), seg(grads ? K : 0, nullptr), seg2(grads ? K : 0, nullptr);
     void* work[2] = {nullptr, nullptr};
     double *lam[2] = {nullptr, nullptr}, *d_rec = nullptr, *gb = nullptr, *gu = nullptr;
-    auto release = [&]() {
-        for (void* q : cp) if (q) cudaFree(q);
-        for (size_t q = 1; q < seg.size(); ++q) if (seg[q]) cudaFree(seg[q]);   // seg[0] borrows a checkpoint
-        for (void* q : {work[0], work[1], (void*)lam[0], (void*)lam[1], (void*)d_rec, (void*)gb, (void*)gu}) if (q) cudaFree(q);
-    };
-    auto alloc_level = [&](void** q) {
-        if (cudaMalloc(q, LB) != cudaSuccess) return false;
+    // One workspace for the checkpoints, two sets of segment levels (one replayed, one being
+    // recomputed), two working levels, the drag records and the adjoint fields, kept with the
+    // handle so repeated calls (a gradient loop) allocate nothing; it grows when a call needs more.
+    const auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t n_levels = (size_t)ncp + (seg.empty() ? 0 : 2 * (seg.size() - 1)) + 2;
+    const size_t ws = n_levels * al(LB) + al((size_t)N * REC_WORDS * sizeof(double)) +
+                      (grads ? 2 * al(LAM) + al((size_t)2 * nodes * sizeof(double)) + al((size_t)h->L.ny * sizeof(double)) : 0);
+    if (h->adj_ws_bytes < ws) {
+        if (h->adj_ws) cudaFree(h->adj_ws);
+        h->adj_ws = nullptr;
+        h->adj_ws_bytes = 0;
+        if (cudaMalloc(&h->adj_ws, ws) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(h, MRLBM_ECUDA, "adjoint: device memory for checkpoints and adjoint fields");
+        }
+        h->adj_ws_bytes = ws;
+    }
+    char* wp = (char*)h->adj_ws;
+    auto carve = [&](size_t b) { void* q = wp; wp += al(b); return q; };
+    bool ok = true;
+    auto level = [&](void** q) {
+        *q = carve(LB);
         // every level carries the never-written ghost values of the current state
         return cudaMemcpyAsync(*q, h->buf[h->cur], LB, cudaMemcpyDeviceToDevice, h->stream) == cudaSuccess;
     };
-    bool ok = true;
-    for (int q = 0; q < ncp && ok; ++q) ok = alloc_level(&cp[q]);
-    for (int q = 1; q < (int)seg.size() && ok; ++q) ok = alloc_level(&seg[q]);
-    ok = ok && alloc_level(&work[0]) && alloc_level(&work[1]) &&
-         cudaMalloc((void**)&d_rec, (size_t)N * REC_WORDS * sizeof(double)) == cudaSuccess;
-    if (ok && grads)
-        ok = cudaMalloc((void**)&lam[0], LAM) == cudaSuccess && cudaMalloc((void**)&lam[1], LAM) == cudaSuccess &&
-             cudaMalloc((void**)&gb, (size_t)2 * nodes * sizeof(double)) == cudaSuccess &&
-             cudaMalloc((void**)&gu, (size_t)h->L.ny * sizeof(double)) == cudaSuccess &&
-             cudaMemsetAsync(lam[0], 0, LAM, h->stream) == cudaSuccess &&
+    for (int q = 0; q < ncp && ok; ++q) ok = level(&cp[q]);
+    for (int q = 1; q < (int)seg.size() && ok; ++q) ok = level(&seg[q]) && level(&seg2[q]);   // [0] borrows a checkpoint
+    ok = ok && level(&work[0]) && level(&work[1]);
+    d_rec = (double*)carve((size_t)N * REC_WORDS * sizeof(double));
+    if (ok && grads) {
+        lam[0] = (double*)carve(LAM);
+        lam[1] = (double*)carve(LAM);
+        gb = (double*)carve((size_t)2 * nodes * sizeof(double));
+        gu = (double*)carve((size_t)h->L.ny * sizeof(double));
+        ok = cudaMemsetAsync(lam[0], 0, LAM, h->stream) == cudaSuccess &&
              cudaMemsetAsync(lam[1], 0, LAM, h->stream) == cudaSuccess &&
              cudaMemsetAsync(gb, 0, (size_t)2 * nodes * sizeof(double), h->stream) == cudaSuccess &&
              cudaMemsetAsync(gu, 0, (size_t)h->L.ny * sizeof(double), h->stream) == cudaSuccess;
+    }
+    auto release = [&]() {};                                       // the workspace stays with the handle
     if (!ok) {
-        release();
         cudaGetLastError();
-        return fail(h, MRLBM_ECUDA, "adjoint: device memory for checkpoints and adjoint fields");
+        return fail(h, MRLBM_ECUDA, "adjoint: initialising checkpoints and adjoint fields");
     }
     const int it0 = h->iter;
     // forward pass: F^0 .. F^N, checkpoint F^{cK}, drag records of the window
-    auto fwd = [&](const void* a, void* b, int it, double* rec, bool ovr) {
-        return fp64 ? adj_forward<double>(h, a, b, it, rec, ovr, tile) : adj_forward<float>(h, a, b, it, rec, ovr, tile);
+    auto fwd = [&](const void* a, void* b, int it, double* rec, bool ovr, cudaStream_t st) {
+        return fp64 ? adj_forward<double>(h, a, b, it, rec, ovr, tile, st) : adj_forward<float>(h, a, b, it, rec, ovr, tile, st);
     };
     const void* prev = cp[0];
     for (int n = 1; n <= N && rc == MRLBM_OK; ++n) {
         void* dst = work[n & 1];
         double* rec = n > N - T ? d_rec + (size_t)(n - 1) * REC_WORDS : nullptr;
-        if (fwd(prev, dst, it0 + n, rec, n == 1 && h->ovr_live) != 0) rc = MRLBM_ECUDA;
+        if (fwd(prev, dst, it0 + n, rec, n == 1 && h->ovr_live, h->stream) != 0) rc = MRLBM_ECUDA;
         if (n % K == 0 && n / K < ncp && cudaMemcpyAsync(cp[n / K], dst, LB, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
             rc = MRLBM_ECUDA;
         prev = dst;
@@ -1502,15 +1520,41 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
         for (int n = N - T + 1; n <= N; ++n) acc = acc + recs[(size_t)(n - 1) * REC_WORDS + 1];
         *J = acc / T;
     }
-    // backward pass, segment by segment from the last checkpoint
+    // Backward pass, segment by segment from the last checkpoint.  Segment c is recomputed from
+    // checkpoint c into one of two buffer sets on a second stream while the adjoint kernels
+    // sweep segment c + 1 from the other set on the handle's stream: a recompute waits for the
+    // sweep that last used its set, a sweep for the recompute of its segment.
+    std::vector<void*>* sets[2] = {&seg, &seg2};
+    cudaStream_t rs = nullptr;
+    cudaEvent_t rec_done[2] = {nullptr, nullptr}, adj_done[2] = {nullptr, nullptr};
+    if (grads && rc == MRLBM_OK) {
+        bool made = cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking) == cudaSuccess;
+        for (int q = 0; q < 2 && made; ++q)
+            made = cudaEventCreateWithFlags(&rec_done[q], cudaEventDisableTiming) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&adj_done[q], cudaEventDisableTiming) == cudaSuccess;
+        if (!made) rc = MRLBM_ECUDA;
+    }
+    auto recompute = [&](int cs, cudaStream_t st) {
+        std::vector<void*>& sg = *sets[cs & 1];
+        const int n0 = cs * K, m = std::min(K, N - n0);
+        sg[0] = cp[cs];
+        for (int t = 1; t < m; ++t)
+            if (fwd(sg[t - 1], sg[t], it0 + n0 + t, nullptr, n0 + t == 1 && h->ovr_live, st) != 0) return MRLBM_ECUDA;
+        return (int)MRLBM_OK;
+    };
+    if (grads && rc == MRLBM_OK) rc = recompute(ncp - 1, h->stream);
     int li = 0;
     for (int cseg = ncp - 1; grads && cseg >= 0 && rc == MRLBM_OK; --cseg) {
         const int n0 = cseg * K, m = std::min(K, N - n0);
-        seg[0] = cp[cseg];
-        for (int t = 1; t < m && rc == MRLBM_OK; ++t)
-            if (fwd(seg[t - 1], seg[t], it0 + n0 + t, nullptr, n0 + t == 1 && h->ovr_live) != 0) rc = MRLBM_ECUDA;
+        std::vector<void*>& sg = *sets[cseg & 1];
+        if (cseg >= 1) {                                   // the next segment, meanwhile
+            if (cseg + 1 <= ncp - 1) cudaStreamWaitEvent(rs, adj_done[(cseg + 1) & 1], 0);
+            rc = recompute(cseg - 1, rs);
+            if (rc == MRLBM_OK && cudaEventRecord(rec_done[(cseg - 1) & 1], rs) != cudaSuccess) rc = MRLBM_ECUDA;
+        }
+        if (cseg < ncp - 1) cudaStreamWaitEvent(h->stream, rec_done[cseg & 1], 0);
         for (int n = n0 + m; n > n0 && rc == MRLBM_OK; --n) {
-            const int t = n - n0 - 1;                  // seg[t] = F^{n-1}
+            const int t = n - n0 - 1;                  // sg[t] = F^{n-1}
             adj::AdjArgs a{};
             a.lam_in = lam[li];
             a.lam_out = lam[li ^ 1];
@@ -1519,10 +1563,11 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             a.wJ = n > N - T ? 1.0 / T : 0.0;
             a.n_edge = 2 * h->L.ny;
             const bool ovr = n == 1 && h->ovr_live;
-            if ((fp64 ? adj_backward<double>(h, seg[t], it0 + n, ovr, a) : adj_backward<float>(h, seg[t], it0 + n, ovr, a)) != 0)
+            if ((fp64 ? adj_backward<double>(h, sg[t], it0 + n, ovr, a) : adj_backward<float>(h, sg[t], it0 + n, ovr, a)) != 0)
                 rc = MRLBM_ECUDA;
             li ^= 1;
         }
+        if (rc == MRLBM_OK && cudaEventRecord(adj_done[cseg & 1], h->stream) != cudaSuccess) rc = MRLBM_ECUDA;
     }
     if (rc == MRLBM_OK && grads) {
         if (grad_body && cudaMemcpyAsync(grad_body, gb, (size_t)2 * nodes * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
@@ -1531,6 +1576,14 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             rc = MRLBM_ECUDA;
     }
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = MRLBM_ECUDA;
+    if (rs) {
+        if (cudaStreamSynchronize(rs) != cudaSuccess) rc = MRLBM_ECUDA;
+        cudaStreamDestroy(rs);
+    }
+    for (int q = 0; q < 2; ++q) {
+        if (rec_done[q]) cudaEventDestroy(rec_done[q]);
+        if (adj_done[q]) cudaEventDestroy(adj_done[q]);
+    }
     release();
     if (rc != MRLBM_OK) return fail(h, rc, std::string("adjoint: ") + cudaGetErrorString(cudaGetLastError()));
     return MRLBM_OK;

@@ -25,8 +25,8 @@ __device__ __forceinline__ void wait_prior_grid() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-template <class K, class P>
-inline cudaError_t launch_after_prior(K kernel, unsigned grid, unsigned block, size_t smem, cudaStream_t s, const P& p) {
+template <class K, class... A>
+inline cudaError_t launch_after_prior(K kernel, unsigned grid, unsigned block, size_t smem, cudaStream_t s, const A&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -37,7 +37,7 @@ inline cudaError_t launch_after_prior(K kernel, unsigned grid, unsigned block, s
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, p);
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 // Columns 1 and nx are domain edges unless the lattice is one x-slab of a larger domain and

@@ -96,8 +96,7 @@ template <class T>
 static int launch_adjoint(const StepParams<T>& p, const adj::AdjArgs& a, cudaStream_t s) {
     const int64_t nodes = (int64_t)p.L.nx * p.L.ny;
     const int64_t blocks = (int64_t)p.nb + (a.n_edge + 6) / 7 + (nodes + 127) / 128;
-    adj::adjoint_step<StepParams<T>><<<(unsigned)blocks, 128, 0, s>>>(p, a);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    return launch_after_prior(adj::adjoint_step<StepParams<T>>, (unsigned)blocks, 128, 0, s, p, a) == cudaSuccess ? 0 : -1;
 }
 
 int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s) { return launch_adjoint(p, a, s); }
