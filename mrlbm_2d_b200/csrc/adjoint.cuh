@@ -449,7 +449,7 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
 // One adjoint step in one launch of 128-thread blocks: [nb wall blocks][edge blocks, 7 nodes
 // x 18 inputs each][bulk blocks, 128 nodes each].
 template <class P>
-__global__ void __launch_bounds__(128, 4) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(128, 5) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
     wait_prior_grid();                                  // launched like the step kernels (step_common.cuh)
     const int b = (int)blockIdx.x;
     const int n_edge_blk = (a.n_edge + 6) / 7;
