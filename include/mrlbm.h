@@ -218,12 +218,17 @@ int mrlbm_cp_statistics(const double* p_surface, int32_t nstep, int32_t nbct,
  * the per-step records, the curved-wall tables) lives in fixed-size file-scope device arrays
  * of about 2 MB that every GPU loading this library holds until the process exits.  Limits:
  * at most 1024 curved-wall nodes, 8192 rows and a cylinder bounding box of at most 512 x 512
- * cells; larger cases are rejected with MRLBM_EINVAL.  The first call on a device looks up the
- * arrays' device addresses (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  All calls share the arrays and re-upload the case tables
- * and clear the counters each time, so calls that overlap on the GPU (other streams or
- * devices' threads using the same device) race; serialise them.  Allocates nothing: no
- * cudaMalloc, cudaFree or allocating library routine on any path. */
+ * cells; larger cases are rejected with MRLBM_EINVAL.  d_state must be 16-byte aligned (the
+ * vector tile shapes access it 16 bytes at a time) and d_f0 8-byte aligned; a misaligned
+ * pointer (a sub-allocation or a view at an odd offset) is rejected with MRLBM_EINVAL.  The
+ * first call on a device looks up the arrays' device addresses (cudaGetSymbolAddress) with
+ * that device current and caches them for the life of the process (they assume the device's
+ * primary context is not reset meanwhile); make that first call before any stream capture.
+ * Every call uploads the case tables from host memory and synchronises cuda_stream at its end,
+ * to read the device error flag and the step records.  All calls share the arrays and
+ * re-upload the case tables and clear the counters each time, so calls that overlap on the
+ * GPU (other streams or other host threads using the same device) race; serialise them.
+ * Allocates nothing: no cudaMalloc, cudaFree or allocating library routine on any path. */
 int mrlbm_step_noalloc(mrlbm_handle* h, void* d_state, const double* d_f0, int32_t nsteps,
                        double* records, int32_t* n_records, void* cuda_stream);
 
@@ -363,6 +368,12 @@ int mrlbm_batch_get_schedule(const mrlbm_batch* b, int32_t* tile_cfg, int32_t* s
 /* Time every vector shape under both schedules for trial_steps steps (states, counters and
  * histories restored afterwards) and keep the fastest; returns its time per batch step. */
 int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_per_step);
+/* Watchdog of the persistent schedule: how many times a block polls the grid barrier between
+ * two steps before it decides the launch has lost a block, raises MRLBM_EDEVICE_TIMEOUT and
+ * ends the launch (every other waiting block follows).  Each poll sleeps about 0.1 us; the
+ * default (polls = 0) is 2^24 polls, a few seconds.  A tiny limit makes a healthy launch give up
+ * (the timeout path is testable that way); the cases' states are then undefined. */
+int mrlbm_batch_set_wait_limit(mrlbm_batch* b, int64_t polls);
 /* Sticky status: a grid-barrier timeout (MRLBM_EDEVICE_TIMEOUT) or the first case's error. */
 int mrlbm_batch_status(mrlbm_batch* b);
 int mrlbm_batch_last_error(const mrlbm_batch* b, char* buf, size_t len);

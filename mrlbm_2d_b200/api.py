@@ -36,6 +36,7 @@ EXPORTED = [
     "mrlbm_batch_create", "mrlbm_batch_destroy", "mrlbm_batch_case", "mrlbm_batch_step",
     "mrlbm_batch_set_schedule", "mrlbm_batch_get_schedule", "mrlbm_batch_autotune", "mrlbm_batch_status",
     "mrlbm_batch_last_error", "mrlbm_batch_launch_count", "mrlbm_batch_get_stream",
+    "mrlbm_batch_set_wait_limit",
     "mrlbm_set_body_force", "mrlbm_adjoint_drag",
     "mrlbm_surface_enable", "mrlbm_get_probe_nodes", "mrlbm_get_surface",
     "mrlbm_create_slab", "mrlbm_halo_size", "mrlbm_halo_pack", "mrlbm_halo_unpack", "mrlbm_slabs_step",
@@ -110,6 +111,7 @@ def load_library(path=None):
         "mrlbm_batch_last_error": [vp, ctypes.c_char_p, ctypes.c_size_t],
         "mrlbm_batch_launch_count": [vp, vp],
         "mrlbm_batch_get_stream": [vp, vp],
+        "mrlbm_batch_set_wait_limit": [vp, ctypes.c_int64],
         "mrlbm_set_body_force": [vp, vp],
         "mrlbm_adjoint_drag": [vp, i32, i32, i32, vp, vp, vp],
         "mrlbm_surface_enable": [vp, i32],
@@ -521,6 +523,11 @@ class Batch:
 
     def status(self):
         return self._L.mrlbm_batch_status(self._b)
+
+    def set_wait_limit(self, polls):
+        """Grid-barrier polls (about 0.1 us each) before a block of the persistent schedule
+        gives up with MRLBM_EDEVICE_TIMEOUT; 0 restores the default."""
+        self._check(self._L.mrlbm_batch_set_wait_limit(self._b, int(polls)))
 
     def launch_count(self):
         n = ctypes.c_int64()

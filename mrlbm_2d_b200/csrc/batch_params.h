@@ -5,6 +5,7 @@
 namespace mrlbm {
 
 constexpr int ERR_BARRIER_TIMEOUT = 8;     // device flag bit: a grid-barrier wait gave up
+constexpr unsigned BAR_SPIN_LIMIT = 1u << 24;   // default grid-barrier polls (~0.1 us each)
 
 // Per-case, per-call values the kernel derives each step's flags from.
 struct BatchCase {
@@ -42,6 +43,7 @@ struct BatchArgs {
     int call_steps;                // steps of the whole call (macro output on the last)
     int want_macro;
     int full;                      // some case has field statistics, macroscopic output or a body force
+    unsigned spin_limit;           // polls a block waits at the grid barrier before it gives up
 };
 
 // Host-side launch entry points (step_f64.cu / step_f32.cu).  tile_cfg is a vector shape

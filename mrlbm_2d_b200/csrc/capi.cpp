@@ -1614,6 +1614,7 @@ struct mrlbm_batch {
     size_t stage_bytes = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_cfg = -1, graph_steps = 0, graph_macro = -1, graph_full = -1;
+    unsigned wait_limit = BAR_SPIN_LIMIT;   // grid-barrier polls before a block gives up
 };
 
 namespace {
@@ -1765,6 +1766,7 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
         a.call_steps = steps;
         a.want_macro = want_macro;
         a.full = full;
+        a.spin_limit = b->wait_limit;
     };
     setup(a64, (const StepParams<double>*)b->d_params);
     setup(a32, (const StepParams<float>*)b->d_params);
@@ -1907,6 +1909,12 @@ int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule,
     b->tile_cfg = tile_cfg;
     b->schedule = schedule;
     b->steps_per_launch = steps_per_launch;
+    return MRLBM_OK;
+}
+
+int mrlbm_batch_set_wait_limit(mrlbm_batch* b, int64_t polls) {
+    if (!b || polls < 0 || polls > 0xffffffffLL) return MRLBM_EINVAL;
+    b->wait_limit = polls == 0 ? BAR_SPIN_LIMIT : (unsigned)polls;
     return MRLBM_OK;
 }
 

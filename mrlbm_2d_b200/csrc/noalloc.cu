@@ -11,6 +11,7 @@
 // allocating library routine.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -60,7 +61,9 @@ static NaSymbols g_na[NA_MAX_DEVICES];
 static std::mutex g_na_mutex;
 
 // Device addresses of the arrays above for the current device.  Host code cannot use the
-// array names as device pointers: they are host-side stand-ins.  Looked up once per device.
+// array names as device pointers: they are host-side stand-ins.  Looked up once per device
+// and cached for the life of the process: the cache assumes the device's primary context
+// lives that long (a cudaDeviceReset would leave these addresses stale).
 static cudaError_t na_symbols(int dev, NaSymbols** out) {
     if (dev < 0 || dev >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_na_mutex);
@@ -99,6 +102,14 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
         return MRLBM_EINVAL;
     }
     if (!d_state) { err = "d_state is NULL"; return MRLBM_EINVAL; }
+    // the 128-bit vector shapes read and write d_state with 16-byte accesses; the initial
+    // populations are read as doubles
+    if ((uintptr_t)d_state % 16 != 0) { err = "d_state must be 16-byte aligned"; return MRLBM_EINVAL; }
+    if (d_f0 && (uintptr_t)d_f0 % 8 != 0) { err = "d_f0 must be 8-byte aligned"; return MRLBM_EINVAL; }
+    if (d_f0 && c.conflicts.size() > (size_t)NA_MAX_OVR) {
+        err = "too many loaded-state overrides (at most " + std::to_string(NA_MAX_OVR) + ")";
+        return MRLBM_EINVAL;
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     NaSymbols* S = nullptr;
@@ -129,8 +140,7 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
     if (d_f0) {
         e = launch_scatter_state(c.precision, d_f0, half[0], half[1], c.L, c.xper, c.yper, c.freeslip, c.w, st);
         if (e != cudaSuccess) { err = cudaGetErrorString(e); return MRLBM_ECUDA; }
-        n_ovr = (int)c.conflicts.size();
-        if (n_ovr > NA_MAX_OVR) { err = "too many loaded-state overrides"; return MRLBM_EINVAL; }
+        n_ovr = (int)c.conflicts.size();                      // checked against NA_MAX_OVR above
         if (n_ovr > 0) {
             e = cudaMemcpyAsync(S->ovr, c.conflicts.data(), (size_t)n_ovr * sizeof(OvrEntry), cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) { err = cudaGetErrorString(e); return MRLBM_ECUDA; }

@@ -14,15 +14,14 @@
 //     host captures in a CUDA graph and replays.
 // Per-call state (iteration, time level, force-ring position) is uploaded before each call,
 // so a captured graph replays correctly.  The grid barrier's wait is bounded: after
-// BAR_SPIN_LIMIT polls a block raises ERR_BARRIER_TIMEOUT, sets the abort flag that every
-// waiting block also polls, and the kernel returns.
+// BatchArgs::spin_limit polls (BAR_SPIN_LIMIT unless the host sets another limit) a block raises
+// ERR_BARRIER_TIMEOUT, sets the abort flag that every waiting block also polls, and the kernel
+// returns.
 #pragma once
 #include "batch_params.h"
 #include "step_common.cuh"
 
 namespace mrlbm {
-
-constexpr unsigned BAR_SPIN_LIMIT = 1u << 24;
 
 // Stats steps (post_process and statsbegin <= it <= statsend) among iterations a..b.
 __device__ __forceinline__ int batch_stats_count(const BatchCase& c, int a, int b) {
@@ -32,7 +31,9 @@ __device__ __forceinline__ int batch_stats_count(const BatchCase& c, int a, int 
 }
 
 // Bounded grid barrier of a cooperative launch (all blocks resident).  False after an abort.
-__device__ __forceinline__ bool batch_barrier(BatchBarrier* bar) {
+// A block that polls `limit` times without the generation moving raises ERR_BARRIER_TIMEOUT and
+// the abort flag, which every other waiting block polls too, so the launch ends.
+__device__ __forceinline__ bool batch_barrier(BatchBarrier* bar, unsigned limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -48,7 +49,7 @@ __device__ __forceinline__ bool batch_barrier(BatchBarrier* bar) {
         } else {
             for (unsigned it = 0; *gen == g; ++it) {
                 if (*abort) { ok = 0; break; }
-                if (it >= BAR_SPIN_LIMIT) {
+                if (it >= limit) {
                     atomicOr(&bar->err, ERR_BARRIER_TIMEOUT);
                     atomicExch(&bar->abort, 1);
                     ok = 0;
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
             else vec_tile<Phys, WARPS, NJ>(sp, local);
             __syncthreads();
         }
-        if (a.nsteps > 1 && !batch_barrier(a.bar)) return;
+        if (a.nsteps > 1 && !batch_barrier(a.bar, a.spin_limit)) return;
     }
 }
 

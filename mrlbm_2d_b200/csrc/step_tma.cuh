@@ -136,8 +136,11 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
         if (!__syncthreads_and(ok)) {
             if (tid == 0) {
                 atomicOr(p.errflag, ERR_TMA_TIMEOUT);
-                // let the copies still in flight land before the CTA's shared memory goes away
+                // let the copies still in flight land before the CTA's shared memory goes away:
+                // the loads of the other stages (bounded waits) and the tensor stores committed
+                // for earlier tiles, which still read the output tile
                 for (int r = 1; r < STAGES; ++r) (void)mbar_wait(&bars[(q + r) % STAGES], (unsigned)((q + r) / STAGES) & 1u);
+                if (STORE) bulk_wait_all();
             }
             __syncthreads();
             return;
