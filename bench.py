@@ -5,15 +5,22 @@ free-slip walls, seeded-noise start); one bench step = one lattice time step ove
 grid, forces reduced every step.  Synthetic, seeded inputs only.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision 32|64] [--case mid|large|small]
+                  [--precision 32|64] [--case mid|large|small] [--no-studies]
 
-`value` is the aggregate MLUPS of the headline precision (FP32 deviation form unless
---precision 64), each timed step preceded by an L2 flush outside its CUDA event pair (a
-256 MiB write, then a read of the same buffer, so L2 holds none of the state and the flush's
-own dirty lines are written back before the step starts); `e2e` is the same metric through the public C ABI with host buffers: upload the
-initial populations, K steps, drain the force history every 100 steps, read the last step's
-rho/ux/uy back.  Under torchrun every rank runs an independent replica (its own seed) on its
-own GPU: weak scaling, no collective on the data path; times are max over ranks.
+`value` is the aggregate MLUPS of the headline precision, FP64 (the reference's arithmetic;
+--precision 32 selects the FP32 deviation form), each timed step preceded by an L2 flush
+outside its CUDA event pair (a 256 MiB write, then a read of the same buffer, so L2 holds none
+of the state and the flush's own dirty lines are written back before the step starts); the
+FP32 form is timed the same way beside it (`fp32`).  `e2e` is the same metric through the
+public C ABI with host buffers, as a restart segment: upload the populations, max(K, 1000)
+steps, drain the force history every 100 steps, read the last step's rho/ux/uy back.  The
+rest of the benchmark metric is measured in the same run: `precision` (FP32 against FP64 on
+the 2048 x 512 case over 100,000 steps: Cd, Cl_rms, St, velocity field), `precision_large`
+(16384 x 4096 with FP64 mean/rms field statistics), `adjoint` (gradient of mean drag on
+512 x 128: cost over the forward run and the check against central differences) and `batch`
+(the 64-case sweep against the same cases stepped one after another).  Under torchrun every
+rank runs an independent replica (its own seed) on its own GPU: weak scaling, no collective on
+the data path; times are max over ranks.
 """
 import argparse
 import json
@@ -50,6 +57,17 @@ def parse():
                     help="with --profile: accumulate the FP64 field statistics in every step")
     ap.add_argument("--profile", action="store_true",
                     help="only run warmup + steps of the case (for ncu); prints nothing else")
+    ap.add_argument("--e2e-steps", type=int, default=1000,
+                    help="steps of the end-to-end restart segment (at least --steps)")
+    ap.add_argument("--no-studies", action="store_true",
+                    help="skip the precision, adjoint and batch blocks")
+    ap.add_argument("--precision-steps", type=int, default=100000,
+                    help="steps of the FP32-vs-FP64 study on the 2048 x 512 case")
+    ap.add_argument("--large-precision-steps", type=int, default=2000,
+                    help="steps of the FP32-vs-FP64 study with field statistics on 16384 x 4096 (0: skip)")
+    ap.add_argument("--adjoint-directions", type=int, default=16)
+    ap.add_argument("--batch-steps", type=int, default=2000)
+    ap.add_argument("--batch-seq-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -374,11 +392,13 @@ def main():
         return total_ms, launches, per, noflush_ms, (t_wall0, t_wall1), tile
 
     def time_e2e(precision, K, tile):
-        """Public-API run with host buffers: load state, K steps, force drains, fields back."""
+        """Public-API restart segment with host buffers: load the state from pinned host
+        memory, K steps, force history drained every 100 steps, rho/ux/uy of the last step
+        read back into pinned buffers.  Wall clock, max over ranks."""
         sim = m.Simulation(cfg, precision=precision, device=dev)
         sim.set_stream(stream.cuda_stream)
         sim.tile_config = tile               # the autotuner's choice for this case (untimed setup)
-        # pinned host buffers: the initial populations (Fortran order) and rho, ux, uy
+        # pinned host buffers: the initial populations (Fortran order, FP64 as in restart.dat)
         f0 = torch.empty(nodes * 9, dtype=torch.float64).pin_memory().numpy()
         sim.get_state(out=f0)                # host copy of the seeded initial populations
         mac = [torch.empty(nodes, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
@@ -398,16 +418,17 @@ def main():
         el = time.perf_counter() - t0
         el = max_over_ranks(el)
         sim.close()
-        elem = 8
-        h2d = nodes * 9 * elem / K
+        h2d = nodes * 9 * 8 / K
         d2h = (nrec * 4 * 8 + 3 * nodes * 8) / K
         del mac
-        return {"value": world * nodes * K / el / 1e6, "unit": "MLUPS",
+        return {"value": world * nodes * K / el / 1e6, "unit": "MLUPS", "steps": K,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "note": "load_state(pinned host f, FP64) + K x step + force drain every 100 steps + "
-                        "rho/ux/uy of the last step into pinned buffers, wall clock, max over ranks"}
+                "note": f"restart segment through the C ABI: load_state (FP64 populations from pinned host "
+                        f"memory) + {K} steps + force records drained every 100 steps + rho/ux/uy of the last "
+                        f"step into pinned buffers; wall clock, max over ranks"}
 
-    precisions = [args.precision] if args.precision else ([32, 64] if _fp32_available(m, cfg) else [64])
+    # FP64 (the reference's arithmetic) is the headline; the FP32 deviation form runs beside it
+    precisions = [args.precision] if args.precision else ([64, 32] if _fp32_available(m, cfg) else [64])
     head = precisions[0]
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
@@ -440,7 +461,8 @@ def main():
     if sampler:
         time.sleep(0.3)
         sampler.stop()
-    e2e = time_e2e(head, args.steps, results[head][5])
+    e2e_steps = max(args.steps, args.e2e_steps)
+    e2e = {prec: time_e2e(prec, e2e_steps, results[prec][5]) for prec in precisions}
 
     total_ms, launches, per, noflush_ms, win, tile = results[head]
     ms_step = total_ms / args.steps
@@ -453,7 +475,8 @@ def main():
         "metric": "D2Q9 MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if head == 32 else "f64", "data": "synthetic (seeded noise init)",
-        "config": dict(case_desc(args.case, cfg), precision=f"fp{head}", l2="flushed before every timed step (256 MiB written, then read)",
+        "config": dict(case_desc(args.case, cfg), precision=f"fp{head}",
+                       l2="flushed before every timed step (256 MiB written, then read)",
                        parallelism=f"replicas{world}", tile_shape=tile),
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -461,14 +484,14 @@ def main():
                      "traffic": (tr * nodes) if tr is not None else None,
                      "algorithmic_bytes_per_launch": BYTES_PER_LU[head] * nodes,
                      "traffic_source": tr_src},
-        "e2e": e2e,
+        "e2e": e2e[head],
     }
     for prec in precisions:
         t, _, _, nf, _, tl = results[prec]
+        gbs = BYTES_PER_LU[prec] * nodes / (t / args.steps * 1e-3) / 1e9
         line[f"fp{prec}"] = {"mlups": world * nodes * args.steps / (t * 1e-3) / 1e6, "ms_per_step": t / args.steps,
-                             "tile_shape": tl,
-                             "ms_per_step_unflushed": nf,
-                             "hbm_gbs_alg": BYTES_PER_LU[prec] * nodes / (t / args.steps * 1e-3) / 1e9}
+                             "tile_shape": tl, "ms_per_step_unflushed": nf, "hbm_gbs_alg": gbs,
+                             "bytes_per_lu": BYTES_PER_LU[prec], "frac_of_peak": gbs / peak, "e2e": e2e[prec]}
     if 32 in results and 64 in results:
         line["fp32_over_fp64"] = results[64][0] / results[32][0]
     if large:
@@ -494,6 +517,8 @@ def main():
         t0 = min(w[0] for w in wins) - 1.2
         t1 = max(w[1] for w in wins)
         line["clocks"] = sampler.summary(t0, t1)
+    if world == 1 and not args.no_studies:
+        line.update(run_studies(args, peak))
     ranks.barrier()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -504,6 +529,64 @@ def main():
         print(json.dumps(line), flush=True)
     ranks.close()
     return 0
+
+
+def run_studies(args, peak):
+    """The rest of the benchmark metric, measured in the same run: FP32 against FP64 on the
+    2048 x 512 case (and with field statistics on 16384 x 4096), the adjoint's cost and its check
+    against central differences on 512 x 128, and the 64-case batched sweep."""
+    out = {}
+    from mrlbm_2d_b200 import adjoint_check, batch_sweep, precision_study
+    t0 = time.perf_counter()
+    try:
+        p = precision_study.study("mid", args.precision_steps)
+        keep = ("case", "nx", "ny", "steps", "stats_from", "rel_err_Cd", "abs_err_St", "abs_err_St_spectral",
+                "rel_err_Cl_rms", "velocity_rel_l2", "velocity_max_abs_over_U", "drag_history_rel_l2")
+        out["precision"] = {k: p[k] for k in keep if k in p}
+        for prec in (64, 32):
+            r = p[f"fp{prec}"]
+            out["precision"][f"fp{prec}"] = {k: r[k] for k in ("Cd", "Cl_rms", "St", "St_spectral", "mlups_wall")
+                                             if k in r}
+        out["precision"]["targets"] = {"rel_err_Cd": 1e-3, "abs_err_St": 1e-3}
+        out["precision"]["seconds"] = time.perf_counter() - t0
+    except Exception as ex:
+        out["precision"] = {"error": str(ex)}
+    if args.large_precision_steps > 0:
+        t0 = time.perf_counter()
+        try:
+            n = args.large_precision_steps
+            p = precision_study.study("large", n, stats_from=n // 2, fields=True, chunk=n)
+            keep = ("case", "nx", "ny", "steps", "stats_from", "rel_err_Cd", "velocity_rel_l2", "drag_history_rel_l2",
+                    "mean_u_rel_l2", "mean_v_rel_l2", "mean_p_rel_l2", "rms_u_rel_l2", "rms_v_rel_l2", "rms_p_rel_l2",
+                    "field_samples")
+            out["precision_large"] = {k: p[k] for k in keep if k in p}
+            out["precision_large"]["seconds"] = time.perf_counter() - t0
+        except Exception as ex:
+            out["precision_large"] = {"error": str(ex)}
+    t0 = time.perf_counter()
+    try:
+        a = adjoint_check.check(directions=args.adjoint_directions)
+        out["adjoint"] = {k: a[k] for k in ("case", "steps", "window", "checkpoint_every", "J", "directions",
+                                            "rel_step", "max_rel_err", "median_rel_err", "forward_s", "gradient_s",
+                                            "gradient_over_forward")}
+        out["adjoint"]["targets"] = {"max_rel_err": 1e-3, "gradient_over_forward": 4.0}
+        out["adjoint"]["seconds"] = time.perf_counter() - t0
+    except Exception as ex:
+        out["adjoint"] = {"error": str(ex)}
+    t0 = time.perf_counter()
+    try:
+        b = batch_sweep.sweep(64, args.batch_steps, args.batch_seq_steps, 32, trial_steps=20)
+        bb = b["batch"]
+        gbs = BYTES_PER_LU[32] * bb["mlups"] * 1e6 / 1e9
+        out["batch"] = {"cases": b["cases"], "nodes_total": b["nodes_total"], "steps": b["steps"],
+                        "autotune": b["autotune"], "mlups": bb["mlups"], "ms_per_step": bb["ms_per_step"],
+                        "hbm_gbs_alg": gbs, "frac_of_peak": gbs / peak, "bytes_per_lu": BYTES_PER_LU[32],
+                        "sequential_mlups": b["sequential"]["mlups"], "speedup_vs_sequential": b["speedup"],
+                        "unstable_cases": len(b["unstable_cases"]), "l2": "working set 554 MB (4.4x the L2), no flush"}
+        out["batch"]["seconds"] = time.perf_counter() - t0
+    except Exception as ex:
+        out["batch"] = {"error": str(ex)}
+    return out
 
 
 def _fp32_available(m, cfg):

@@ -21,25 +21,16 @@ from . import api
 from .config import case_adjoint
 
 
-def main(argv=None):
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--steps", type=int, default=8000)
-    ap.add_argument("--window", type=int, default=2000)
-    ap.add_argument("--checkpoint", type=int, default=100)
-    ap.add_argument("--directions", type=int, default=16)
-    ap.add_argument("--rel-step", type=float, default=1e-4)
-    ap.add_argument("--seed", type=int, default=2026)
-    ap.add_argument("--fp32", action="store_true",
-                    help="also run the adjoint on an FP32 handle (FP32 trajectory, FP64 adjoint) and compare")
-    a = ap.parse_args(argv)
+def check(steps=8000, window=2000, checkpoint=100, directions=16, rel_step=1e-4, seed=2026, fp32=False):
+    """Adjoint against central differences on the 512 x 128 case; returns the record as a dict."""
     cfg = case_adjoint()
     sim = api.Simulation(cfg, precision=api.FP64)
-    rng = np.random.default_rng(a.seed)
+    rng = np.random.default_rng(seed)
     body = 1e-7 * rng.standard_normal((2, sim.nx, sim.ny))
     uin = cfg.uo + 1e-3 * rng.standard_normal(sim.ny)
     sim.set_body_force(body)
     sim.set_inlet_profile(uin)
-    N, T, K = a.steps, a.window, a.checkpoint
+    N, T, K = steps, window, checkpoint
     sim.adjoint_drag(N, T, K)                                  # warm-up
     t0 = time.perf_counter()
     J0 = sim.adjoint_drag(N, T, K, grads=False)
@@ -47,8 +38,8 @@ def main(argv=None):
     J, gb, gu = sim.adjoint_drag(N, T, K)
     t2 = time.perf_counter()
     errs = []
-    h = a.rel_step
-    for _ in range(a.directions):
+    h = rel_step
+    for _ in range(directions):
         db = 1e-7 * rng.standard_normal(body.shape)
         du = 1e-3 * rng.standard_normal(uin.shape)
         vals = []
@@ -60,27 +51,42 @@ def main(argv=None):
         ad = float((gb * db).sum() + (gu * du).sum())
         errs.append({"adjoint": ad, "fd": fd, "rel_err": abs(ad - fd) / abs(fd)})
     sim.close()
-    fp32 = None
-    if a.fp32:
+    rec32 = None
+    if fp32:
         s32 = api.Simulation(cfg, precision=api.FP32)
         s32.set_body_force(body)
         s32.set_inlet_profile(uin)
         J32, gb32, gu32 = s32.adjoint_drag(N, T, K)
         s32.close()
         rel = []
-        for _ in range(a.directions):
+        for _ in range(directions):
             db = rng.standard_normal(body.shape)
             du = rng.standard_normal(uin.shape)
             d64 = float((gb * db).sum() + (gu * du).sum())
             d32 = float((gb32 * db).sum() + (gu32 * du).sum())
             rel.append(abs(d32 - d64) / abs(d64))
-        fp32 = {"J": J32, "rel_err_J": abs(J32 - J) / abs(J), "max_rel_err_vs_fp64_adjoint": max(rel)}
-    out = {"case": "512x128 D=32 Re=100 U=0.05", "steps": N, "window": T, "checkpoint_every": K, "J": J,
-           "J_forward_only": J0, "directions": a.directions, "rel_step": h,
-           "max_rel_err": max(e["rel_err"] for e in errs), "median_rel_err": float(np.median([e["rel_err"] for e in errs])),
-           "forward_s": t1 - t0, "gradient_s": t2 - t1, "gradient_over_forward": (t2 - t1) / (t1 - t0),
-           "grad_body_max": float(np.abs(gb).max()), "grad_uin_max": float(np.abs(gu).max()), "fp32": fp32,
-           "checks": errs}
+        rec32 = {"J": J32, "rel_err_J": abs(J32 - J) / abs(J), "max_rel_err_vs_fp64_adjoint": max(rel)}
+    return {"case": "512x128 D=32 Re=100 U=0.05", "steps": N, "window": T, "checkpoint_every": K, "J": J,
+            "J_forward_only": J0, "directions": directions, "rel_step": h,
+            "max_rel_err": max(e["rel_err"] for e in errs),
+            "median_rel_err": float(np.median([e["rel_err"] for e in errs])),
+            "forward_s": t1 - t0, "gradient_s": t2 - t1, "gradient_over_forward": (t2 - t1) / (t1 - t0),
+            "grad_body_max": float(np.abs(gb).max()), "grad_uin_max": float(np.abs(gu).max()), "fp32": rec32,
+            "checks": errs}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=8000)
+    ap.add_argument("--window", type=int, default=2000)
+    ap.add_argument("--checkpoint", type=int, default=100)
+    ap.add_argument("--directions", type=int, default=16)
+    ap.add_argument("--rel-step", type=float, default=1e-4)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--fp32", action="store_true",
+                    help="also run the adjoint on an FP32 handle (FP32 trajectory, FP64 adjoint) and compare")
+    a = ap.parse_args(argv)
+    out = check(a.steps, a.window, a.checkpoint, a.directions, a.rel_step, a.seed, a.fp32)
     print(json.dumps(out), flush=True)
     return out
 

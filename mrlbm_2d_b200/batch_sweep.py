@@ -21,27 +21,20 @@ from . import api
 from .config import sweep_cases
 
 
-def main(argv=None):
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--cases", type=int, default=64)
-    ap.add_argument("--steps", type=int, default=20000)
-    ap.add_argument("--seq-steps", type=int, default=2000)
-    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
-    ap.add_argument("--trial-steps", type=int, default=50)
-    ap.add_argument("--seed", type=int, default=4242)
-    ap.add_argument("--no-sequential", action="store_true", help="skip the one-case-at-a-time baseline")
-    a = ap.parse_args(argv)
+def sweep(cases=64, steps=20000, seq_steps=2000, precision=32, trial_steps=50, seed=4242, sequential=True,
+          stream=None):
+    """The batched sweep and (optionally) the one-case-at-a-time baseline; returns a dict."""
     import torch
-    cfgs = sweep_cases(a.cases, seed=a.seed)
+    cfgs = sweep_cases(cases, seed=seed)
     nodes = [c.nx * c.ny for c in cfgs]
     total = float(sum(nodes))
-    out = {"cases": a.cases, "nodes_total": int(total), "precision": a.precision, "steps": a.steps,
+    out = {"cases": cases, "nodes_total": int(total), "precision": precision, "steps": steps,
            "nx_range": [min(c.nx for c in cfgs), max(c.nx for c in cfgs)],
            "Re_range": [round(min(c.Re for c in cfgs), 2), round(max(c.Re for c in cfgs), 2)]}
 
-    b = api.Batch(cfgs, precision=a.precision)
+    b = api.Batch(cfgs, precision=precision)
     t0 = time.perf_counter()
-    (tile, sched, spl), ms = b.autotune(trial_steps=a.trial_steps)
+    (tile, sched, spl), ms = b.autotune(trial_steps=trial_steps)
     out["autotune"] = {"tile_shape": tile, "schedule": ["persistent", "graph"][sched], "steps_per_launch": spl,
                        "trial_ms_per_step": ms, "seconds": time.perf_counter() - t0}
     b.step(spl)                                   # warm-up of the chosen schedule
@@ -50,7 +43,7 @@ def main(argv=None):
     n0 = b.launch_count()
     torch.cuda.synchronize()
     e0.record(bs)
-    b.step(a.steps)
+    b.step(steps)
     e1.record(bs)
     e1.synchronize()
     el = e0.elapsed_time(e1) * 1e-3
@@ -62,7 +55,7 @@ def main(argv=None):
     out["unstable_cases"] = [{"case": i, "nx": cfgs[i].nx, "Re": round(cfgs[i].Re, 2),
                               "tau": round(0.5 + 3.0 * cfgs[i].uo * 2.0 * cfgs[i].r_c / cfgs[i].Re, 5)}
                              for i in flagged]
-    out["batch"] = {"seconds": el, "ms_per_step": el / a.steps * 1e3, "mlups": total * a.steps / el / 1e6,
+    out["batch"] = {"seconds": el, "ms_per_step": el / steps * 1e3, "mlups": total * steps / el / 1e6,
                     "launches": b.launch_count() - n0}
     drag = []
     for i, c in enumerate(b.cases):
@@ -71,27 +64,39 @@ def main(argv=None):
             drag.append(float(fd[-1]))
     out["finite_forces_of_stable_cases"] = bool(np.all(np.isfinite(drag)))
     b.close()
-
-    if a.no_sequential:
-        print(json.dumps(out), flush=True)
+    if not sequential:
         return out
     seq_el = 0.0
-    st = torch.cuda.Stream()
+    st = stream or torch.cuda.Stream()
     for cfg in cfgs:
-        s = api.Simulation(cfg, precision=a.precision)
+        s = api.Simulation(cfg, precision=precision)
         s.set_stream(st.cuda_stream)
         s.autotune(trial_steps=10)
         s.step(3)
         torch.cuda.synchronize()
         e0.record(st)
-        s.step(a.seq_steps)
+        s.step(seq_steps)
         e1.record(st)
         e1.synchronize()
         seq_el += e0.elapsed_time(e1) * 1e-3
         s.close()
-    out["sequential"] = {"seconds": seq_el, "steps_per_case": a.seq_steps,
-                         "mlups": total * a.seq_steps / seq_el / 1e6}
+    out["sequential"] = {"seconds": seq_el, "steps_per_case": seq_steps,
+                         "mlups": total * seq_steps / seq_el / 1e6}
     out["speedup"] = out["batch"]["mlups"] / out["sequential"]["mlups"]
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--seq-steps", type=int, default=2000)
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--trial-steps", type=int, default=50)
+    ap.add_argument("--seed", type=int, default=4242)
+    ap.add_argument("--no-sequential", action="store_true", help="skip the one-case-at-a-time baseline")
+    a = ap.parse_args(argv)
+    out = sweep(a.cases, a.steps, a.seq_steps, a.precision, a.trial_steps, a.seed, not a.no_sequential)
     print(json.dumps(out), flush=True)
     return out
 

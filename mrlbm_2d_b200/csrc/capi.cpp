@@ -46,7 +46,11 @@ struct mrlbm_handle {
     void* d_bgeo = nullptr;
     int* d_bint = nullptr;
     int* d_boxmap = nullptr;
-    double* d_partials = nullptr;
+    double* d_partials = nullptr;             // two slots of the per-step record terms
+    size_t partials_n = 0;                    // doubles per slot
+    int pslot = 0;                            // slot the next stats step writes
+    // a stats step whose record sums are deferred to the next launch (StepParams::defer)
+    struct Pending { bool on = false; int slot = 0; int rec_idx = 0; int iter = 0; } pend;
     unsigned* d_counter = nullptr;
     double* d_ring = nullptr;
     int ring_n = 0;
@@ -215,7 +219,21 @@ int upload_state(mrlbm_handle* h, const double* f) {
     return MRLBM_OK;
 }
 
+// Sum the terms of a stats step whose record was deferred (one small launch on the handle's
+// stream) so the device ring holds every record of the steps launched so far.
+int finish_pending(mrlbm_handle* h) {
+    if (!h->pend.on) return MRLBM_OK;
+    h->pend.on = false;
+    if (launch_finish_record(h->d_partials + (size_t)h->pend.slot * h->partials_n, h->geo.nb, h->L.ny, h->halo_l ? 1 : 0,
+                             h->d_ring + (size_t)h->pend.rec_idx * REC_WORDS, h->pend.iter, h->stream) != 0)
+        return fail(h, MRLBM_ECUDA, "record sums launch failed");
+    ++h->launches;
+    return MRLBM_OK;
+}
+
 int drain_ring(mrlbm_handle* h) {
+    int prc = finish_pending(h);
+    if (prc != MRLBM_OK) return prc;
     if (h->ring_n == 0) return MRLBM_OK;
     CK(cudaMemcpyAsync(h->h_ring, h->d_ring, (size_t)h->ring_n * REC_WORDS * sizeof(double),
                        cudaMemcpyDeviceToHost, h->stream));
@@ -369,6 +387,19 @@ int surface_step(mrlbm_handle* h) {
     return MRLBM_OK;
 }
 
+// Deferred record sums for a step launched through launch_one: this step's terms go to the
+// slot pslot, and the pending step's terms (the other slot) are summed by this launch.
+template <class T>
+void set_deferred(const mrlbm_handle* h, StepParams<T>& p) {
+    p.defer = 1;
+    p.partials = h->d_partials + (size_t)h->pslot * h->partials_n;
+    if (h->pend.on) {
+        p.prev_partials = h->d_partials + (size_t)h->pend.slot * h->partials_n;
+        p.prev_rec = h->d_ring + (size_t)h->pend.rec_idx * REC_WORDS;
+        p.prev_iter = h->pend.iter;
+    }
+}
+
 int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     const int tc = h->tile_cfg;
     const bool fstat = h->d_fstat && h->iter >= h->fstat_begin && h->iter <= h->fstat_end;
@@ -381,6 +412,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     if (h->precision == MRLBM_FP64) {
         StepParams<double> p{};
         fill_common(h, p);
+        set_deferred(h, p);
         p.src = (const double*)h->buf[h->cur];
         p.dst = (double*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? h->d_uin : nullptr;
@@ -403,6 +435,7 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     } else {
         StepParams<float> p{};
         fill_common(h, p);
+        set_deferred(h, p);
         p.src = (const float*)h->buf[h->cur];
         p.dst = (float*)h->buf[1 - h->cur];
         p.u_in = h->has_uin ? (const float*)h->d_uin : nullptr;
@@ -431,6 +464,12 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
     if (rc != 0) {
         h->err = std::string("kernel launch failed: ") + cudaGetErrorString(cudaGetLastError());
         return MRLBM_ECUDA;
+    }
+    // the pending record (if any) is summed by this launch; this step's, if a stats step, is next
+    h->pend.on = false;
+    if (stats) {
+        h->pend = mrlbm_handle::Pending{true, h->pslot, h->ring_n, h->iter};
+        h->pslot ^= 1;
     }
     if (tma) {
         int bw, bh, st;
@@ -637,7 +676,8 @@ static int create_impl(const mrlbm_config* cfg, int precision, int device, int s
     const size_t nbox = std::max<size_t>(h->geo.boxmap.size(), 1);
     ok = ok && ck(cudaMalloc((void**)&h->d_boxmap, nbox * sizeof(int)), "cudaMalloc boxmap");
     const size_t nscratch = 2 * (size_t)nb + (size_t)ny + 8;
-    ok = ok && ck(cudaMalloc((void**)&h->d_partials, nscratch * sizeof(double)), "cudaMalloc partials") &&
+    h->partials_n = nscratch;
+    ok = ok && ck(cudaMalloc((void**)&h->d_partials, 2 * nscratch * sizeof(double)), "cudaMalloc partials") &&
          ck(cudaMalloc((void**)&h->d_counter, 2 * sizeof(unsigned)), "cudaMalloc counter") &&
          ck(cudaMalloc((void**)&h->d_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMalloc ring") &&
          ck(cudaMalloc((void**)&h->d_err, sizeof(int)), "cudaMalloc err") &&
@@ -1353,6 +1393,7 @@ int mrlbm_autotune(mrlbm_handle* h, int32_t trial_steps, int32_t* best_cfg, doub
         h->ring_n = ring0;
         h->ovr_live = ovr0;
         h->hist.resize(hist0);
+        h->pend.on = false;                             // the trials' last record is discarded
     }
     h->surf_on = surf0;
     h->fstat_begin = fsb0;

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
                 }
             }
             __syncthreads();
-            if (aux) aux_item<Phys>(sp, smem, local);
+            if (aux) aux_item<Phys, wide_wall<Phys>(WARPS * 32, MINB)>(sp, smem, local);
             else vec_tile<Phys, WARPS, NJ>(sp, local);
             __syncthreads();
         }

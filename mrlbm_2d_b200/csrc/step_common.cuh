@@ -269,6 +269,22 @@ __device__ __forceinline__ void force_tail(const typename Phys::P& p, unsigned c
     }
 }
 
+// The three sums of a force record, each over its terms in index order (one warp per sum):
+// Fx over part[0, nb), Fy over part[nb, 2 nb), rho(1,j) over part[2 nb, 2 nb + ny) (0 on an
+// x-slab without column 1).  Used for deferred records (the next launch sums the terms of the
+// previous stats step) and by the finishing kernel; smem holds 3 * AUX_CHUNK doubles.
+__device__ __forceinline__ void record_sums(const double* part, int nb, int ny, int halo_l, double* rec, int iter,
+                                            unsigned char* smem) {
+    const int tid = threadIdx.x, lane = tid & 31, nw = (int)(blockDim.x >> 5);
+    double* st = reinterpret_cast<double*>(smem);
+    for (int w = tid >> 5; w < 3; w += nw) {
+        const int n = w < 2 ? nb : (halo_l ? 0 : ny);
+        const double sum = warp_ordered_sum(part + w * nb, n, st + w * AUX_CHUNK, lane);
+        if (lane == 0) rec[w + 1] = sum;
+    }
+    if (tid == 0) rec[0] = (double)iter;
+}
+
 // Edge blocks [0, inlet_blocks) hold the inlet column (it comes first in their enumeration).
 __device__ __forceinline__ int inlet_blocks(int ny, int halo_l) {
     return halo_l ? 0 : (ny + (int)blockDim.x - 1) / (int)blockDim.x;
@@ -291,7 +307,9 @@ __device__ __forceinline__ void inlet_tail(const typename Phys::P& p, unsigned c
     }
 }
 
-template <class Phys>
+// WIDE: the kernel has registers enough (Phys::WIDE_REGS per thread) for lane 0 to gather its
+// node's own populations together with its stencil node's, and for the closure to be inlined.
+template <class Phys, bool WIDE>
 __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsigned char* smem, int bb) {
     using T = typename Phys::T;
     T* sg = reinterpret_cast<T*>(smem);                               // G_STAGED * BNODES
@@ -299,31 +317,55 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
     const int nthr = blockDim.x, tid = threadIdx.x;
     const int bn = nthr / BLANES;
     const int l0 = bb * bn;
-    for (int idx = tid; idx < G_STAGED * bn; idx += nthr) {
-        const int f = idx / bn, n = idx - f * bn;
-        sg[idx] = (l0 + n < p.nb) ? p.bgeo[f * p.nb + l0 + n] : T(0);
+    // Every load of the staging is issued before the first shared-memory store, so the tables
+    // arrive in one memory round trip instead of one per loop trip (after an L2 flush each trip
+    // is a DRAM access, and the wall-node chain is on the step's critical path).  Each thread
+    // stages G_STAGED / BLANES real and I_NFIELDS / BLANES integer entries (rounded up).
+    {
+        constexpr int GU = (G_STAGED + BLANES - 1) / BLANES, IU = (I_NFIELDS + BLANES - 1) / BLANES;
+        T gv[GU];
+        int iv[IU];
+#pragma unroll
+        for (int u = 0; u < GU; ++u) {
+            const int idx = tid + u * nthr, f = idx / bn, n = idx - f * bn;
+            gv[u] = (idx < G_STAGED * bn && l0 + n < p.nb) ? p.bgeo[f * p.nb + l0 + n] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < IU; ++u) {
+            const int idx = tid + u * nthr, f = idx / bn, n = idx - f * bn;
+            iv[u] = (idx < I_NFIELDS * bn && l0 + n < p.nb) ? p.bint[f * p.nb + l0 + n] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < GU; ++u)
+            if (tid + u * nthr < G_STAGED * bn) sg[tid + u * nthr] = gv[u];
+#pragma unroll
+        for (int u = 0; u < IU; ++u)
+            if (tid + u * nthr < I_NFIELDS * bn) sgi[tid + u * nthr] = iv[u];
     }
-    for (int idx = tid; idx < I_NFIELDS * bn; idx += nthr) {
-        const int f = idx / bn, n = idx - f * bn;
-        sgi[idx] = (l0 + n < p.nb) ? p.bint[f * p.nb + l0 + n] : 0;
+    const int li = tid / BLANES, lane = tid % BLANES;
+    const int l = l0 + li;
+    const bool active = l < p.nb;
+    const bool interp = p.closure == CLOSURE_UNROTATED || p.vel_interp || p.mom_interp;
+    const int r = lane >> 2, c = lane & 3;        // reference point 2 + r, corner c
+    const int s = 4 * r + c;
+    // this lane's stencil weights (creation-time tables, like the staged ones)
+    T cc = T(0), ss = T(0), s2 = T(0);
+    if (active && interp) {
+        cc = p.bgeo[(G_SCC + s) * p.nb + l];
+        ss = p.bgeo[(G_SSS + s) * p.nb + l];
+        s2 = p.bgeo[(G_SS2 + s) * p.nb + l];
     }
     // The tables are written once, when the handle is created, so the staging above may run
     // while the previous step finishes; everything below reads or writes what steps change.
     wait_prior_grid();
     __syncthreads();
     const BTab<T> tb{sg, sgi, bn};
-    const int li = tid / BLANES, lane = tid % BLANES;
-    const int l = l0 + li;
-    const bool active = l < p.nb;
-    const bool interp = p.closure == CLOSURE_UNROTATED || p.vel_interp || p.mom_interp;
+    T fown[Q];
+    if (WIDE && active && lane == 0) gather(p, tb.gi(I_NODEI, li), tb.gi(I_NODEJ, li), fown);
     T ux = T(0), uy = T(0), mx = T(0), my = T(0);
-    const int r = lane >> 2, c = lane & 3;        // reference point 2 + r, corner c
     const T xd = active ? tb.gf(r == 0 ? G_XD2 : G_XD3, li) : T(0);
     const T yd = active ? tb.gf(r == 0 ? G_YD2 : G_YD3, li) : T(0);
     if (active && interp) {
-        const int s = 4 * r + c;
-        const T cc = p.bgeo[(G_SCC + s) * p.nb + l], ss = p.bgeo[(G_SSS + s) * p.nb + l];
-        const T s2 = p.bgeo[(G_SS2 + s) * p.nb + l];
         Phys::stencil_node(p, tb.gi(I_SI + s, li), tb.gi(I_SJ + s, li), cc, ss, s2, ux, uy, mx, my);
         const T wx = (c & 1) ? xd : (T(1) - xd);
         ux = wx * ux; uy = wx * uy; mx = wx * mx; my = wx * my;
@@ -347,10 +389,11 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
     const T mx3 = __shfl_down_sync(full, mx, 4, BLANES), my3 = __shfl_down_sync(full, my, 4, BLANES);
     double Fx = 0.0, Fy = 0.0;
     if (active && lane == 0) {
-        Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
+        if constexpr (WIDE) Phys::boundary_close_pre(p, tb, li, l, fown, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
+        else Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
         if (p.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
     }
-    force_tail<Phys>(p, smem);
+    if (!p.defer) force_tail<Phys>(p, smem);
 }
 
 // Edge blocks: one thread per domain-edge node, so the edge closures (outlet neighbour gather,
@@ -376,7 +419,8 @@ __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, un
         const double rho = Phys::edge_bulk_node(p, i, j, CLS_FLUID);
         if (p.do_stats && i == 1 && !p.halo_l) p.partials[2 * p.nb + j - 1] = rho;
     }
-    inlet_tail<Phys>(p, smem, eb);
+    if (!p.defer) inlet_tail<Phys>(p, smem, eb);
+    else if (eb == 0 && p.prev_rec) record_sums(p.prev_partials, p.nb, p.L.ny, p.halo_l, p.prev_rec, p.prev_iter, smem);
 }
 
 // Shared memory of an auxiliary block: the boundary tables and, afterwards, the tail's
@@ -389,20 +433,24 @@ constexpr int aux_smem_bytes() {
 }
 
 // Auxiliary work item b of a step: boundary block b (b < nbblk) or edge block b - nbblk.
-template <class Phys>
+template <class Phys, bool WIDE>
 __device__ __forceinline__ void aux_item(const typename Phys::P& p, unsigned char* smem, int b) {
-    if (b < p.nbblk) boundary_block<Phys>(p, smem, b);
+    if (b < p.nbblk) boundary_block<Phys, WIDE>(p, smem, b);
     else edge_block<Phys>(p, b - p.nbblk, smem);
 }
 
+// Whether a kernel of `threads` threads and `minb` resident blocks per SM takes the wide wall path.
+template <class Phys>
+constexpr bool wide_wall(int threads, int minb) { return 65536 / (threads * minb) >= Phys::WIDE_REGS; }
+
 // Boundary and edge blocks sit at the start of the grid.  True when this block is one of them
 // (and has done its work); bulk tile t is then blockIdx.x - nbblk - neblk.
-template <class Phys>
+template <class Phys, bool WIDE>
 __device__ __forceinline__ bool run_aux_block(const typename Phys::P& p) {
     __shared__ __align__(16) unsigned char smem[aux_smem_bytes<typename Phys::T>()];
     const int b = (int)blockIdx.x;
     if (b >= p.nbblk + p.neblk) return false;
-    aux_item<Phys>(p, smem, b);
+    aux_item<Phys, WIDE>(p, smem, b);
     return true;
 }
 
@@ -410,6 +458,15 @@ template <class P>
 inline int edge_blocks(const P& p, int nthr) {
     const int n = 2 * p.L.nx + (p.halo_l ? 0 : p.L.ny - 2) + (p.halo_r ? 0 : p.L.ny - 2);
     return (n + nthr - 1) / nthr;
+}
+
+// True when every node of columns i0..i1 and rows j0..j1 is an interior bulk node: no domain
+// edge (an x-slab's halo faces are not edges), nothing beyond the lattice, no node of the
+// cylinder's bounding box.  Block-uniform when the bounds are.
+template <class T>
+__device__ __forceinline__ bool plain_tile(const StepParams<T>& p, int i0, int i1, int j0, int j1) {
+    return col_interior(p, i0) && i1 <= p.L.nx && col_interior(p, i1) && j0 > 1 && j1 < p.L.ny &&
+           (i1 < p.box_x0 || i0 >= p.box_x0 + p.box_w || j1 < p.box_y0 || j0 >= p.box_y0 + p.box_h);
 }
 
 // Interior populations (no wraps, no ghosts): the branch-free half of `gather`.
@@ -429,12 +486,21 @@ template <class Phys, int BX, int BY, int NJ, int MINB>
 __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
     if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys>(p)) return;
+    if (run_aux_block<Phys, wide_wall<Phys>(BX * BY, MINB)>(p)) return;
     const int t = blockIdx.x - p.nbblk - p.neblk;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
     const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
     const int i = 1 + tx * BX + lx;
     const int nx = p.L.nx, ny = p.L.ny;
+    if (plain_tile(p, 1 + tx * BX, 1 + tx * BX + BX - 1, 1 + ty * BY * NJ, ty * BY * NJ + BY * NJ)) {
+        // no edge, ghost or cylinder-box node in the tile: no per-node class or edge tests
+        T f[NJ][Q];
+#pragma unroll
+        for (int r = 0; r < NJ; ++r) gather_interior(p, i, 1 + ty * BY * NJ + r * BY + ly, f[r]);
+#pragma unroll
+        for (int r = 0; r < NJ; ++r) Phys::finish(p, i, 1 + ty * BY * NJ + r * BY + ly, CLS_FLUID, f[r]);
+        return;
+    }
     if (i > nx) return;
     T f[NJ][Q];
     int cls[NJ];
@@ -566,7 +632,7 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
 template <class Phys, int WARPS, int NJ, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
     if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys>(p)) return;
+    if (run_aux_block<Phys, wide_wall<Phys>(WARPS * 32, MINB)>(p)) return;
     vec_tile<Phys, WARPS, NJ>(p, (int)blockIdx.x - p.nbblk - p.neblk);
 }
 
@@ -596,7 +662,7 @@ template <class Phys, int B, int MINB>
 __global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constant__ typename Phys::P p) {
     using T = typename Phys::T;
     if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys>(p)) return;
+    if (run_aux_block<Phys, wide_wall<Phys>(B, MINB)>(p)) return;
     const int nx = p.L.nx, ny = p.L.ny, tiles_x = p.tiles_x;
     const int units = tiles_x * ny;
     const int G = (int)gridDim.x - p.nbblk - p.neblk;

@@ -8,6 +8,17 @@
 
 namespace mrlbm {
 
+__global__ void __launch_bounds__(96) finish_record_kernel(const double* __restrict__ part, int nb, int ny, int halo_l,
+                                                           double* rec, int iter) {
+    __shared__ __align__(16) unsigned char smem[3 * AUX_CHUNK * sizeof(double)];
+    record_sums(part, nb, ny, halo_l, rec, iter, smem);
+}
+
+int launch_finish_record(const double* partials, int nb, int ny, int halo_l, double* rec, int iter, void* stream) {
+    finish_record_kernel<<<1, 96, 0, (cudaStream_t)stream>>>(partials, nb, ny, halo_l, rec, iter);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int launch_face_f64(const StepParams<double>& p, bool full, void* stream) {
     return full ? launch_face<fp64::Physics>(p, (cudaStream_t)stream)
                 : launch_face<fp64::PhysicsLean>(p, (cudaStream_t)stream);

@@ -226,13 +226,18 @@ __device__ __forceinline__ void closure_strong(const P& p, const BTab<float>& tb
 
 // Lane 0 of a boundary node: extrapolation (wall value 0), closure, collision, store and
 // the momentum-exchange force accumulated in FP64 from w_k + g_k (2d_mrlbm.f90:558-591).
-template <bool FULL>
-__device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb, int li, int l, float ux2, float uy2,
-                                            float mx2, float my2, float ux3, float uy3, float mx3, float my3,
+template <bool FULL, bool PRE>
+__device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb, int li, int l, const float* gpre, float ux2,
+                                            float uy2, float mx2, float my2, float ux3, float uy3, float mx3, float my3,
                                             double& Fx, double& Fy) {
     const int i = tb.gi(I_NODEI, li), j = tb.gi(I_NODEJ, li);
     float g[Q];
-    gather(p, i, j, g);
+    if (PRE) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) g[k] = gpre[k];
+    } else {
+        gather(p, i, j, g);
+    }
     Mac m = moments(p, g);
     float mxxp = 0.f, myyp = 0.f;
     const float t2 = tb.gf(G_T2, li), t3 = tb.gf(G_T3, li);
@@ -325,8 +330,15 @@ struct PhysicsT {
     static __device__ __forceinline__ void boundary_close(const P& p, const BTab<T>& tb, int li, int l, T ux2, T uy2,
                                                           T mx2, T my2, T ux3, T uy3, T mx3, T my3, double& Fx,
                                                           double& Fy) {
-        fp32::boundary_close<FULL>(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
+        fp32::boundary_close<FULL, false>(p, tb, li, l, nullptr, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
+    static __device__ __forceinline__ void boundary_close_pre(const P& p, const BTab<T>& tb, int li, int l, const T g[Q],
+                                                              T ux2, T uy2, T mx2, T my2, T ux3, T uy3, T mx3, T my3,
+                                                              double& Fx, double& Fy) {
+        fp32::boundary_close<FULL, true>(p, tb, li, l, g, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
+    }
+    // registers per thread a kernel needs before its wall node's populations are gathered ahead
+    static constexpr int WIDE_REGS = 96;
 };
 using Physics = PhysicsT<true>;
 using PhysicsLean = PhysicsT<false>;

@@ -223,8 +223,8 @@ __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, double 
 }
 
 // Rotated closures, 2d_mrlbm.f90:1635-1765 (strong), 1873-1972 (rhoeq), 1767-1871 (weak).
-__device__ __noinline__ void closure_rotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp, double uyp,
-                                             double Mxx, double Myy, Mac& m) {
+__device__ __forceinline__ void closure_rotated_body(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp,
+                                                     double uyp, double Mxx, double Myy, Mac& m) {
     const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     const double omega = p.omega;
     const int variant = p.closure;
@@ -288,6 +288,11 @@ __device__ __noinline__ void closure_rotated(const P& p, const BTab<double>& tb,
     m.mxy = (Mxx - Myy) * 0.50 * s2 + Mxy * c2;
 }
 
+__device__ __noinline__ void closure_rotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp, double uyp,
+                                             double Mxx, double Myy, Mac& m) {
+    closure_rotated_body(p, tb, li, f, uxp, uyp, Mxx, Myy, m);
+}
+
 // Unrotated closure with Cramer's rule, 2d_mrlbm.f90:1496-1633 and 1974-2003.
 __device__ __noinline__ void closure_unrotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp,
                                                double uyp, Mac& m) {
@@ -339,14 +344,22 @@ __device__ __noinline__ void closure_unrotated(const P& p, const BTab<double>& t
 
 // Lane 0 of a boundary node: extrapolated velocity / rotated moments from the reference
 // points (the wall value is 0; 2d_mrlbm.f90:809-814, 919-924), closure, collision, store,
-// momentum-exchange force (evaluate_forces, 2d_mrlbm.f90:558-591).
-template <bool FULL>
-__device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, int li, int l, double ux2, double uy2,
-                                            double mx2, double my2, double ux3, double uy3, double mx3, double my3,
-                                            double& Fx, double& Fy) {
+// momentum-exchange force (evaluate_forces, 2d_mrlbm.f90:558-591).  PRE: the node's
+// populations were gathered by the caller (fpre) and every call below is inlined, so nothing
+// of the node goes through local memory; without PRE (kernels with few registers per thread)
+// the node gathers its own populations and the closures stay out of line.
+template <bool FULL, bool PRE>
+__device__ __forceinline__ void boundary_close_core(const P& p, const BTab<double>& tb, int li, int l, const double* fpre,
+                                                    double ux2, double uy2, double mx2, double my2, double ux3, double uy3,
+                                                    double mx3, double my3, double& Fx, double& Fy) {
     const int i = tb.gi(I_NODEI, li), j = tb.gi(I_NODEJ, li);
     double f[Q];
-    gather(p, i, j, f);
+    if (PRE) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) f[k] = fpre[k];
+    } else {
+        gather(p, i, j, f);
+    }
     Mac m = moments(f, p.hm, p.hp);
     const bool rotated = p.closure != CLOSURE_UNROTATED;
     double mxxp = 0.0, myyp = 0.0;
@@ -364,7 +377,8 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
             const double c = tb.gf(G_CTH, li), s = tb.gf(G_STH, li);
             const double uxp = m.ux * c + m.uy * s;    // 2d_mrlbm.f90:304-305
             const double uyp = m.uy * c - m.ux * s;
-            closure_rotated(p, tb, li, f, uxp, uyp, mxxp, myyp, m);
+            if (PRE) closure_rotated_body(p, tb, li, f, uxp, uyp, mxxp, myyp, m);
+            else closure_rotated(p, tb, li, f, uxp, uyp, mxxp, myyp, m);
         }
     } else {
         closure_unrotated(p, tb, li, f, m.ux, m.uy, m);
@@ -385,6 +399,13 @@ __device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, 
     Fx = fxi - fxo;
     Fy = fyi - fyo;
     if (p.node_force) { p.node_force[2 * l] = Fx; p.node_force[2 * l + 1] = Fy; }
+}
+
+template <bool FULL>
+__device__ __noinline__ void boundary_close(const P& p, const BTab<double>& tb, int li, int l, double ux2, double uy2,
+                                            double mx2, double my2, double ux3, double uy3, double mx3, double my3,
+                                            double& Fx, double& Fy) {
+    boundary_close_core<FULL, false>(p, tb, li, l, nullptr, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
 }
 
 // Edge nodes (first/last row or column): own gather, Dirichlet values and closures.  Inline,
@@ -455,6 +476,13 @@ struct PhysicsT {
                                                           double& Fy) {
         fp64::boundary_close<FULL>(p, tb, li, l, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
     }
+    static __device__ __forceinline__ void boundary_close_pre(const P& p, const BTab<T>& tb, int li, int l, const T f[Q],
+                                                              T ux2, T uy2, T mx2, T my2, T ux3, T uy3, T mx3, T my3,
+                                                              double& Fx, double& Fy) {
+        fp64::boundary_close_core<FULL, true>(p, tb, li, l, f, ux2, uy2, mx2, my2, ux3, uy3, mx3, my3, Fx, Fy);
+    }
+    // registers per thread a kernel needs before its wall-node path is inlined (boundary_close_pre)
+    static constexpr int WIDE_REGS = 128;
 };
 using Physics = PhysicsT<true>;
 using PhysicsLean = PhysicsT<false>;

@@ -72,6 +72,14 @@ struct alignas(64) StepParams {
     double* partials;             // per-step scratch: Fx[nb], Fy[nb], rho(1,j)[ny]
     unsigned* counter;            // [0] arrivals of boundary blocks, [1] of inlet edge blocks (reset by the last)
     double* rec;                  // REC_WORDS doubles for this step, or null
+    // Deferred record sums (single-case steps): with defer set, a stats step leaves its terms in
+    // `partials` and no block of it waits for the others to sum them; the next launch's first
+    // edge block (or the finishing kernel, launch_finish_record) sums them in index order into
+    // prev_rec, taking the in-order sums off the step's critical path.
+    int defer;
+    const double* prev_partials;  // terms of the last stats step still to be summed, or null
+    double* prev_rec;             // its record
+    int prev_iter;
     double* node_force;           // optional per-boundary-node (Fx, Fy) [2 * nb], or null
     int iter;
     int* errflag;
@@ -169,6 +177,9 @@ inline bool is_vec_cfg(int c) { return c >= VEC_CFG0 && c < PIPE_CFG0; }
 // shape does not fit this precision.
 int launch_step_f64(const StepParams<double>& p, int tile_cfg, void* stream, int workers);
 int launch_step_f32(const StepParams<float>& p, int tile_cfg, void* stream, int workers);
+// Record (iter, sum Fx, sum Fy, sum rho(1,:)) of a stats step run with deferred sums, from its
+// terms (Fx[nb], Fy[nb], rho(1,j)[ny]), summed in index order by one small launch.
+int launch_finish_record(const double* partials, int nb, int ny, int halo_l, double* rec, int iter, void* stream);
 // Halo-face columns of an x-slab ahead of its step (face_kernel, step_common.cuh).
 int launch_face_f64(const StepParams<double>& p, bool full, void* stream);
 int launch_face_f32(const StepParams<float>& p, bool full, void* stream);

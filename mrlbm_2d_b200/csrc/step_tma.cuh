@@ -152,10 +152,8 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
         const int i = 1 + tx * BX + tid;
         // a tile with no edge, ghost or cylinder-box node goes back through tensor stores
         const int i0 = 1 + tx * BX, j0 = 1 + ty * BY;
-        const bool full = STORE && col_interior(p, i0) && i0 + BX - 1 <= nx && col_interior(p, i0 + BX - 1) &&
-                          j0 > 1 && j0 + BY - 1 < ny &&
-                          (i0 + BX - 1 < p.box_x0 || i0 >= p.box_x0 + p.box_w || j0 + BY - 1 < p.box_y0 ||
-                           j0 >= p.box_y0 + p.box_h);
+        const bool plain = plain_tile(p, i0, i0 + BX - 1, j0, j0 + BY - 1);
+        const bool full = STORE && plain;
         if (full) {
             if (tid == 0) bulk_wait_read_all();               // the previous tile's stores have read `out`
             __syncthreads();
@@ -175,9 +173,12 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
                 for (int k = 0; k < Q; ++k) out[(k * G::OUT_PLANE) / (int)sizeof(T) + r * BX + tid] = fo[k];
                 continue;
             }
-            const int cls = node_class(p, i, j);
-            if (cls >= 0) continue;                           // curved-wall node
-            if (!is_interior(p, i, j)) continue;            // edge blocks
+            int cls = CLS_FLUID;
+            if (!plain) {
+                cls = node_class(p, i, j);
+                if (cls >= 0) continue;                       // curved-wall node
+                if (!is_interior(p, i, j)) continue;        // edge blocks
+            }
 #pragma unroll
             for (int k = 0; k < Q; ++k)
                 f[k] = st[(k * G::PLANE_BYTES) / (int)sizeof(T) + r * G::W + tid + G::M - ex(k)];
@@ -205,7 +206,7 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
 template <class Phys, int BX, int BY, int STAGES, bool STORE>
 __global__ void __launch_bounds__(BX, 1) step_kernel_tma(const __grid_constant__ typename Phys::P p) {
     if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys>(p)) return;
+    if (run_aux_block<Phys, wide_wall<Phys>(BX, 1)>(p)) return;
     tma_bulk_worker<Phys, BX, BY, STAGES, STORE>(p);
 }
 

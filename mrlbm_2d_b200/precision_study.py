@@ -68,23 +68,17 @@ def spectral_strouhal(fl, D, U, rho_infty=1.0, pad=16):
     return f * D / U
 
 
-def main(argv=None):
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="small", choices=sorted(CASES))
-    ap.add_argument("--steps", type=int, default=20000)
-    ap.add_argument("--stats-from", type=int, default=None, help="first step of the statistics window")
-    ap.add_argument("--fields", action="store_true",
-                    help="also accumulate FP64 mean/rms fields of u, v, p over the statistics window")
-    a = ap.parse_args(argv)
-    cfg = CASES[a.case]()
-    start = a.stats_from if a.stats_from is not None else a.steps // 2
-    cfg = cfg.replace(statsbegin=start, statsend=a.steps + 10)
-    out = {"case": a.case, "nx": cfg.nx, "ny": cfg.ny, "steps": a.steps, "stats_from": start,
+def study(case="small", steps=20000, stats_from=None, fields=False, chunk=5000):
+    """Both precisions on one case; returns the comparison as a dict (see the module text)."""
+    cfg = CASES[case]()
+    start = stats_from if stats_from is not None else steps // 2
+    cfg = cfg.replace(statsbegin=start, statsend=steps + 10)
+    out = {"case": case, "nx": cfg.nx, "ny": cfg.ny, "steps": steps, "stats_from": start,
            "D": 2 * cfg.r_c, "U": cfg.uo, "Re": cfg.Re}
     res = {}
     for prec in (64, 32):
-        fd, fl, mac, mlups, fields = run(cfg, prec, a.steps, fields_from=start if a.fields else None)
-        res.setdefault("fields", {})[prec] = fields
+        fd, fl, mac, mlups, flds = run(cfg, prec, steps, chunk=chunk, fields_from=start if fields else None)
+        res.setdefault("fields", {})[prec] = flds
         r = {"mlups_wall": mlups}
         try:
             s = api.force_statistics(fd, fl, cfg.r_c, cfg.uo, 1.0)
@@ -106,13 +100,25 @@ def main(argv=None):
     out["velocity_rel_l2"] = float(np.sqrt((du ** 2).sum() / (u64 ** 2).sum()))
     out["velocity_max_abs_over_U"] = float(du.max() / cfg.uo)
     out["drag_history_rel_l2"] = float(np.linalg.norm(fd32 - fd64) / np.linalg.norm(fd64))
-    if a.fields:
+    if fields:
         f32, f64 = res["fields"][32], res["fields"][64]
         for k in ("mean_u", "mean_v", "mean_p", "rms_u", "rms_v", "rms_p"):
             ref = f64[k] - (1.0 / 3.0 if k == "mean_p" else 0.0)   # p relative to rest pressure
             out[f"{k}_rel_l2"] = float(np.linalg.norm(f32[k] - f64[k]) / max(np.linalg.norm(ref), 1e-300))
             out[f"{k}_max_abs"] = float(np.abs(f32[k] - f64[k]).max())
         out["field_samples"] = int(f64["n"])
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="small", choices=sorted(CASES))
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--stats-from", type=int, default=None, help="first step of the statistics window")
+    ap.add_argument("--fields", action="store_true",
+                    help="also accumulate FP64 mean/rms fields of u, v, p over the statistics window")
+    a = ap.parse_args(argv)
+    out = study(a.case, a.steps, a.stats_from, a.fields)
     print(json.dumps(out), flush=True)
     return out
 
