@@ -16,6 +16,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libmrlbm.so")
 DRIVER = os.path.join(PKG, "mrlbm_run")
+STATS = os.path.join(PKG, "mrlbm_statistics")
 BUILD = os.path.join(PKG, "_build")
 ROOT = os.path.dirname(PKG)
 
@@ -48,7 +49,7 @@ def _sources():
 
 
 def up_to_date():
-    if not os.path.exists(OUT) or not os.path.exists(DRIVER):
+    if not os.path.exists(OUT) or not os.path.exists(DRIVER) or not os.path.exists(STATS):
         return False
     t = os.path.getmtime(OUT)
     return all(os.path.getmtime(s) <= t for s in _sources())
@@ -86,6 +87,11 @@ def build(force=False, verbose=False):
     subprocess.run(["g++", "-std=c++17", "-O2", "-c", os.path.join(CSRC, "driver_main.cpp"), "-o", drv_obj],
                    check=True)
     subprocess.run(["g++", "-o", DRIVER, drv_obj, "-L" + PKG, "-lmrlbm", "-Wl,-rpath,$ORIGIN"], check=True)
+    # the input_stat.dat-driven post-processing driver (mrlbm_statistics) over the same ABI
+    st_obj = os.path.join(BUILD, "stats_main.cpp.o")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-c", os.path.join(CSRC, "stats_main.cpp"), "-o",
+                    st_obj], check=True)
+    subprocess.run(["g++", "-o", STATS, st_obj, "-L" + PKG, "-lmrlbm", "-Wl,-rpath,$ORIGIN"], check=True)
     return OUT
 
 

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../../include/mrlbm.h"
+#include "fortran_io.h"
 
 namespace {
 
@@ -38,73 +39,6 @@ void die(const char* what, int rc, mrlbm_handle* h) {
     mrlbm_last_error(h, buf, sizeof buf);
     std::fprintf(stderr, "%s failed (%d): %s\n", what, rc, buf);
     std::exit(1);
-}
-
-// Fortran unformatted sequential record: 4-byte length markers around the data; records
-// longer than 2147483639 bytes are split into subrecords the way gfortran does (leading
-// marker negative when the record continues, trailing marker negative when the subrecord
-// continues a previous one).
-struct FortranWriter {
-    FILE* f = nullptr;
-    std::vector<char> rec;
-    explicit FortranWriter(const std::string& path, const char* mode = "wb") { f = std::fopen(path.c_str(), mode); }
-    ~FortranWriter() { if (f) std::fclose(f); }
-    template <class T> void put(const T* p, size_t n) {
-        const char* c = (const char*)p;
-        rec.insert(rec.end(), c, c + n * sizeof(T));
-    }
-    template <class T> void put1(T v) { put(&v, 1); }
-    void end_record() {
-        const size_t maxsub = 2147483639u;
-        size_t off = 0, total = rec.size();
-        bool first = true;
-        do {
-            const size_t len = std::min(maxsub, total - off);
-            const bool more = off + len < total;
-            const int32_t lead = more ? -(int32_t)len : (int32_t)len;
-            const int32_t trail = first ? (int32_t)len : -(int32_t)len;
-            std::fwrite(&lead, 4, 1, f);
-            if (len) std::fwrite(rec.data() + off, 1, len, f);
-            std::fwrite(&trail, 4, 1, f);
-            off += len;
-            first = false;
-        } while (off < total);
-        rec.clear();
-    }
-};
-
-bool read_fortran_record(FILE* f, std::vector<char>& out) {
-    out.clear();
-    while (true) {
-        int32_t lead;
-        if (std::fread(&lead, 4, 1, f) != 1) return false;
-        const size_t len = (size_t)std::abs(lead);
-        const size_t at = out.size();
-        out.resize(at + len);
-        if (len && std::fread(out.data() + at, 1, len, f) != len) return false;
-        int32_t trail;
-        if (std::fread(&trail, 4, 1, f) != 1) return false;
-        if (lead >= 0) return true;
-    }
-}
-
-// list-directed output of gfortran: integers in width 12, REAL(8) as 17 significant digits
-std::string ld_int(long long v) {
-    char b[32];
-    std::snprintf(b, sizeof b, "%12lld", v);
-    return b;
-}
-std::string ld_real(double v) {
-    char b[64];
-    const double a = std::fabs(v);
-    if (v == 0.0 || (a >= 0.1 && a < 1e16)) {
-        int digits_before = v == 0.0 ? 1 : (int)std::floor(std::log10(a)) + 1;
-        if (digits_before < 1) digits_before = 1;
-        std::snprintf(b, sizeof b, "%25.*f     ", std::max(0, 17 - digits_before), v);
-    } else {
-        std::snprintf(b, sizeof b, "%26.16E", v);
-    }
-    return b;
 }
 
 void mkdirs() {
