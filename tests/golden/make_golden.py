@@ -2,9 +2,12 @@
 
     python tests/golden/make_golden.py [--only NAME]
 
-Reads 2d_mrlbm.f90 from the reference checkout (REFERENCE_DIR, default /root/reference),
-runs it with tests/golden/fortran_subset.py on small inputs the unmodified reference can
-express, and writes tests/golden/<case>.npz.  Each case is an input.dat (written below)
+Reads 2d_mrlbm.f90 and 2d_statistics.f90 from the reference checkout named by the
+REFERENCE_DIR environment variable (required), runs them with tests/golden/fortran_subset.py on
+small inputs the unmodified reference can express, and writes tests/golden/<case>.npz.  Every
+random input is drawn from a generator keyed by a stable function of the case name, and the
+archives are written with fixed member timestamps, so a second run reproduces the committed
+files byte for byte.  Each case is an input.dat (written below)
 plus, for the restart cases, a restart.dat record (soln_time, f, f_eq, ux, uy, rho) that
 the reference reads through its own irestart = 1 path (2d_mrlbm.f90:208-212, 2204-2220), so
 the curved-wall closure runs on a developed, non-symmetric flow from the first step.
@@ -19,9 +22,12 @@ Captured outputs (the reference's own files, as records of values):
 The fixtures are committed; this script is only re-run when the cases change.
 """
 import argparse
+import io
 import os
 import sys
 import time
+import zipfile
+import zlib
 
 import numpy as np
 
@@ -29,7 +35,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 from fortran_subset import Interpreter  # noqa: E402
 
-REF = os.environ.get("REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("REFERENCE_DIR")
+
+
+def reference_source(name):
+    if not REF:
+        raise SystemExit("set REFERENCE_DIR to the reference checkout (the directory holding 2d_mrlbm.f90)")
+    return open(os.path.join(REF, name)).read()
+
+
+def save_npz(path, **arrays):
+    """np.savez_compressed with fixed member timestamps (byte-reproducible archives)."""
+    with zipfile.ZipFile(path, "w", compression=zipfile.ZIP_DEFLATED) as z:
+        for key in sorted(arrays):
+            buf = io.BytesIO()
+            np.lib.format.write_array(buf, np.asanyarray(arrays[key]), allow_pickle=False)
+            info = zipfile.ZipInfo(key + ".npy", date_time=(1980, 1, 1, 0, 0, 0))
+            info.compress_type = zipfile.ZIP_DEFLATED
+            info.external_attr = 0o600 << 16
+            z.writestr(info, buf.getvalue())
 
 INPUT = """&DomainSize
 \tnx = 16
@@ -98,7 +122,7 @@ CASES = {
 def restart_state(case, nx, ny):
     """A seeded, developed-looking population field: regularized equilibrium of a
     perturbed uniform flow (rho = 1 + 1e-2 n, u = U + 0.2 U n, v = 0.2 U n)."""
-    rng = np.random.default_rng(abs(hash(case)) % (2 ** 32))
+    rng = np.random.default_rng(zlib.crc32(case.encode()))      # stable across processes
     U = 0.05
     rho = 1.0 + 1e-2 * rng.standard_normal((nx, ny))
     u = U + 0.2 * U * rng.standard_normal((nx, ny))
@@ -117,7 +141,7 @@ def restart_state(case, nx, ny):
 
 def run_case(name, over):
     prm = dict(BASE, **over)
-    src = open(os.path.join(REF, "2d_mrlbm.f90")).read()
+    src = reference_source("2d_mrlbm.f90")
     text = INPUT.format(**prm)
     ncy = prm["ncy"]
     nx = (prm["L_front"] + 1 + prm["L_back"]) * ncy
@@ -132,7 +156,8 @@ def run_case(name, over):
     it.run()
     el = time.time() - t0
     files = it.files
-    out = {"input_dat": np.array(text), "nx": nx, "ny": ny, "elapsed_s": el}
+    out = {"input_dat": np.array(text), "nx": nx, "ny": ny}
+    print(f"{name}: interpreted in {el:.1f} s", flush=True)
     if f0 is not None:
         out["restart_in_f"] = f0
         out["restart_in_iter"] = 0
@@ -176,8 +201,8 @@ def main():
             continue
         out = run_case(name, over)
         path = os.path.join(HERE, name + ".npz")
-        np.savez_compressed(path, **out)
-        print(f"{name}: {out['elapsed_s']:.1f} s, {len(out['forces'])} force records -> {path}", flush=True)
+        save_npz(path, **out)
+        print(f"{name}: {len(out['forces'])} force records -> {path}", flush=True)
 
 
 if __name__ == "__main__" and "--stats" not in sys.argv:
@@ -203,7 +228,7 @@ def run_stats_case(name, prm):
     theta = np.sort(rng.uniform(0, 2 * np.pi, nbct))
     ps = (1.0 / 3.0) * (1 + 1e-3 * rng.standard_normal((nstep, nbct)))
     psf = ps + 1e-5 * rng.standard_normal((nstep, nbct))
-    src = open(os.path.join(REF, "2d_statistics.f90")).read()
+    src = reference_source("2d_statistics.f90")
     text = (f"&parameters\n\tnbct = {nbct}\n\tr_cy = {r_cy!r}\n\tuo = {uo!r}\n\trho_infty = {rho_inf!r}\n/\n")
     it = Interpreter(src, inputs={"input_stat.dat": text})
     it.text_records["data_mean/forces_time.dat"] = [[int(a), float(b), float(c)] for a, b, c in zip(t, fd, fl)]
@@ -229,7 +254,7 @@ def main_stats(only=None):
         if only and name != only:
             continue
         out = run_stats_case(name, prm)
-        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        save_npz(os.path.join(HERE, name + ".npz"), **out)
         print(f"{name}: St={out['St']:.6f} Cd={out['Cd']:.6f} Cl_rms={out['Cl_rms']:.6f}", flush=True)
 
 
