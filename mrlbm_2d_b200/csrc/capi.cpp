@@ -456,9 +456,9 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         }
         rc = launch_step_f32(p, tc, h->stream, h->workers);
     }
-    ++h->launches;
+    h->launches += 2;                                  // the step's auxiliary and bulk launches
     if (rc == -2) {
-        --h->launches;
+        h->launches -= 2;
         return fail(h, MRLBM_EUNSUPPORTED, "tile shape does not fit this precision");
     }
     if (rc != 0) {
@@ -678,7 +678,7 @@ static int create_impl(const mrlbm_config* cfg, int precision, int device, int s
     const size_t nscratch = 2 * (size_t)nb + (size_t)ny + 8;
     h->partials_n = nscratch;
     ok = ok && ck(cudaMalloc((void**)&h->d_partials, 2 * nscratch * sizeof(double)), "cudaMalloc partials") &&
-         ck(cudaMalloc((void**)&h->d_counter, 2 * sizeof(unsigned)), "cudaMalloc counter") &&
+         ck(cudaMalloc((void**)&h->d_counter, 3 * sizeof(unsigned)), "cudaMalloc counter") &&
          ck(cudaMalloc((void**)&h->d_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMalloc ring") &&
          ck(cudaMalloc((void**)&h->d_err, sizeof(int)), "cudaMalloc err") &&
          ck(cudaMallocHost((void**)&h->h_ring, (size_t)RING_CAP * REC_WORDS * sizeof(double)), "cudaMallocHost ring");
@@ -695,7 +695,7 @@ static int create_impl(const mrlbm_config* cfg, int precision, int device, int s
     if (!h->geo.boxmap.empty())
         ok = ok && ck(cudaMemcpy(h->d_boxmap, h->geo.boxmap.data(), h->geo.boxmap.size() * sizeof(int),
                                  cudaMemcpyHostToDevice), "upload boxmap");
-    ok = ok && ck(cudaMemset(h->d_counter, 0, 2 * sizeof(unsigned)), "memset") && ck(cudaMemset(h->d_err, 0, sizeof(int)), "memset");
+    ok = ok && ck(cudaMemset(h->d_counter, 0, 3 * sizeof(unsigned)), "memset") && ck(cudaMemset(h->d_err, 0, sizeof(int)), "memset");
     if (!ok) { std::string m = g_create_error; return bail(MRLBM_ECUDA, m); }
     std::vector<double> f0;
     initial_state(h->cfg, h->lat, gnx, ny, f0);
@@ -1447,7 +1447,7 @@ int adj_forward(mrlbm_handle* h, const void* src, void* dst, int iter, double* r
     p.do_stats = rec != nullptr;
     p.rec = rec;
     p.iter = iter;
-    ++h->launches;
+    h->launches += 2;
     if (sizeof(T) == 8) return launch_step_f64(reinterpret_cast<const StepParams<double>&>(p), tile, st, 0);
     return launch_step_f32(reinterpret_cast<const StepParams<float>&>(p), tile, st, 0);
 }

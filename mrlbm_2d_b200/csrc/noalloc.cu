@@ -36,7 +36,7 @@ static __device__ __align__(256) double na_geo[G_NFIELDS * NA_MAX_NB];        //
 static __device__ __align__(256) int na_int[I_NFIELDS * NA_MAX_NB];
 static __device__ __align__(256) int na_box[NA_MAX_BOX];
 static __device__ __align__(256) double na_partials[2 * NA_MAX_NB + NA_MAX_NY];
-static __device__ __align__(256) unsigned na_counter[2];
+static __device__ __align__(256) unsigned na_counter[3];
 static __device__ __align__(256) int na_err[1];
 static __device__ __align__(256) double na_ring[REC_WORDS * NA_RING];
 static __device__ __align__(256) OvrEntry na_ovr[NA_MAX_OVR];
@@ -131,7 +131,7 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
     if (e == cudaSuccess && !g.boxmap.empty())
         e = cudaMemcpyAsync(S->box, g.boxmap.data(), g.boxmap.size() * sizeof(int), cudaMemcpyHostToDevice, st);
     // the arrays keep the previous call's contents: clear what must start at zero
-    if (e == cudaSuccess) e = cudaMemsetAsync(S->counter, 0, 2 * sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S->counter, 0, 3 * sizeof(unsigned), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->err, 0, sizeof(int), st);
     if (e != cudaSuccess) { err = std::string("upload: ") + cudaGetErrorString(e); return MRLBM_ECUDA; }
     void* half[2] = {d_state, (char*)d_state + (size_t)c.L.total() * elem};
@@ -209,7 +209,7 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
             p.n_ovr = ovr_live ? n_ovr : 0;
             rc = launch_step_f32(p, c.tile_cfg, st, 0);
         }
-        ++c.launches;
+        c.launches += 2;
         if (rc != 0) { err = std::string("kernel launch failed: ") + cudaGetErrorString(cudaGetLastError()); return MRLBM_ECUDA; }
         ovr_live = false;
         c.cur ^= 1;

@@ -309,7 +309,9 @@ __device__ __forceinline__ void inlet_tail(const typename Phys::P& p, unsigned c
 
 // WIDE: the kernel has registers enough (Phys::WIDE_REGS per thread) for lane 0 to gather its
 // node's own populations together with its stencil node's, and for the closure to be inlined.
-template <class Phys, bool WIDE>
+// WAIT: the block itself waits for the previous step after staging its (creation-time) tables;
+// otherwise the kernel waited before calling it.
+template <class Phys, bool WIDE, bool WAIT>
 __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsigned char* smem, int bb) {
     using T = typename Phys::T;
     T* sg = reinterpret_cast<T*>(smem);                               // G_STAGED * BNODES
@@ -357,7 +359,7 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
     }
     // The tables are written once, when the handle is created, so the staging above may run
     // while the previous step finishes; everything below reads or writes what steps change.
-    wait_prior_grid();
+    if (WAIT) wait_prior_grid();
     __syncthreads();
     const BTab<T> tb{sg, sgi, bn};
     T fown[Q];
@@ -433,9 +435,9 @@ constexpr int aux_smem_bytes() {
 }
 
 // Auxiliary work item b of a step: boundary block b (b < nbblk) or edge block b - nbblk.
-template <class Phys, bool WIDE>
+template <class Phys, bool WIDE, bool WAIT = true>
 __device__ __forceinline__ void aux_item(const typename Phys::P& p, unsigned char* smem, int b) {
-    if (b < p.nbblk) boundary_block<Phys, WIDE>(p, smem, b);
+    if (b < p.nbblk) boundary_block<Phys, WIDE, WAIT>(p, smem, b);
     else edge_block<Phys>(p, b - p.nbblk, smem);
 }
 
@@ -443,21 +445,53 @@ __device__ __forceinline__ void aux_item(const typename Phys::P& p, unsigned cha
 template <class Phys>
 constexpr bool wide_wall(int threads, int minb) { return 65536 / (threads * minb) >= Phys::WIDE_REGS; }
 
-// Boundary and edge blocks sit at the start of the grid.  True when this block is one of them
-// (and has done its work); bulk tile t is then blockIdx.x - nbblk - neblk.
-template <class Phys, bool WIDE>
-__device__ __forceinline__ bool run_aux_block(const typename Phys::P& p) {
+// ---- one time step as two launches ---------------------------------------------------------
+// A step is an auxiliary launch (aux_kernel: the curved-wall boundary blocks, then the domain-edge
+// blocks) followed by a bulk launch (every interior node by tiles of one shape); both write the
+// next time level at disjoint nodes and read the previous one.  Each has its own register budget
+// and instruction footprint, so the wall-node closures cost the bulk tiles nothing.  Ordering
+// with programmatic dependent launch, per step n (A = auxiliary, B = bulk):
+//   * A(n): every block waits for its predecessor in the stream (B(n-1), or whatever the caller
+//     put in between) to complete, then allows B(n) to launch, then works;
+//   * B(n): launches once every A(n) block has waited, hence after B(n-1) completed; it does
+//     not wait itself, so its tiles run beside the wall-node chain.  It allows the next launch
+//     (A(n+1)) at once, and the last of its blocks to finish waits for A(n) to complete, so
+//     B(n) completes only after A(n): whatever follows B(n) in the stream sees the whole step.
+constexpr int AUX_THREADS = 128;
+
+template <class Phys>
+__global__ void __launch_bounds__(AUX_THREADS) aux_kernel(const __grid_constant__ typename Phys::P p) {
     __shared__ __align__(16) unsigned char smem[aux_smem_bytes<typename Phys::T>()];
-    const int b = (int)blockIdx.x;
-    if (b >= p.nbblk + p.neblk) return false;
-    aux_item<Phys, WIDE>(p, smem, b);
-    return true;
+    wait_prior_grid();
+    aux_item<Phys, true, false>(p, smem, (int)blockIdx.x);
 }
+
+// Start of a bulk launch: let the next launch (the next step's auxiliary blocks) be scheduled.
+__device__ __forceinline__ void bulk_begin() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// End of a bulk block: the last block of the launch to get here waits for the step's auxiliary
+// launch to complete (counter[2] counts the bulk blocks; the last one resets it).
+template <class T>
+__device__ __forceinline__ void bulk_end(const StepParams<T>& p) {
+    if (threadIdx.x == 0 && atomicAdd(p.counter + 2, 1u) == gridDim.x - 1) {
+        p.counter[2] = 0u;
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+    }
+}
+
 
 template <class P>
 inline int edge_blocks(const P& p, int nthr) {
     const int n = 2 * p.L.nx + (p.halo_l ? 0 : p.L.ny - 2) + (p.halo_r ? 0 : p.L.ny - 2);
     return (n + nthr - 1) / nthr;
+}
+
+template <class Phys>
+inline int launch_aux(typename Phys::P p, cudaStream_t s) {
+    const int bn = AUX_THREADS / BLANES;
+    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
+    p.neblk = edge_blocks(p, AUX_THREADS);
+    return launch_after_prior(aux_kernel<Phys>, (unsigned)(p.nbblk + p.neblk), AUX_THREADS, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 
 // True when every node of columns i0..i1 and rows j0..j1 is an interior bulk node: no domain
@@ -478,16 +512,13 @@ __device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, i
     for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
 }
 
-// One time step.  Blocks [0, nbblk) are boundary blocks, the next neblk edge blocks; the rest are bulk tiles of
-// BX x (BY*NJ) nodes, one thread per column and NJ rows.  A thread first issues the loads of
-// all its interior rows, then finishes them (collide and store) one by one, so up to 9*NJ
-// loads per thread are in flight.
-template <class Phys, int BX, int BY, int NJ, int MINB>
-__global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
+// Bulk tiles of BX x (BY*NJ) nodes, one thread per column and NJ rows, one tile per block.  A
+// thread first issues the loads of all its interior rows, then finishes them (collide and store)
+// one by one, so up to 9*NJ loads per thread are in flight.
+template <class Phys, int BX, int BY, int NJ>
+__device__ __forceinline__ void tile_body(const typename Phys::P& p) {
     using T = typename Phys::T;
-    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys, wide_wall<Phys>(BX * BY, MINB)>(p)) return;
-    const int t = blockIdx.x - p.nbblk - p.neblk;
+    const int t = blockIdx.x;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
     const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
     const int i = 1 + tx * BX + lx;
@@ -522,6 +553,13 @@ __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_consta
         const int j = 1 + ty * BY * NJ + r * BY + ly;
         if ((interior >> r) & 1u) Phys::finish(p, i, j, cls[r], f[r]);    // edge nodes: edge blocks
     }
+}
+
+template <class Phys, int BX, int BY, int NJ, int MINB>
+__global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
+    bulk_begin();
+    tile_body<Phys, BX, BY, NJ>(p);
+    bulk_end(p);
 }
 
 // ---- 128-bit vector bulk path -------------------------------------------------------------
@@ -631,9 +669,9 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
 
 template <class Phys, int WARPS, int NJ, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_vec(const __grid_constant__ typename Phys::P p) {
-    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys, wide_wall<Phys>(WARPS * 32, MINB)>(p)) return;
-    vec_tile<Phys, WARPS, NJ>(p, (int)blockIdx.x - p.nbblk - p.neblk);
+    bulk_begin();
+    vec_tile<Phys, WARPS, NJ>(p, (int)blockIdx.x);
+    bulk_end(p);
 }
 
 template <class Phys, int WARPS, int NJ, int MINB>
@@ -641,13 +679,11 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
     using T = typename Phys::T;
     constexpr int VW = Vec16<T>::N;
     const int nthr = WARPS * 32;
-    static_assert(WARPS * 32 % BLANES == 0 && WARPS * 32 / BLANES <= BNODES, "boundary block size");
-    const int bn = nthr / BLANES;
-    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p, nthr);
+    if (launch_aux<Phys>(p, s) != 0) return -1;
+    p.nbblk = p.neblk = 0;
     p.tiles_x = (p.L.nx + 32 * VW - 1) / (32 * VW);
     const int tiles_y = (p.L.ny + WARPS * NJ - 1) / (WARPS * NJ);
-    const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
+    const long long nblocks = (long long)p.tiles_x * tiles_y;
     return launch_after_prior(step_kernel_vec<Phys, WARPS, NJ, MINB>, (unsigned)nblocks, nthr, 0, s, p) == cudaSuccess ? 0
                                                                                                             : -1;
 }
@@ -658,14 +694,12 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
 // thread loads the populations of its next node before it collides and stores the current
 // one, so a load is always in flight behind the arithmetic and no block waits out a tail
 // wave.  Edge and wall nodes are skipped (edge and boundary blocks own them).
-template <class Phys, int B, int MINB>
-__global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constant__ typename Phys::P p) {
+template <class Phys, int B>
+__device__ __forceinline__ void pipe_body(const typename Phys::P& p) {
     using T = typename Phys::T;
-    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys, wide_wall<Phys>(B, MINB)>(p)) return;
     const int nx = p.L.nx, ny = p.L.ny, tiles_x = p.tiles_x;
     const int units = tiles_x * ny;
-    const int G = (int)gridDim.x - p.nbblk - p.neblk;
+    const int G = (int)gridDim.x;
     auto fetch = [&](int u, T (&f)[Q], int& i, int& j) -> bool {
         if (u >= units) return false;
         j = 1 + u / tiles_x;
@@ -674,7 +708,7 @@ __global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constan
         gather_interior(p, i, j, f);
         return true;
     };
-    int u = (int)blockIdx.x - p.nbblk - p.neblk;
+    int u = (int)blockIdx.x;
     T a[Q], b[Q];
     int ia = 0, ja = 0, ib = 0, jb = 0;
     bool va = fetch(u, a, ia, ja);
@@ -695,8 +729,14 @@ __global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constan
 }
 
 template <class Phys, int B, int MINB>
+__global__ void __launch_bounds__(B, MINB) step_kernel_pipe(const __grid_constant__ typename Phys::P p) {
+    bulk_begin();
+    pipe_body<Phys, B>(p);
+    bulk_end(p);
+}
+
+template <class Phys, int B, int MINB>
 int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
-    static_assert(B % BLANES == 0 && B / BLANES <= BNODES, "boundary block size");
     static int per_sm[64] = {0}, sms[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -707,15 +747,12 @@ int launch_step_pipe(typename Phys::P p, cudaStream_t s) {
                 cudaSuccess || per_sm[dev] <= 0)
             return -1;
     }
-    const int bn = B / BLANES;
-    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p, B);
+    if (launch_aux<Phys>(p, s) != 0) return -1;
+    p.nbblk = p.neblk = 0;
     p.tiles_x = (p.L.nx + B - 1) / B;
     const long long units = (long long)p.tiles_x * p.L.ny;
     const long long G = std::min<long long>(units, (long long)sms[dev] * per_sm[dev]);
-    return launch_after_prior(step_kernel_pipe<Phys, B, MINB>, (unsigned)(p.nbblk + p.neblk + G), B, 0, s, p) == cudaSuccess
-               ? 0
-               : -1;
+    return launch_after_prior(step_kernel_pipe<Phys, B, MINB>, (unsigned)G, B, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 
 // Halo faces of an x-slab, ahead of the step: one thread per node of column 1 (left halo
@@ -755,13 +792,11 @@ int launch_face(const typename Phys::P& p, cudaStream_t s) {
 template <class Phys, int BX, int BY, int NJ, int MINB>
 int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     const int nthr = BX * BY;
-    static_assert(BX * BY % BLANES == 0 && BX * BY / BLANES <= BNODES, "boundary block size");
-    const int bn = nthr / BLANES;
-    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p, nthr);
+    if (launch_aux<Phys>(p, s) != 0) return -1;
+    p.nbblk = p.neblk = 0;
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
-    const long long nblocks = (long long)p.nbblk + p.neblk + (long long)p.tiles_x * tiles_y;
+    const long long nblocks = (long long)p.tiles_x * tiles_y;
     return launch_after_prior(step_kernel<Phys, BX, BY, NJ, MINB>, (unsigned)nblocks, nthr, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 

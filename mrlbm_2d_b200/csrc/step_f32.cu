@@ -13,8 +13,8 @@ int launch_face_f32(const StepParams<float>& p, bool full, void* stream) {
 template <class Ph>
 static int launch_step_impl(const StepParams<float>& p, int tile_cfg, cudaStream_t s, int workers) {
     switch (tile_cfg) {
-#define MRLBM_TILE_CASE(id, bx, by, nj, mb) \
-    case id: return launch_step_tiles<Ph, bx, by, nj, mb>(p, s);
+#define MRLBM_TILE_CASE(id, bx, by, nj, mb64, mb32) \
+    case id: return launch_step_tiles<Ph, bx, by, nj, mb32>(p, s);
         MRLBM_TILE_LIST(MRLBM_TILE_CASE)
 #undef MRLBM_TILE_CASE
 #define MRLBM_TMA_CASE(id, bx, by, st) \

@@ -92,21 +92,23 @@ struct alignas(64) StepParams {
 };
 
 // Bulk tile shapes of step_kernel (threads BX x BY, NJ rows per thread, MINB resident blocks
-// per SM, which sets the register budget 65536 / (BX*BY*MINB)).  The autotuner picks one.
-struct TileCfg { int bx, by, nj, minb; };
+// per SM, which sets the register budget 65536 / (BX*BY*MINB)); MINB is given per precision
+// (FP64, FP32): the FP32 node path needs fewer registers, so more of its blocks can be
+// resident.  The autotuner picks one.
+struct TileCfg { int bx, by, nj, minb64, minb32; };
 #define MRLBM_TILE_LIST(X) \
-    X(0, 32, 8, 1, 4)      \
-    X(1, 32, 8, 2, 4)      \
-    X(2, 32, 8, 2, 3)      \
-    X(3, 32, 4, 4, 4)      \
-    X(4, 32, 4, 4, 6)      \
-    X(5, 32, 8, 4, 3)      \
-    X(6, 64, 4, 2, 4)      \
-    X(7, 32, 4, 8, 4)      \
-    X(8, 32, 8, 4, 2)      \
-    X(9, 32, 4, 2, 8)
+    X(0, 32, 8, 1, 4, 4)   \
+    X(1, 32, 8, 2, 4, 4)   \
+    X(2, 32, 8, 2, 3, 5)   \
+    X(3, 32, 4, 4, 4, 4)   \
+    X(4, 32, 4, 4, 6, 6)   \
+    X(5, 32, 8, 4, 3, 3)   \
+    X(6, 64, 4, 2, 4, 4)   \
+    X(7, 32, 4, 2, 6, 11)  \
+    X(8, 32, 8, 4, 2, 2)   \
+    X(9, 32, 4, 2, 8, 8)
 constexpr int N_TILE_CFGS = 10;
-#define MRLBM_TILE_ENTRY(id, bx, by, nj, mb) {bx, by, nj, mb},
+#define MRLBM_TILE_ENTRY(id, bx, by, nj, mb64, mb32) {bx, by, nj, mb64, mb32},
 constexpr TileCfg TILE_CFGS[N_TILE_CFGS] = {MRLBM_TILE_LIST(MRLBM_TILE_ENTRY)};
 #undef MRLBM_TILE_ENTRY
 

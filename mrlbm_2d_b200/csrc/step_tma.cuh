@@ -9,7 +9,7 @@
 // which holds exactly the pull-stream sources of plane k for every node of the tile.  The
 // copies complete on the stage's mbarrier (expect_tx); threads wait on it, read their nine
 // populations from shared memory, collide and store straight to global memory.  Edge and
-// curved-wall nodes belong to the edge and boundary blocks, as in step_kernel.
+// curved-wall nodes belong to the step's auxiliary launch, as with step_kernel.
 //
 // Every mbarrier wait is bounded: after TMA_SPIN_LIMIT polls the CTA raises errflag bit 4,
 // drains its outstanding copies (again bounded) and returns.
@@ -205,9 +205,9 @@ __device__ __forceinline__ void tma_bulk_worker(const typename Phys::P& p) {
 
 template <class Phys, int BX, int BY, int STAGES, bool STORE>
 __global__ void __launch_bounds__(BX, 1) step_kernel_tma(const __grid_constant__ typename Phys::P p) {
-    if ((int)blockIdx.x >= p.nbblk) wait_prior_grid();   // boundary blocks wait after staging their tables
-    if (run_aux_block<Phys, wide_wall<Phys>(BX, 1)>(p)) return;
+    bulk_begin();
     tma_bulk_worker<Phys, BX, BY, STAGES, STORE>(p);
+    bulk_end(p);
 }
 
 template <class T, int BX, int BY, int STAGES, bool STORE>
@@ -221,9 +221,6 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
     using T = typename Phys::T;
     using G = TmaGeom<T, BX, BY>;
     const int nthr = BX;
-    const int bn = nthr / BLANES;
-    p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
-    p.neblk = edge_blocks(p, nthr);
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int smem = tma_smem_bytes<T, BX, BY, STAGES, STORE>();
     if (smem > 200 * 1024) return -2;                        // shape too large for this precision
@@ -236,7 +233,9 @@ int launch_step_tma(typename Phys::P p, cudaStream_t s, int workers) {
             return -1;
         if (dev < 64) attr_set |= 1ull << dev;
     }
-    return launch_after_prior(step_kernel_tma<Phys, BX, BY, STAGES, STORE>, (unsigned)(p.nbblk + p.neblk + workers),
+    if (launch_aux<Phys>(p, s) != 0) return -1;
+    p.nbblk = p.neblk = 0;
+    return launch_after_prior(step_kernel_tma<Phys, BX, BY, STAGES, STORE>, (unsigned)workers,
                               nthr, (size_t)smem, s, p) == cudaSuccess
                ? 0
                : -1;

@@ -97,6 +97,7 @@ def test_forces_per_step_ring_drains_in_order(mrlbm):
     s.step(5)
     it2, *_ = s.forces()
     assert np.array_equal(it2, np.arange(102, 107))
-    # one fused kernel per step; the last stats step's record is summed by the next step's
-    # kernel, or, when the history is read first, by one small kernel per read
-    assert s.launch_count() - n0 == 105 + 2
+    # two launches per step (wall and edge nodes, then the bulk tiles); the last stats step's
+    # record is summed by the next step's launch, or, when the history is read first, by one
+    # small kernel per read
+    assert s.launch_count() - n0 == 2 * 105 + 2
