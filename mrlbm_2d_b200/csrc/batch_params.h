@@ -27,6 +27,7 @@ struct BatchBarrier {
     unsigned gen;
     int abort;
     int err;
+    unsigned bulk_done;            // bulk blocks of the step launch that have finished (split steps)
 };
 
 template <class T>
@@ -35,7 +36,9 @@ struct BatchArgs {
     const BatchCase* cases;
     const int* aux_off;            // [ncases + 1] prefix sums of aux items
     const int* tile_off;           // [ncases + 1] prefix sums of bulk tiles
-    const int* item_case;          // [aux items + bulk tiles] case of each work item
+    const int* item_case;          // [aux items + bulk tiles] case of each work item (persistent schedule)
+    const int* aux_case;           // split steps: case of each auxiliary item
+    const int* tile_case;          // split steps: case of each bulk tile
     BatchBarrier* bar;
     int ncases;
     int nsteps;                    // steps this launch advances (persistent schedule)
@@ -51,6 +54,19 @@ struct BatchArgs {
 // error, -2 for a shape that is not a vector shape.
 int launch_batch_f64(const BatchArgs<double>& a, int tile_cfg, int grid, bool cooperative, void* stream);
 int launch_batch_f32(const BatchArgs<float>& a, int tile_cfg, int grid, bool cooperative, void* stream);
+// One step of every case as two launches (graph schedule): the auxiliary items (walked by
+// aux_grid blocks of AUX_THREADS), then the bulk tiles of shape tile_cfg (a one-tile-per-block or
+// vector shape) over `grid` blocks, each taking a contiguous run of tiles.  Return 0, -1 on a
+// launch error, -2 for a shape the split step does not take.
+int launch_batch_split_f64(const BatchArgs<double>& a, int tile_cfg, int aux_grid, int grid, void* stream);
+int launch_batch_split_f32(const BatchArgs<float>& a, int tile_cfg, int aux_grid, int grid, void* stream);
+// Bulk blocks per SM of the split step's bulk kernel for a shape, and its threads per block.
+int batch_split_blocks_per_sm(int precision, int tile_cfg);
+int batch_split_blocks_per_sm_f64(int tile_cfg);
+int batch_split_blocks_per_sm_f32(int tile_cfg);
+int batch_split_threads(int tile_cfg);
+// Auxiliary block size of the split step (step_common.cuh AUX_THREADS).
+constexpr int BATCH_AUX_THREADS = 128;
 // Resident blocks per SM of the batch kernel of a vector shape (0: not a vector shape).
 int batch_blocks_per_sm(int precision, int tile_cfg);
 int batch_blocks_per_sm_f64(int tile_cfg);

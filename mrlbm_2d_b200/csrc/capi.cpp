@@ -1678,16 +1678,32 @@ int stats_in(const mrlbm_config& c, int a, int z) {
 }
 
 // Work items of one step of case h for vector shape cfg.
-void batch_items(const mrlbm_handle* h, int cfg, int& aux, int& tiles, int& nbblk, int& neblk, int& tiles_x) {
-    const VecCfg v = VEC_CFGS[cfg - VEC_CFG0];
-    const int nthr = v.warps * 32, vw = 16 / h->elem;
-    const int bn = nthr / 8;
+// Work items of one step of case h: auxiliary blocks of aux_threads threads, and the bulk tiles
+// of shape cfg (a vector shape, or for split steps also a one-tile-per-block shape).
+void batch_items(const mrlbm_handle* h, int cfg, int aux_threads, int& aux, int& tiles, int& nbblk, int& neblk,
+                 int& tiles_x) {
+    const int bn = aux_threads / 8;
     nbblk = h->geo.nb > 0 ? (h->geo.nb + bn - 1) / bn : 1;
-    neblk = (2 * h->L.nx + (h->halo_l ? 0 : h->L.ny - 2) + (h->halo_r ? 0 : h->L.ny - 2) + nthr - 1) / nthr;
-    tiles_x = (h->L.nx + 32 * vw - 1) / (32 * vw);
-    const int tiles_y = (h->L.ny + v.warps * v.nj - 1) / (v.warps * v.nj);
+    neblk = (2 * h->L.nx + (h->halo_l ? 0 : h->L.ny - 2) + (h->halo_r ? 0 : h->L.ny - 2) + aux_threads - 1) / aux_threads;
+    int tiles_y;
+    if (is_vec_cfg(cfg)) {
+        const VecCfg v = VEC_CFGS[cfg - VEC_CFG0];
+        const int vw = 16 / h->elem;
+        tiles_x = (h->L.nx + 32 * vw - 1) / (32 * vw);
+        tiles_y = (h->L.ny + v.warps * v.nj - 1) / (v.warps * v.nj);
+    } else {
+        const TileCfg t = TILE_CFGS[cfg];
+        tiles_x = (h->L.nx + t.bx - 1) / t.bx;
+        tiles_y = (h->L.ny + t.by * t.nj - 1) / (t.by * t.nj);
+    }
     aux = nbblk + neblk;
     tiles = tiles_x * tiles_y;
+}
+
+// Split steps (the graph schedule) run the auxiliary items in blocks of their own size.
+bool batch_split(const mrlbm_batch* b) { return b->schedule == MRLBM_BATCH_GRAPH; }
+int batch_aux_threads(const mrlbm_batch* b) {
+    return batch_split(b) ? BATCH_AUX_THREADS : VEC_CFGS[b->tile_cfg - VEC_CFG0].warps * 32;
 }
 
 template <class T>
@@ -1708,7 +1724,7 @@ void batch_fill(mrlbm_batch* b, unsigned char* stage, int want_macro) {
         p.ovr = h->ovr_live ? h->d_ovr : nullptr;
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         int aux, tiles;
-        batch_items(h, b->tile_cfg, aux, tiles, p.nbblk, p.neblk, p.tiles_x);
+        batch_items(h, b->tile_cfg, batch_aux_threads(b), aux, tiles, p.nbblk, p.neblk, p.tiles_x);
         ps[c] = p;
         BatchCase bc{};
         const mrlbm_config& k = h->cfg;
@@ -1769,7 +1785,8 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
     b->stage_i ^= 1;
     const int* off = reinterpret_cast<const int*>(b->h_stage[si] + pb + cb);
     const int items = off[n] + off[2 * n + 1];
-    if (b->item_case_cfg != b->tile_cfg) {             // the item -> case table of this shape
+    const int table_key = 2 * b->tile_cfg + (batch_split(b) ? 1 : 0);
+    if (b->item_case_cfg != table_key) {               // the item -> case table of this shape and schedule
         std::vector<int> tab((size_t)items);
         for (int c = 0; c < n; ++c) {
             for (int k = off[c]; k < off[c + 1]; ++k) tab[(size_t)k] = c;
@@ -1784,7 +1801,7 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
             b->item_case_cap = (size_t)items;
         }
         BCK(cudaMemcpy(b->d_item_case, tab.data(), sizeof(int) * (size_t)items, cudaMemcpyHostToDevice));
-        b->item_case_cfg = b->tile_cfg;
+        b->item_case_cfg = table_key;
     }
 
     // the full kernel instantiation when any case has field statistics or a body force in this
@@ -1802,6 +1819,8 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
         a.aux_off = b->d_off;
         a.tile_off = b->d_off + n + 1;
         a.item_case = b->d_item_case;
+        a.aux_case = b->d_item_case;                   // split steps: aux items first, then the tiles
+        a.tile_case = b->d_item_case + off[n];
         a.bar = b->d_bar;
         a.ncases = n;
         a.call_steps = steps;
@@ -1817,6 +1836,19 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
         return b->precision == MRLBM_FP64 ? launch_batch_f64(a64, b->tile_cfg, grid, coop, b->stream)
                                           : launch_batch_f32(a32, b->tile_cfg, grid, coop, b->stream);
     };
+    // split step k of the call: the auxiliary items walked by two blocks per SM, then the bulk
+    // tiles in contiguous runs over eight times the resident blocks (runs short enough that the
+    // blocks finish together; measured on the 64-case sweep: 1x 162 us, 4x 143 us, 8x 139 us,
+    // 16x 146 us per step)
+    const int per_sm_split = batch_split(b) ? batch_split_blocks_per_sm(b->precision, b->tile_cfg) : 0;
+    const int split_grid = std::max(1, std::min(off[2 * n + 1], 8 * b->num_sms * std::max(per_sm_split, 1)));
+    auto launch_split = [&](int k) {
+        a64.nsteps = a32.nsteps = 1;
+        a64.step0 = a32.step0 = k;
+        const int aux_grid = std::min(off[n], 2 * b->num_sms);
+        return b->precision == MRLBM_FP64 ? launch_batch_split_f64(a64, b->tile_cfg, aux_grid, split_grid, b->stream)
+                                          : launch_batch_split_f32(a32, b->tile_cfg, aux_grid, split_grid, b->stream);
+    };
     if (b->schedule == MRLBM_BATCH_PERSISTENT) {
         const int per_sm = batch_blocks_per_sm(b->precision, b->tile_cfg);
         if (per_sm <= 0) return bfail(b, MRLBM_EUNSUPPORTED, "batch shape does not fit");
@@ -1825,13 +1857,14 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
             return bfail(b, MRLBM_ECUDA, std::string("batch launch: ") + cudaGetErrorString(cudaGetLastError()));
         ++b->launches;
     } else {
+        if (per_sm_split <= 0) return bfail(b, MRLBM_EUNSUPPORTED, "batch shape does not fit");
         if (!b->graph || b->graph_cfg != b->tile_cfg || b->graph_steps != steps || b->graph_macro != want_macro ||
             b->graph_full != full) {
             if (b->graph) cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
             BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
             int rc = 0;
-            for (int k = 0; k < steps && rc == 0; ++k) rc = launch(1, k, items, false);
+            for (int k = 0; k < steps && rc == 0; ++k) rc = launch_split(k);
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamEndCapture(b->stream, &g);
             if (rc != 0 || e != cudaSuccess) {
@@ -1848,7 +1881,7 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
             b->graph_full = full;
         }
         BCK(cudaGraphLaunch(b->graph, b->stream));
-        b->launches += steps;
+        b->launches += 2 * steps;
     }
     for (mrlbm_handle* h : b->h) {
         const int a0 = h->iter + 1, z = h->iter + steps;
@@ -1944,7 +1977,10 @@ int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h) {
 }
 
 int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch) {
-    if (!b || !is_vec_cfg(tile_cfg) || steps_per_launch < 1 || steps_per_launch > RING_CAP ||
+    // the persistent schedule takes the vector shapes; split steps (graph schedule) also the
+    // one-tile-per-block shapes
+    const bool shape_ok = is_vec_cfg(tile_cfg) || (schedule == MRLBM_BATCH_GRAPH && tile_cfg >= 0 && tile_cfg < N_TILE_CFGS);
+    if (!b || !shape_ok || steps_per_launch < 1 || steps_per_launch > RING_CAP ||
         (schedule != MRLBM_BATCH_PERSISTENT && schedule != MRLBM_BATCH_GRAPH))
         return MRLBM_EINVAL;
     b->tile_cfg = tile_cfg;
@@ -2062,8 +2098,10 @@ int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_pe
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const int steps = std::min(trial_steps, RING_CAP);
-    for (int cfg = VEC_CFG0; cfg < PIPE_CFG0 && rc == MRLBM_OK; ++cfg) {
+    for (int cfg = 0; cfg < PIPE_CFG0 && rc == MRLBM_OK; ++cfg) {
+        if (cfg >= N_TILE_CFGS && cfg < VEC_CFG0) continue;     // TMA shapes are single-case only
         for (int sched = MRLBM_BATCH_PERSISTENT; sched <= MRLBM_BATCH_GRAPH && rc == MRLBM_OK; ++sched) {
+            if (!is_vec_cfg(cfg) && sched == MRLBM_BATCH_PERSISTENT) continue;
             b->tile_cfg = cfg;
             b->schedule = sched;
             b->steps_per_launch = steps;

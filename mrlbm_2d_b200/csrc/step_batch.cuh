@@ -19,6 +19,7 @@
 // returns.
 #pragma once
 #include "batch_params.h"
+#include <cstddef>
 #include "step_common.cuh"
 
 namespace mrlbm {
@@ -115,6 +116,112 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) step_kernel_batch(const __gr
         }
         if (a.nsteps > 1 && !batch_barrier(a.bar, a.spin_limit)) return;
     }
+}
+
+// ---- split steps (graph schedule): an auxiliary launch and a bulk launch per step ----------
+// The same ordering as a single case's step (step_common.cuh): the auxiliary launch waits for
+// the previous step and lets the bulk launch start; the bulk launch's last block waits for the
+// auxiliary launch.  A block stages the parameters of its case for this step in shared memory
+// (the bytes after the tensor maps, which no batched path reads), with the per-step fields
+// derived from the case's call state; a bulk block takes a contiguous run of tiles, so it
+// stages again only when the run crosses into the next case.
+template <class T>
+__device__ __forceinline__ void batch_stage(const BatchArgs<T>& a, int c, int cs, unsigned char* sp_raw) {
+    using P = StepParams<T>;
+    constexpr int OFF = (int)offsetof(P, tile_ctr);
+    static_assert(OFF % 16 == 0 && sizeof(P) % 16 == 0, "16-byte staging");
+    P& sp = *reinterpret_cast<P*>(sp_raw);
+    __syncthreads();                                   // the previous item is done with sp
+    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const char*>(a.params + c) + OFF);
+    uint4* dst = reinterpret_cast<uint4*>(sp_raw + OFF);
+    for (int q = threadIdx.x; q < (int)((sizeof(P) - OFF) / 16); q += blockDim.x) dst[q] = src[q];
+    BatchCase bc;
+    if (threadIdx.x == 0) bc = a.cases[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int iter = bc.iter0 + cs + 1;
+        if (cs & 1) {                                  // params hold the call's first time level
+            const T* t = sp.src;
+            sp.src = sp.dst;
+            sp.dst = const_cast<T*>(t);
+        }
+        const bool stats = bc.post_process && iter >= bc.statsbegin && iter <= bc.statsend;
+        sp.iter = iter;
+        sp.do_stats = stats;
+        sp.rec = stats ? bc.ring + (size_t)(bc.ring_n0 + batch_stats_count(bc, bc.iter0 + 1, iter - 1)) * REC_WORDS : nullptr;
+        sp.zero_solid_u = bc.post_process && bc.iplot > 0 && iter % bc.iplot == 0 && bc.plot_cyl;
+        sp.macro = (a.want_macro && cs == a.call_steps - 1) ? bc.macro : nullptr;
+        sp.fstat = (bc.fstat && iter >= bc.fs_begin && iter <= bc.fs_end) ? bc.fstat : nullptr;
+        if (!(cs == 0 && bc.ovr_live)) {
+            sp.ovr = nullptr;
+            sp.n_ovr = 0;
+        }
+    }
+    __syncthreads();
+}
+
+static_assert(BATCH_AUX_THREADS == AUX_THREADS, "auxiliary block size of the split batch step");
+
+template <class Phys>
+__global__ void __launch_bounds__(AUX_THREADS) batch_aux_kernel(const __grid_constant__ BatchArgs<typename Phys::T> a) {
+    using P = typename Phys::P;
+    __shared__ __align__(64) unsigned char sp_raw[sizeof(P)];
+    __shared__ __align__(16) unsigned char smem[aux_smem_bytes<typename Phys::T>()];
+    wait_prior_grid();
+    // a grid that fits the GPU at once walks all the cases' auxiliary items, so every block has
+    // allowed the bulk launch to start within the first moments of the step
+    const int n_aux = __ldg(a.aux_off + a.ncases);
+    for (int item = (int)blockIdx.x; item < n_aux; item += (int)gridDim.x) {
+        const int c = __ldg(a.aux_case + item);
+        batch_stage(a, c, a.step0, sp_raw);
+        aux_item<Phys, true, false>(*reinterpret_cast<const P*>(sp_raw), smem, item - __ldg(a.aux_off + c));
+    }
+}
+
+// Bulk tiles of one split step.  TILE: a one-tile-per-block shape (BX x BY threads, NJ rows);
+// otherwise a vector shape (BX warps, NJ rows per warp).
+template <class Phys, bool TILE, int BX, int BY, int NJ, int MINB>
+__global__ void __launch_bounds__(TILE ? BX * BY : BX * 32, MINB)
+    batch_bulk_kernel(const __grid_constant__ BatchArgs<typename Phys::T> a) {
+    using P = typename Phys::P;
+    __shared__ __align__(64) unsigned char sp_raw[sizeof(P)];
+    bulk_begin();
+    const long long n = __ldg(a.tile_off + a.ncases);
+    const int i0 = (int)(n * blockIdx.x / gridDim.x), i1 = (int)(n * (blockIdx.x + 1) / gridDim.x);
+    int cur = -1;
+    for (int item = i0; item < i1; ++item) {
+        const int c = __ldg(a.tile_case + item);
+        if (c != cur) {
+            batch_stage(a, c, a.step0, sp_raw);
+            cur = c;
+        }
+        const P& sp = *reinterpret_cast<const P*>(sp_raw);
+        const int t = item - __ldg(a.tile_off + c);
+        if constexpr (TILE) tile_body<Phys, BX, BY, NJ>(sp, t);
+        else vec_tile<Phys, BX, NJ>(sp, t);
+    }
+    if (threadIdx.x == 0 && atomicAdd(&a.bar->bulk_done, 1u) == gridDim.x - 1) {
+        a.bar->bulk_done = 0u;
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+    }
+}
+
+template <class Phys, bool TILE, int BX, int BY, int NJ, int MINB>
+int launch_batch_split(const BatchArgs<typename Phys::T>& a, int n_aux, int grid, cudaStream_t s) {
+    if (launch_after_prior(batch_aux_kernel<Phys>, (unsigned)n_aux, AUX_THREADS, 0, s, a) != cudaSuccess) return -1;
+    return launch_after_prior(batch_bulk_kernel<Phys, TILE, BX, BY, NJ, MINB>, (unsigned)grid, TILE ? BX * BY : BX * 32, 0, s,
+                              a) == cudaSuccess
+               ? 0
+               : -1;
+}
+
+template <class Phys, bool TILE, int BX, int BY, int NJ, int MINB>
+int batch_split_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_bulk_kernel<Phys, TILE, BX, BY, NJ, MINB>,
+                                                      TILE ? BX * BY : BX * 32, 0) != cudaSuccess)
+        return 0;
+    return n;
 }
 
 // Block sizes and register budgets of the batch kernels: the vector shapes' (warps per block,

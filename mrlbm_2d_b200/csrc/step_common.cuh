@@ -516,9 +516,8 @@ __device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, i
 // thread first issues the loads of all its interior rows, then finishes them (collide and store)
 // one by one, so up to 9*NJ loads per thread are in flight.
 template <class Phys, int BX, int BY, int NJ>
-__device__ __forceinline__ void tile_body(const typename Phys::P& p) {
+__device__ __forceinline__ void tile_body(const typename Phys::P& p, int t) {
     using T = typename Phys::T;
-    const int t = blockIdx.x;
     const int tx = t % p.tiles_x, ty = t / p.tiles_x;
     const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
     const int i = 1 + tx * BX + lx;
@@ -558,7 +557,7 @@ __device__ __forceinline__ void tile_body(const typename Phys::P& p) {
 template <class Phys, int BX, int BY, int NJ, int MINB>
 __global__ void __launch_bounds__(BX * BY, MINB) step_kernel(const __grid_constant__ typename Phys::P p) {
     bulk_begin();
-    tile_body<Phys, BX, BY, NJ>(p);
+    tile_body<Phys, BX, BY, NJ>(p, (int)blockIdx.x);
     bulk_end(p);
 }
 

@@ -121,4 +121,41 @@ int launch_surface_f32(const StepParams<float>& p, const SurfaceTables& t, doubl
     return surf::launch_surface(p, t, rec, prec, s);
 }
 
+
+template <class Ph>
+static int launch_batch_split_impl(const BatchArgs<double>& a, int tile_cfg, int n_aux, int grid, cudaStream_t s) {
+    switch (tile_cfg) {
+#define MRLBM_TILE_CASE(id, bx, by, nj, mb64, mb32) \
+    case id: return launch_batch_split<Ph, true, bx, by, nj, mb64>(a, n_aux, grid, s);
+        MRLBM_TILE_LIST(MRLBM_TILE_CASE)
+#undef MRLBM_TILE_CASE
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return launch_batch_split<Ph, false, w, 1, nj, mb>(a, n_aux, grid, s);
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return -2;
+    }
+}
+
+int launch_batch_split_f64(const BatchArgs<double>& a, int tile_cfg, int n_aux, int grid, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    return a.full ? launch_batch_split_impl<fp64::Physics>(a, tile_cfg, n_aux, grid, s)
+                  : launch_batch_split_impl<fp64::PhysicsLean>(a, tile_cfg, n_aux, grid, s);
+}
+
+int batch_split_blocks_per_sm_f64(int tile_cfg) {
+    using Ph = fp64::PhysicsLean;
+    switch (tile_cfg) {
+#define MRLBM_TILE_CASE(id, bx, by, nj, mb64, mb32) \
+    case id: return batch_split_per_sm<Ph, true, bx, by, nj, mb64>();
+        MRLBM_TILE_LIST(MRLBM_TILE_CASE)
+#undef MRLBM_TILE_CASE
+#define MRLBM_VEC_CASE(id, w, nj, mb) \
+    case id: return batch_split_per_sm<Ph, false, w, 1, nj, mb>();
+        MRLBM_VEC_LIST(MRLBM_VEC_CASE)
+#undef MRLBM_VEC_CASE
+    default: return 0;
+    }
+}
+
 }  // namespace mrlbm
