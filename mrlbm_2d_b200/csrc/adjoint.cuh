@@ -446,35 +446,43 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
     if (slot[q] >= 0) atomicAdd(a.lam_out + slot[q], c);
 }
 
-// One adjoint step in one launch of 128-thread blocks: [nb wall blocks][edge blocks, 7 nodes
-// x 18 inputs each][bulk blocks, 128 nodes each].
+// One adjoint step as two launches, ordered like the forward step's (step_common.cuh): the
+// wall and edge blocks [nb wall blocks][edge blocks, 7 nodes x 18 inputs each], whose dual-number
+// maps get the registers they need, then the bulk blocks (128 nodes each), which start once the
+// first launch has waited for the previous step and run beside it; the last bulk block to finish
+// waits for the first launch, so the step completes as a whole.
 template <class P>
-__global__ void __launch_bounds__(128, 5) adjoint_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
-    wait_prior_grid();                                  // launched like the step kernels (step_common.cuh)
+__global__ void __launch_bounds__(128) adjoint_aux(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    wait_prior_grid();
     const int b = (int)blockIdx.x;
-    const int n_edge_blk = (a.n_edge + 6) / 7;
     if (b < p.nb) {
         adjoint_wall(p, a, b);
         return;
     }
-    if (b < p.nb + n_edge_blk) {
-        // lambda^n of the block's 7 edge nodes, staged once and cleared for reuse
-        __shared__ double lam[7][Q];
-        const int t = threadIdx.x, e0 = 7 * (b - p.nb);
-        if (t < 7 * Q) {
-            const int e = e0 + t / Q, k = t % Q;
-            if (e < a.n_edge) {
-                const int i = e < p.L.ny ? 1 : p.L.nx, j = 1 + (e < p.L.ny ? e : e - p.L.ny);
-                const int64_t at = p.L.at(i, j, k);
-                lam[t / Q][k] = a.lam_in[at];
-                a.lam_in[at] = 0.0;
-            }
+    // lambda^n of the block's 7 edge nodes, staged once and cleared for reuse
+    __shared__ double lam[7][Q];
+    const int t = threadIdx.x, e0 = 7 * (b - p.nb);
+    if (t < 7 * Q) {
+        const int e = e0 + t / Q, k = t % Q;
+        if (e < a.n_edge) {
+            const int i = e < p.L.ny ? 1 : p.L.nx, j = 1 + (e < p.L.ny ? e : e - p.L.ny);
+            const int64_t at = p.L.at(i, j, k);
+            lam[t / Q][k] = a.lam_in[at];
+            a.lam_in[at] = 0.0;
         }
-        __syncthreads();
-        if (t < 126) adjoint_edge(p, a, e0 + t / 18, t % 18, lam[t / 18]);
-        return;
     }
-    adjoint_bulk(p, a, (int64_t)(b - p.nb - n_edge_blk) * 128 + threadIdx.x);
+    __syncthreads();
+    if (t < 126) adjoint_edge(p, a, e0 + t / 18, t % 18, lam[t / 18]);
+}
+
+template <class P>
+__global__ void __launch_bounds__(128, 6) adjoint_bulk_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+    bulk_begin();
+    adjoint_bulk(p, a, (int64_t)blockIdx.x * 128 + threadIdx.x);
+    if (threadIdx.x == 0 && atomicAdd(a.done, 1u) == gridDim.x - 1) {
+        *a.done = 0u;
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+    }
 }
 
 }  // namespace adj

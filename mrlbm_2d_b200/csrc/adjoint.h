@@ -13,6 +13,7 @@ struct AdjArgs {
     double* grad_uin;          // [ny] accumulated dJ/d(u_in), or null
     double wJ;                 // weight of this step's drag in J (1/T inside the window, else 0)
     int n_edge;                // edge-column nodes: 2 ny
+    unsigned* done;            // bulk blocks of the step's bulk launch that have finished (zero between steps)
 };
 
 }  // namespace adj

@@ -1464,7 +1464,7 @@ int adj_backward(mrlbm_handle* h, const void* src, int iter, bool ovr, const adj
     p.n_ovr = ovr ? (int)h->ovr.size() : 0;
     p.zero_solid_u = c.post_process && c.iplot > 0 && iter % c.iplot == 0 && (c.channel_with_cylinder || c.channel_with_square);
     p.iter = iter;
-    h->launches += 1;
+    h->launches += 2;
     return launch_adjoint_step(p, a, h->stream);
 }
 
@@ -1498,7 +1498,7 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     // handle so repeated calls (a gradient loop) allocate nothing; it grows when a call needs more.
     const auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t n_levels = (size_t)ncp + (seg.empty() ? 0 : 2 * (seg.size() - 1)) + 2;
-    const size_t ws = n_levels * al(LB) + al((size_t)N * REC_WORDS * sizeof(double)) +
+    const size_t ws = n_levels * al(LB) + al((size_t)N * REC_WORDS * sizeof(double)) + al(sizeof(unsigned)) +
                       (grads ? 2 * al(LAM) + al((size_t)2 * nodes * sizeof(double)) + al((size_t)h->L.ny * sizeof(double)) : 0);
     if (h->adj_ws_bytes < ws) {
         if (h->adj_ws) cudaFree(h->adj_ws);
@@ -1522,6 +1522,8 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     for (int q = 1; q < (int)seg.size() && ok; ++q) ok = level(&seg[q]) && level(&seg2[q]);   // [0] borrows a checkpoint
     ok = ok && level(&work[0]) && level(&work[1]);
     d_rec = (double*)carve((size_t)N * REC_WORDS * sizeof(double));
+    unsigned* d_done = (unsigned*)carve(sizeof(unsigned));      // the adjoint bulk launches' counter
+    ok = ok && cudaMemsetAsync(d_done, 0, sizeof(unsigned), h->stream) == cudaSuccess;
     if (ok && grads) {
         lam[0] = (double*)carve(LAM);
         lam[1] = (double*)carve(LAM);
@@ -1603,6 +1605,7 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             a.grad_uin = gu;
             a.wJ = n > N - T ? 1.0 / T : 0.0;
             a.n_edge = 2 * h->L.ny;
+            a.done = d_done;
             const bool ovr = n == 1 && h->ovr_live;
             if ((fp64 ? adj_backward<double>(h, sg[t], it0 + n, ovr, a) : adj_backward<float>(h, sg[t], it0 + n, ovr, a)) != 0)
                 rc = MRLBM_ECUDA;
