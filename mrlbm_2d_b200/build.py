@@ -26,6 +26,7 @@ NVCC_COMMON = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexp
 CU_UNITS = {
     "step_f64.cu": ["-fmad=false"],
     "step_f32.cu": [],
+    "adjoint.cu": [],
     "noalloc.cu": [],
     "state_io.cu": [],
 }

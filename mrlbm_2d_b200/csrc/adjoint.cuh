@@ -303,23 +303,30 @@ __device__ __forceinline__ void body_grad(const P& p, const AdjArgs& a, int i, i
 
 // Bulk node, reverse mode by hand.  Forward: rho = sum g, u = j / rho, m = Pi / rho,
 // m' = (1 - w) m + w u u, fo_k = w_k rho A_k with A_k = 1 + 3 c.u + 4.5 m'_xx Hxx
-// + 4.5 m'_yy Hyy + 9 m'_xy Hxy.
+// + 4.5 m'_yy Hyy + 9 m'_xy Hxy.  Every load the node needs (its inputs, lambda^n, the
+// body-gradient sums) is issued before the first use, so a node waits for memory once.
 template <class P>
-__device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int64_t t) {
+__device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int t) {
     const int nx = p.L.nx, ny = p.L.ny;
-    if (t >= (int64_t)nx * ny) return;
-    const int i = 1 + (int)(t % nx), j = 1 + (int)(t / nx);
+    if (t >= nx * ny) return;
+    const int j = 1 + t / nx, i = t - (j - 1) * nx + 1;
     if (!p.xper && (i == 1 || i == nx)) return;            // edge columns: adjoint_edge
     const int cls = node_class(p, i, j);
     if (cls >= 0) return;                                  // curved-wall node: adjoint_wall
+    const int64_t own = p.L.at(i, j, 0), plane = p.L.plane;
     double g[Q], lam[Q];
     gather_d(p, i, j, g);
 #pragma unroll
-    for (int k = 0; k < Q; ++k) {
-        const int64_t at = p.L.at(i, j, k);
-        lam[k] = a.lam_in[at];
-        a.lam_in[at] = 0.0;                      // read once: the buffer becomes step n-2's target
+    for (int k = 0; k < Q; ++k) lam[k] = __ldcg(a.lam_in + own + k * plane);
+    const int64_t n = (int64_t)(i - 1) + (int64_t)nx * (j - 1), N = (int64_t)nx * ny;
+    const bool bg = p.body && a.grad_body;
+    double gbx = 0.0, gby = 0.0;
+    if (bg) {
+        gbx = a.grad_body[n];
+        gby = a.grad_body[N + n];
     }
+#pragma unroll
+    for (int k = 0; k < Q; ++k) a.lam_in[own + k * plane] = 0.0;   // read once: the buffer becomes step n-2's target
     const fp64::Mac m = fp64::moments(g, p.hm, p.hp);
     const bool u_zero = cls == CLS_SOLID && p.zero_solid_u;
     const double ux = u_zero ? 0.0 : m.ux, uy = u_zero ? 0.0 : m.uy;
@@ -346,14 +353,33 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int64
     mxyb *= om1;
     if (u_zero) { uxb = 0.0; uyb = 0.0; }
     const double inv = 1.0 / m.rho;
+    double mu[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const double hxx = ex(k) != 0 ? p.hp : p.hm, hyy = ey(k) != 0 ? p.hp : p.hm, hxy = (double)(ex(k) * ey(k));
-        const double mu = rb + inv * (uxb * (ex(k) - m.ux) + uyb * (ey(k) - m.uy) + mxxb * (hxx - m.mxx) +
-                                      myyb * (hyy - m.myy) + mxyb * (hxy - m.mxy));
-        scatter(p, a, i, j, k, mu);
+        mu[k] = rb + inv * (uxb * (ex(k) - m.ux) + uyb * (ey(k) - m.uy) + mxxb * (hxx - m.mxx) + myyb * (hyy - m.myy) +
+                            mxyb * (hxy - m.mxy));
     }
-    if (p.body) body_grad(p, a, i, j, lam);
+    const bool shared = i == nx - 1 || (i >= a.sx0 && i <= a.sx1 && j >= a.sy0 && j <= a.sy1);
+    if (!shared && is_interior(p, i, j)) {
+        // the nine source slots are this node's alone: plain stores into the zeroed buffer
+        double* d = a.lam_out + own;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) d[k * plane - ey(k) * (int64_t)p.L.pitch - ex(k)] = mu[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) scatter(p, a, i, j, k, mu[k]);
+    }
+    if (bg) {
+        double gx = 0.0, gy = 0.0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            gx += 3.0 * p.w[k] * ex(k) * lam[k];
+            gy += 3.0 * p.w[k] * ey(k) * lam[k];
+        }
+        a.grad_body[n] = gbx + gx;
+        a.grad_body[N + n] = gby + gy;
+    }
 }
 
 // Edge columns: thread (e, q), e over the 2 ny nodes of columns 1 and nx, q over 18 inputs:
@@ -476,9 +502,9 @@ __global__ void __launch_bounds__(128) adjoint_aux(const __grid_constant__ P p, 
 }
 
 template <class P>
-__global__ void __launch_bounds__(128, 6) adjoint_bulk_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(128, 4) adjoint_bulk_step(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
     bulk_begin();
-    adjoint_bulk(p, a, (int64_t)blockIdx.x * 128 + threadIdx.x);
+    adjoint_bulk(p, a, (int)blockIdx.x * 128 + (int)threadIdx.x);
     if (threadIdx.x == 0 && atomicAdd(a.done, 1u) == gridDim.x - 1) {
         *a.done = 0u;
         asm volatile("griddepcontrol.wait;" ::: "memory");

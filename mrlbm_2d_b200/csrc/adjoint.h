@@ -14,6 +14,11 @@ struct AdjArgs {
     double wJ;                 // weight of this step's drag in J (1/T inside the window, else 0)
     int n_edge;                // edge-column nodes: 2 ny
     unsigned* done;            // bulk blocks of the step's bulk launch that have finished (zero between steps)
+    // Bounding box of the curved-wall stencil nodes (empty: sx0 > sx1).  A slot of lambda^{n-1}
+    // is pulled by one node only, except the slots a stencil node pulls (its wall node reads them
+    // too) and those of column nx - 1 (the outlet copies them): bulk nodes inside the box or in
+    // that column add atomically, every other interior node stores its nine slots outright.
+    int sx0, sx1, sy0, sy1;
 };
 
 }  // namespace adj

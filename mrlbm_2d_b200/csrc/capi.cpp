@@ -1568,6 +1568,12 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     // sweep segment c + 1 from the other set on the handle's stream: a recompute waits for the
     // sweep that last used its set, a sweep for the recompute of its segment.
     std::vector<void*>* sets[2] = {&seg, &seg2};
+    int sx0 = h->L.nx + 1, sx1 = 0, sy0 = h->L.ny + 1, sy1 = 0;   // stencil-node bounding box
+    for (int l = 0; l < h->geo.nb; ++l)
+        for (int m = 0; m < 12; ++m) {
+            const int si = h->geo.tint[(size_t)(I_SI + m) * h->geo.nb + l], sj = h->geo.tint[(size_t)(I_SJ + m) * h->geo.nb + l];
+            sx0 = std::min(sx0, si); sx1 = std::max(sx1, si); sy0 = std::min(sy0, sj); sy1 = std::max(sy1, sj);
+        }
     cudaStream_t rs = nullptr;
     cudaEvent_t rec_done[2] = {nullptr, nullptr}, adj_done[2] = {nullptr, nullptr};
     if (grads && rc == MRLBM_OK) {
@@ -1606,6 +1612,7 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             a.wJ = n > N - T ? 1.0 / T : 0.0;
             a.n_edge = 2 * h->L.ny;
             a.done = d_done;
+            a.sx0 = sx0; a.sx1 = sx1; a.sy0 = sy0; a.sy1 = sy1;
             const bool ovr = n == 1 && h->ovr_live;
             if ((fp64 ? adj_backward<double>(h, sg[t], it0 + n, ovr, a) : adj_backward<float>(h, sg[t], it0 + n, ovr, a)) != 0)
                 rc = MRLBM_ECUDA;

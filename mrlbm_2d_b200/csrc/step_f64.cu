@@ -3,7 +3,6 @@
 #include "step_fp64.cuh"
 #include "step_tma.cuh"
 #include "step_batch.cuh"
-#include "adjoint.cuh"
 #include "surface.cuh"
 
 namespace mrlbm {
@@ -101,21 +100,6 @@ int batch_blocks_per_sm_f64(int tile_cfg) {
     default: return 0;
     }
 }
-
-// Adjoint step (adjoint.cuh): the wall and edge-column blocks, then the bulk blocks.
-template <class T>
-static int launch_adjoint(const StepParams<T>& p, const adj::AdjArgs& a, cudaStream_t s) {
-    const int64_t nodes = (int64_t)p.L.nx * p.L.ny;
-    const int64_t aux = (int64_t)p.nb + (a.n_edge + 6) / 7;
-    if (launch_after_prior(adj::adjoint_aux<StepParams<T>>, (unsigned)aux, 128, 0, s, p, a) != cudaSuccess) return -1;
-    return launch_after_prior(adj::adjoint_bulk_step<StepParams<T>>, (unsigned)((nodes + 127) / 128), 128, 0, s, p, a) ==
-                   cudaSuccess
-               ? 0
-               : -1;
-}
-
-int launch_adjoint_step(const StepParams<double>& p, const adj::AdjArgs& a, cudaStream_t s) { return launch_adjoint(p, a, s); }
-int launch_adjoint_step(const StepParams<float>& p, const adj::AdjArgs& a, cudaStream_t s) { return launch_adjoint(p, a, s); }
 
 int launch_surface_f64(const StepParams<double>& p, const SurfaceTables& t, double* rec, double* prec, cudaStream_t s) {
     return surf::launch_surface(p, t, rec, prec, s);

@@ -288,14 +288,14 @@ __device__ __forceinline__ void closure_rotated_body(const P& p, const BTab<doub
     m.mxy = (Mxx - Myy) * 0.50 * s2 + Mxy * c2;
 }
 
-__device__ __noinline__ void closure_rotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp, double uyp,
-                                             double Mxx, double Myy, Mac& m) {
+static __device__ __noinline__ void closure_rotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp, double uyp,
+                                                    double Mxx, double Myy, Mac& m) {
     closure_rotated_body(p, tb, li, f, uxp, uyp, Mxx, Myy, m);
 }
 
 // Unrotated closure with Cramer's rule, 2d_mrlbm.f90:1496-1633 and 1974-2003.
-__device__ __noinline__ void closure_unrotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp,
-                                               double uyp, Mac& m) {
+static __device__ __noinline__ void closure_unrotated(const P& p, const BTab<double>& tb, int li, const double f[Q], double uxp,
+                                                      double uyp, Mac& m) {
     const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     const double omega = p.omega, hm = p.hm, hp = p.hp;
     double rhoI = 0, mxxI = 0, myyI = 0, mxyI = 0, A_p = 0, E_p = 0, B11 = 0, B22 = 0, B12 = 0;
