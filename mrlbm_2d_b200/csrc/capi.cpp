@@ -456,9 +456,10 @@ int launch_one(mrlbm_handle* h, bool stats, bool plot, bool macro) {
         }
         rc = launch_step_f32(p, tc, h->stream, h->workers);
     }
-    h->launches += 2;                                  // the step's auxiliary and bulk launches
+    const int nl = step_launches(h->precision == MRLBM_FP32, tc);
+    h->launches += nl;
     if (rc == -2) {
-        h->launches -= 2;
+        h->launches -= nl;
         return fail(h, MRLBM_EUNSUPPORTED, "tile shape does not fit this precision");
     }
     if (rc != 0) {
@@ -1447,7 +1448,7 @@ int adj_forward(mrlbm_handle* h, const void* src, void* dst, int iter, double* r
     p.do_stats = rec != nullptr;
     p.rec = rec;
     p.iter = iter;
-    h->launches += 2;
+    h->launches += step_launches(sizeof(T) == 4, tile);
     if (sizeof(T) == 8) return launch_step_f64(reinterpret_cast<const StepParams<double>&>(p), tile, st, 0);
     return launch_step_f32(reinterpret_cast<const StepParams<float>&>(p), tile, st, 0);
 }
@@ -1735,6 +1736,7 @@ void batch_fill(mrlbm_batch* b, unsigned char* stage, int want_macro) {
         p.n_ovr = h->ovr_live ? (int)h->ovr.size() : 0;
         int aux, tiles;
         batch_items(h, b->tile_cfg, batch_aux_threads(b), aux, tiles, p.nbblk, p.neblk, p.tiles_x);
+        p.tx_magic = tile_div_magic(p.tiles_x, tiles);
         ps[c] = p;
         BatchCase bc{};
         const mrlbm_config& k = h->cfg;

@@ -209,7 +209,7 @@ int noalloc_step(NaCase& c, void* d_state, const double* d_f0, int32_t nsteps, d
             p.n_ovr = ovr_live ? n_ovr : 0;
             rc = launch_step_f32(p, c.tile_cfg, st, 0);
         }
-        c.launches += 2;
+        c.launches += step_launches(c.precision == MRLBM_FP32, c.tile_cfg);
         if (rc != 0) { err = std::string("kernel launch failed: ") + cudaGetErrorString(cudaGetLastError()); return MRLBM_ECUDA; }
         ovr_live = false;
         c.cur ^= 1;

@@ -188,17 +188,23 @@ __global__ void __launch_bounds__(TILE ? BX * BY : BX * 32, MINB)
     bulk_begin();
     const long long n = __ldg(a.tile_off + a.ncases);
     const int i0 = (int)(n * blockIdx.x / gridDim.x), i1 = (int)(n * (blockIdx.x + 1) / gridDim.x);
-    int cur = -1;
-    for (int item = i0; item < i1; ++item) {
-        const int c = __ldg(a.tile_case + item);
-        if (c != cur) {
-            batch_stage(a, c, a.step0, sp_raw);
-            cur = c;
-        }
+    if (i0 < i1) {
+        // the case's tiles are consecutive items: a run needs the tile table only where it starts
+        // and where it crosses into the next case (skipping cases without tiles)
+        int c = __ldg(a.tile_case + i0);
+        int t = i0 - __ldg(a.tile_off + c), end = __ldg(a.tile_off + c + 1);
+        batch_stage(a, c, a.step0, sp_raw);
         const P& sp = *reinterpret_cast<const P*>(sp_raw);
-        const int t = item - __ldg(a.tile_off + c);
-        if constexpr (TILE) tile_body<Phys, BX, BY, NJ>(sp, t);
-        else vec_tile<Phys, BX, NJ>(sp, t);
+        for (int item = i0; item < i1; ++item, ++t) {
+            if (item == end) {
+                do end = __ldg(a.tile_off + (++c) + 1);
+                while (end == item);
+                t = 0;
+                batch_stage(a, c, a.step0, sp_raw);
+            }
+            if constexpr (TILE) tile_body<Phys, BX, BY, NJ>(sp, t);
+            else vec_tile<Phys, BX, NJ>(sp, t);
+        }
     }
     if (threadIdx.x == 0 && atomicAdd(&a.bar->bulk_done, 1u) == gridDim.x - 1) {
         a.bar->bulk_done = 0u;

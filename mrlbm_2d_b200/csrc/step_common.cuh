@@ -512,13 +512,21 @@ __device__ __forceinline__ void gather_interior(const StepParams<T>& p, int i, i
     for (int k = 0; k < Q; ++k) f[k] = __ldg(s + (k * plane - ey(k) * pitch - ex(k)));
 }
 
+// Tile t's column and row of tiles, by a multiply-high where the launcher provided one.
+template <class T>
+__device__ __forceinline__ void tile_coords(const StepParams<T>& p, int t, int& tx, int& ty) {
+    ty = p.tx_magic ? (int)(((unsigned long long)(unsigned)t * p.tx_magic) >> 32) : t / p.tiles_x;
+    tx = t - ty * p.tiles_x;
+}
+
 // Bulk tiles of BX x (BY*NJ) nodes, one thread per column and NJ rows, one tile per block.  A
 // thread first issues the loads of all its interior rows, then finishes them (collide and store)
 // one by one, so up to 9*NJ loads per thread are in flight.
 template <class Phys, int BX, int BY, int NJ>
 __device__ __forceinline__ void tile_body(const typename Phys::P& p, int t) {
     using T = typename Phys::T;
-    const int tx = t % p.tiles_x, ty = t / p.tiles_x;
+    int tx, ty;
+    tile_coords(p, t, tx, ty);
     const int lx = threadIdx.x % BX, ly = threadIdx.x / BX;
     const int i = 1 + tx * BX + lx;
     const int nx = p.L.nx, ny = p.L.ny;
@@ -598,7 +606,8 @@ __device__ __forceinline__ void vec_tile(const typename Phys::P& p, int t) {
     using T = typename Phys::T;
     using VT = Vec16<T>;
     constexpr int VW = VT::N;
-    const int tx = t % p.tiles_x, ty = t / p.tiles_x;
+    int tx, ty;
+    tile_coords(p, t, tx, ty);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nx = p.L.nx, ny = p.L.ny;
     const int i0 = 1 + (tx * 32 + lane) * VW;
@@ -683,6 +692,7 @@ int launch_step_vec(typename Phys::P p, cudaStream_t s) {
     p.tiles_x = (p.L.nx + 32 * VW - 1) / (32 * VW);
     const int tiles_y = (p.L.ny + WARPS * NJ - 1) / (WARPS * NJ);
     const long long nblocks = (long long)p.tiles_x * tiles_y;
+    p.tx_magic = tile_div_magic(p.tiles_x, nblocks);
     return launch_after_prior(step_kernel_vec<Phys, WARPS, NJ, MINB>, (unsigned)nblocks, nthr, 0, s, p) == cudaSuccess ? 0
                                                                                                             : -1;
 }
@@ -788,14 +798,41 @@ int launch_face(const typename Phys::P& p, cudaStream_t s) {
     return launch_after_prior(face_kernel<Phys>, (unsigned)((n + 127) / 128), 128, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 
+// One launch for the whole step (Phys::FUSED_AUX): blocks [0, nbblk) are wall blocks of BX*BY/8
+// nodes, the next neblk edge blocks of BX*BY nodes, then the bulk tiles; every block waits for
+// the previous step first (the wall blocks after staging their tables), so no block of the
+// step needs to wait for another launch.
+template <class Phys, int BX, int BY, int NJ, int MINB>
+__global__ void __launch_bounds__(BX * BY, MINB) step_kernel_fused(const __grid_constant__ typename Phys::P p) {
+    __shared__ __align__(16) unsigned char smem[aux_smem_bytes<typename Phys::T>()];
+    const int b = (int)blockIdx.x;
+    if (b < p.nbblk) {
+        boundary_block<Phys, wide_wall<Phys>(BX * BY, MINB), true>(p, smem, b);
+        return;
+    }
+    wait_prior_grid();
+    if (b < p.nbblk + p.neblk) edge_block<Phys>(p, b - p.nbblk, smem);
+    else tile_body<Phys, BX, BY, NJ>(p, b - p.nbblk - p.neblk);
+}
+
 template <class Phys, int BX, int BY, int NJ, int MINB>
 int launch_step_tiles(typename Phys::P p, cudaStream_t s) {
     const int nthr = BX * BY;
-    if (launch_aux<Phys>(p, s) != 0) return -1;
-    p.nbblk = p.neblk = 0;
     p.tiles_x = (p.L.nx + BX - 1) / BX;
     const int tiles_y = (p.L.ny + BY * NJ - 1) / (BY * NJ);
     const long long nblocks = (long long)p.tiles_x * tiles_y;
+    p.tx_magic = tile_div_magic(p.tiles_x, nblocks);
+    if constexpr (Phys::FUSED_AUX) {
+        const int bn = nthr / BLANES;
+        p.nbblk = p.nb > 0 ? (p.nb + bn - 1) / bn : 1;
+        p.neblk = edge_blocks(p, nthr);
+        return launch_after_prior(step_kernel_fused<Phys, BX, BY, NJ, MINB>, (unsigned)(p.nbblk + p.neblk + nblocks), nthr,
+                                  0, s, p) == cudaSuccess
+                   ? 0
+                   : -1;
+    }
+    if (launch_aux<Phys>(p, s) != 0) return -1;
+    p.nbblk = p.neblk = 0;
     return launch_after_prior(step_kernel<Phys, BX, BY, NJ, MINB>, (unsigned)nblocks, nthr, 0, s, p) == cudaSuccess ? 0 : -1;
 }
 

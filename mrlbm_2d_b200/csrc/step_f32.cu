@@ -137,11 +137,11 @@ template <class Ph>
 static int launch_batch_split_impl(const BatchArgs<float>& a, int tile_cfg, int n_aux, int grid, cudaStream_t s) {
     switch (tile_cfg) {
 #define MRLBM_TILE_CASE(id, bx, by, nj, mb64, mb32) \
-    case id: return launch_batch_split<Ph, true, bx, by, nj, mb32>(a, n_aux, grid, s);
+    case id: return launch_batch_split<Ph, true, bx, by, nj, BATCH_MINB32[id]>(a, n_aux, grid, s);
         MRLBM_TILE_LIST(MRLBM_TILE_CASE)
 #undef MRLBM_TILE_CASE
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
-    case id: return launch_batch_split<Ph, false, w, 1, nj, mb>(a, n_aux, grid, s);
+    case id: return launch_batch_split<Ph, false, w, 1, nj, BATCH_VEC_MINB32[id - VEC_CFG0]>(a, n_aux, grid, s);
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
     default: return -2;
@@ -158,11 +158,11 @@ int batch_split_blocks_per_sm_f32(int tile_cfg) {
     using Ph = fp32::PhysicsLean;
     switch (tile_cfg) {
 #define MRLBM_TILE_CASE(id, bx, by, nj, mb64, mb32) \
-    case id: return batch_split_per_sm<Ph, true, bx, by, nj, mb32>();
+    case id: return batch_split_per_sm<Ph, true, bx, by, nj, BATCH_MINB32[id]>();
         MRLBM_TILE_LIST(MRLBM_TILE_CASE)
 #undef MRLBM_TILE_CASE
 #define MRLBM_VEC_CASE(id, w, nj, mb) \
-    case id: return batch_split_per_sm<Ph, false, w, 1, nj, mb>();
+    case id: return batch_split_per_sm<Ph, false, w, 1, nj, BATCH_VEC_MINB32[id - VEC_CFG0]>();
         MRLBM_VEC_LIST(MRLBM_VEC_CASE)
 #undef MRLBM_VEC_CASE
     default: return 0;

@@ -21,6 +21,15 @@ struct Mac { float drho, rho, ux, uy, mxx, myy, mxy; };
 
 constexpr float THIRD = 1.0f / 3.0f;
 
+// 1 / x by the hardware approximation (PTX rcp.approx.ftz.f32, within one unit in the last
+// place): the FP32 form is held to accuracy bounds against the FP64 step, not to a rounding
+// pattern, and a node's density is near 1.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // rho = 1 + sum g + (sum w - 1); u = sum f c / rho; m = sum f H / rho with
 // sum f H_xx = (sum_k w_k H_xx,k) + sum g c_x^2 - sum g / 3.
 __device__ __forceinline__ Mac moments(const P& p, const float g[Q]) {
@@ -28,7 +37,7 @@ __device__ __forceinline__ Mac moments(const P& p, const float g[Q]) {
     const float dg = (((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7]))) + g[8];
     m.drho = dg + p.dc.eps_mass;
     m.rho = 1.0f + m.drho;
-    const float inv = 1.0f / m.rho;
+    const float inv = rcp_approx(m.rho);
     const float jx = ((g[1] - g[3]) + (g[5] - g[7])) + (g[8] - g[6]);
     const float jy = ((g[2] - g[4]) + (g[5] - g[7])) + (g[6] - g[8]);
     const float d4 = (g[5] + g[6]) + (g[7] + g[8]);
@@ -339,6 +348,9 @@ struct PhysicsT {
     }
     // registers per thread a kernel needs before its wall node's populations are gathered ahead
     static constexpr int WIDE_REGS = 96;
+    // One launch per step with tile shapes: the FP32 wall closures fit the tiles' register
+    // budgets, so the wall and edge blocks run as the first blocks of the bulk grid.
+    static constexpr bool FUSED_AUX = true;
 };
 using Physics = PhysicsT<true>;
 using PhysicsLean = PhysicsT<false>;

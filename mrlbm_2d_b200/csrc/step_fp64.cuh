@@ -483,6 +483,7 @@ struct PhysicsT {
     }
     // registers per thread a kernel needs before its wall-node path is inlined (boundary_close_pre)
     static constexpr int WIDE_REGS = 128;
+    static constexpr bool FUSED_AUX = false;         // the wall closures get a launch of their own
 };
 using Physics = PhysicsT<true>;
 using PhysicsLean = PhysicsT<false>;

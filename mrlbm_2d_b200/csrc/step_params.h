@@ -88,8 +88,16 @@ struct alignas(64) StepParams {
     double* fstat;                // [6 * nx * ny] running sums of u, v, p, u^2, v^2, p^2, or null
     const T* body;                // [2 * nx * ny] body force (x then y), node order, or null
     int tiles_x;                  // bulk tiles along x
+    unsigned long long tx_magic;  // tile_div_magic(tiles_x, tiles), or 0: t / tiles_x by division
     DevConsts dc;                 // deviation-form constants (FP32 only)
 };
+
+// ceil(2^32 / d), so that t / d == (t * m) >> 32 for every t with t * d < 2^32 (writing
+// m d = 2^32 + e, 0 <= e < d, the quotient's error term t e / (d 2^32) stays below 1/d); 0 when
+// the tiles of a launch reach that bound.
+inline unsigned long long tile_div_magic(int d, long long tiles) {
+    return (unsigned long long)tiles * (unsigned long long)d < (1ull << 32) ? ((1ull << 32) + (unsigned)d - 1) / (unsigned)d : 0ull;
+}
 
 // Bulk tile shapes of step_kernel (threads BX x BY, NJ rows per thread, MINB resident blocks
 // per SM, which sets the register budget 65536 / (BX*BY*MINB)); MINB is given per precision
@@ -104,7 +112,7 @@ struct TileCfg { int bx, by, nj, minb64, minb32; };
     X(4, 32, 4, 4, 6, 6)   \
     X(5, 32, 8, 4, 3, 3)   \
     X(6, 64, 4, 2, 4, 4)   \
-    X(7, 32, 4, 2, 6, 11)  \
+    X(7, 32, 4, 2, 6, 10)  \
     X(8, 32, 8, 4, 2, 2)   \
     X(9, 32, 4, 2, 8, 8)
 constexpr int N_TILE_CFGS = 10;
@@ -157,6 +165,16 @@ constexpr VecCfg VEC_CFGS[N_VEC_CFGS] = {MRLBM_VEC_LIST(MRLBM_VEC_ENTRY)};
 #undef MRLBM_VEC_ENTRY
 constexpr int VEC_CFG0 = TMA_CFG0 + N_TMA_CFGS;
 
+// Resident blocks per SM of the batched bulk kernels, per tile shape (ids 0..9) and vector
+// shape (ids VEC_CFG0..): a batched block reads its case's parameters from shared memory into
+// registers, where a single case reads them from the constant bank, so a batched shape needs
+// more registers than the same single-case shape.  These are the largest counts at which the
+// lean FP32 / FP64 batched instantiations keep every value in registers.
+constexpr int BATCH_MINB32[N_TILE_CFGS] = {4, 3, 2, 4, 3, 2, 3, 7, 1, 6};
+constexpr int BATCH_MINB64[N_TILE_CFGS] = {3, 2, 1, 2, 1, 1, 2, 4, 1, 3};
+constexpr int BATCH_VEC_MINB32[N_VEC_CFGS] = {2, 2, 3, 2, 3, 6};
+constexpr int BATCH_VEC_MINB64[N_VEC_CFGS] = {1, 1, 3, 2, 3, 6};
+
 // Persistent software-pipelined shapes of step_kernel_pipe (B threads per block, MINB
 // resident blocks per SM; the grid is the resident set).
 #define MRLBM_PIPE_LIST(X) \
@@ -173,6 +191,9 @@ inline bool is_tma_store_cfg(int c) { return c >= TMAS_CFG0 && c < N_ALL_CFGS; }
 inline bool is_tma_cfg(int c) { return (c >= TMA_CFG0 && c < VEC_CFG0) || is_tma_store_cfg(c); }
 inline TmaCfg tma_cfg(int c) { return is_tma_store_cfg(c) ? TMAS_CFGS[c - TMAS_CFG0] : TMA_CFGS[c - TMA_CFG0]; }
 inline bool is_vec_cfg(int c) { return c >= VEC_CFG0 && c < PIPE_CFG0; }
+// Kernel launches of one time step: FP32 tile shapes run the step as one launch (the wall and
+// edge blocks first in the grid), every other shape as an auxiliary launch and a bulk launch.
+inline int step_launches(bool fp32, int c) { return fp32 && c >= 0 && c < N_TILE_CFGS ? 1 : 2; }
 
 // Host-side launch entry points (step_f64.cu / step_f32.cu).  `workers` is the persistent
 // CTA count for TMA shapes (ignored otherwise).  Return 0, -1 on a launch error, -2 when the
