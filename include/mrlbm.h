@@ -349,24 +349,32 @@ int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps);
  * the work of every case, either as a persistent cooperative launch that loops over steps
  * with a grid barrier (MRLBM_BATCH_PERSISTENT, steps_per_launch steps per launch) or as one
  * launch per step captured once into a CUDA graph of steps_per_launch launches and replayed
- * (MRLBM_BATCH_GRAPH).  Each case's results are bit-identical to stepping it alone.  The
+ * (MRLBM_BATCH_GRAPH); or each case's own single-case step launches run on a stream of the
+ * case's own, steps_per_launch steps per case captured into one graph and replayed with the
+ * per-call iteration and record slots uploaded before each replay (MRLBM_BATCH_STREAMS; a call
+ * with macroscopic output, field statistics or a loaded state's first step runs as
+ * MRLBM_BATCH_GRAPH instead).  Each case's results are bit-identical to stepping it alone.  The
  * cases are ordinary handles owned by the batch (mrlbm_batch_case): read their forces,
  * fields and state, load states, set inlet profiles and field-statistics windows with the
  * single-case calls, but step them only through mrlbm_batch_step and do not destroy them. */
 typedef struct mrlbm_batch mrlbm_batch;
 #define MRLBM_BATCH_PERSISTENT 0
 #define MRLBM_BATCH_GRAPH      1
+#define MRLBM_BATCH_STREAMS    2
 
 int mrlbm_batch_create(const mrlbm_config* cfgs, int32_t ncases, int precision, int device, mrlbm_batch** out);
 int mrlbm_batch_destroy(mrlbm_batch* b);
 int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h);
 /* Advance every case by nsteps (flags: MRLBM_STEP_MACRO stores each case's fields on the last). */
 int mrlbm_batch_step(mrlbm_batch* b, int32_t nsteps, int32_t flags);
-/* tile_cfg: a 128-bit vector shape (16..21); schedule: MRLBM_BATCH_PERSISTENT or _GRAPH. */
+/* tile_cfg: a 128-bit vector shape (16..21) for MRLBM_BATCH_PERSISTENT; a vector or a
+ * one-tile-per-block shape (0..9) for MRLBM_BATCH_GRAPH; a one-tile-per-block shape for
+ * MRLBM_BATCH_STREAMS. */
 int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch);
 int mrlbm_batch_get_schedule(const mrlbm_batch* b, int32_t* tile_cfg, int32_t* schedule, int32_t* steps_per_launch);
-/* Time every vector shape under both schedules for trial_steps steps (states, counters and
- * histories restored afterwards) and keep the fastest; returns its time per batch step. */
+/* Time every shape under every schedule that takes it for trial_steps steps (rounded up to
+ * even; states, counters and histories restored afterwards) and keep the fastest; returns its
+ * time per batch step. */
 int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_per_step);
 /* Watchdog of the persistent schedule: how many times a block polls the grid barrier between
  * two steps before it decides the launch has lost a block, raises MRLBM_EDEVICE_TIMEOUT and

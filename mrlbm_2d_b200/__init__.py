@@ -5,5 +5,5 @@ the C ABI of libmrlbm.so (include/mrlbm.h).  The CUDA library is required: there
 fallback.
 """
 from .config import Config  # noqa: F401
-from .api import (BATCH_GRAPH, BATCH_PERSISTENT, FP32, FP64, N_TILE_CONFIGS, Batch, MrlbmError, Simulation, config_from_namelist, cp_statistics,  # noqa: F401
+from .api import (BATCH_GRAPH, BATCH_PERSISTENT, BATCH_STREAMS, FP32, FP64, N_TILE_CONFIGS, Batch, MrlbmError, Simulation, config_from_namelist, cp_statistics,  # noqa: F401
                   force_statistics, load_library, rho_inlet_running_mean, slabs_step)

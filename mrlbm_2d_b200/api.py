@@ -42,7 +42,7 @@ EXPORTED = [
     "mrlbm_create_slab", "mrlbm_halo_size", "mrlbm_halo_pack", "mrlbm_halo_unpack", "mrlbm_slabs_step",
     "mrlbm_step_faces", "mrlbm_halo_pack_next", "mrlbm_halo_unpack_next",
 ]
-BATCH_PERSISTENT, BATCH_GRAPH = 0, 1
+BATCH_PERSISTENT, BATCH_GRAPH, BATCH_STREAMS = 0, 1, 2
 
 
 class MrlbmError(RuntimeError):

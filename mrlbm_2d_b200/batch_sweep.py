@@ -5,8 +5,9 @@
 
 The cases are config.sweep_cases(n): nx uniform in [256, 1024] (multiples of 32), ny = nx/4,
 D = ny/5 at (nx/5, ny/2 + 0.5), Re uniform in [40, 200], U = 0.05, seeded.  The batch is
-autotuned (vector tile shape x schedule: persistent cooperative launches or CUDA-graph replays
-of per-step launches), then advanced `steps` steps; the baseline advances each case alone,
+autotuned (tile shape x schedule: persistent cooperative launches, CUDA-graph replays of
+batched split steps, or each case's own step launches on per-case streams captured into one
+replayed graph), then advanced `steps` steps; the baseline advances each case alone,
 with its own autotuned single-case shape, `seq-steps` steps per case, one launch per step.
 Aggregate MLUPS = sum of nodes x steps / device time (CUDA events on the launching
 streams).  One JSON line.
@@ -35,7 +36,7 @@ def sweep(cases=64, steps=20000, seq_steps=2000, precision=32, trial_steps=50, s
     b = api.Batch(cfgs, precision=precision)
     t0 = time.perf_counter()
     (tile, sched, spl), ms = b.autotune(trial_steps=trial_steps)
-    out["autotune"] = {"tile_shape": tile, "schedule": ["persistent", "graph"][sched], "steps_per_launch": spl,
+    out["autotune"] = {"tile_shape": tile, "schedule": ["persistent", "graph", "streams"][sched], "steps_per_launch": spl,
                        "trial_ms_per_step": ms, "seconds": time.perf_counter() - t0}
     b.step(spl)                                   # warm-up of the chosen schedule
     bs = torch.cuda.ExternalStream(b.stream)

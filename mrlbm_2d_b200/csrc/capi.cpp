@@ -1667,6 +1667,21 @@ struct mrlbm_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_cfg = -1, graph_steps = 0, graph_macro = -1, graph_full = -1;
     unsigned wait_limit = BAR_SPIN_LIMIT;   // grid-barrier polls before a block gives up
+    // Per-case streams schedule: every case's own step launches (the single-case kernels, with
+    // their parameters in the constant bank) on a stream of its own, steps_per_launch steps per
+    // case captured once into one graph (forked from and joined back into the batch stream) and
+    // replayed; the record fields of each replay come from the call state uploaded before it.
+    std::vector<cudaStream_t> cstream;
+    std::vector<cudaEvent_t> join_ev;
+    cudaEvent_t fork_ev = nullptr, call_staged = nullptr;
+    int* d_call = nullptr;             // [2 n] iter0, ring_n0 of each case for the current replay
+    int* h_call = nullptr;             // pinned staging of d_call
+    struct StreamsGraph {
+        cudaGraphExec_t exec = nullptr;
+        int cfg = -1, steps = 0;
+        std::vector<uintptr_t> sig;    // per case: time level, inlet-profile and body-force buffers when captured
+    } sg[2];
+    int sg_next = 0;
 };
 
 namespace {
@@ -1712,7 +1727,7 @@ void batch_items(const mrlbm_handle* h, int cfg, int aux_threads, int& aux, int&
 }
 
 // Split steps (the graph schedule) run the auxiliary items in blocks of their own size.
-bool batch_split(const mrlbm_batch* b) { return b->schedule == MRLBM_BATCH_GRAPH; }
+bool batch_split(const mrlbm_batch* b) { return b->schedule == MRLBM_BATCH_GRAPH || b->schedule == MRLBM_BATCH_STREAMS; }
 int batch_aux_threads(const mrlbm_batch* b) {
     return batch_split(b) ? BATCH_AUX_THREADS : VEC_CFGS[b->tile_cfg - VEC_CFG0].warps * 32;
 }
@@ -1772,9 +1787,129 @@ size_t batch_param_bytes(const mrlbm_batch* b) {
     return n * (pb + sizeof(BatchCase)) + (2 * n + 2) * sizeof(int);
 }
 
+// Whether a call of `steps` steps can replay captured single-case launches: a tile shape, and no
+// step of it whose launch would differ from its captured form in more than the record fields
+// (macroscopic output, field statistics, loaded-state overrides).  Other calls take the split
+// graph schedule.
+bool streams_call_ok(const mrlbm_batch* b, int steps, int want_macro) {
+    if (b->tile_cfg < 0 || b->tile_cfg >= N_TILE_CFGS || want_macro) return false;
+    for (const mrlbm_handle* h : b->h) {
+        const mrlbm_config& c = h->cfg;
+        const int a0 = h->iter + 1, z = h->iter + steps;
+        if (h->ovr_live) return false;
+        if (h->d_fstat && std::max(a0, h->fstat_begin) <= std::min(z, h->fstat_end)) return false;
+    }
+    return true;
+}
+
+template <class T>
+int streams_launch_case(mrlbm_batch* b, int c, int steps) {
+    mrlbm_handle* h = b->h[c];
+    const mrlbm_config& k = h->cfg;
+    StepParams<T> p{};
+    fill_common(h, p);
+    p.u_in = h->has_uin ? (const T*)h->d_uin : nullptr;
+    p.body = h->has_body ? (const T*)h->d_body : nullptr;
+    p.call = b->d_call + 2 * c;
+    p.stats_lo = k.post_process ? k.statsbegin : 1;
+    p.stats_hi = k.post_process ? k.statsend : 0;
+    p.ring = h->d_ring;
+    p.plot_every = k.post_process && k.iplot > 0 && (k.channel_with_cylinder || k.channel_with_square) ? k.iplot : 0;
+    int cur = h->cur;
+    for (int s = 0; s < steps; ++s) {
+        p.src = (const T*)h->buf[cur];
+        p.dst = (T*)h->buf[1 - cur];
+        p.bstep = s;
+        const int rc = sizeof(T) == 8 ? launch_step_f64(reinterpret_cast<const StepParams<double>&>(p), b->tile_cfg, b->cstream[c], 0)
+                                      : launch_step_f32(reinterpret_cast<const StepParams<float>&>(p), b->tile_cfg, b->cstream[c], 0);
+        if (rc != 0) return rc;
+        cur ^= 1;
+    }
+    return 0;
+}
+
+int batch_call_streams(mrlbm_batch* b, int steps) {
+    const int n = (int)b->h.size();
+    const bool fp64 = b->precision == MRLBM_FP64;
+    if (b->cstream.empty()) {                          // the per-case streams, once
+        b->cstream.assign(n, nullptr);
+        b->join_ev.assign(n, nullptr);
+        for (int c = 0; c < n; ++c) {
+            BCK(cudaStreamCreateWithFlags(&b->cstream[c], cudaStreamNonBlocking));
+            BCK(cudaEventCreateWithFlags(&b->join_ev[c], cudaEventDisableTiming));
+        }
+        BCK(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+        BCK(cudaEventCreateWithFlags(&b->call_staged, cudaEventDisableTiming));
+        BCK(cudaMalloc((void**)&b->d_call, sizeof(int) * 2 * n));
+        BCK(cudaMallocHost((void**)&b->h_call, sizeof(int) * 2 * n));
+        BCK(cudaEventRecord(b->call_staged, b->stream));
+    }
+    for (mrlbm_handle* h : b->h) {
+        int rc = finish_pending(h);
+        if (rc == MRLBM_OK && h->ring_n + stats_in(h->cfg, h->iter + 1, h->iter + steps) > RING_CAP) rc = drain_ring(h);
+        if (rc != MRLBM_OK) return bfail(b, rc, h->err);
+    }
+    // the call state, uploaded ahead of the replay on the batch stream
+    BCK(cudaEventSynchronize(b->call_staged));
+    for (int c = 0; c < n; ++c) {
+        b->h_call[2 * c] = b->h[c]->iter;
+        b->h_call[2 * c + 1] = b->h[c]->ring_n;
+    }
+    BCK(cudaMemcpyAsync(b->d_call, b->h_call, sizeof(int) * 2 * n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaEventRecord(b->call_staged, b->stream));
+    // the graph captured for these cases' time levels (two are kept: an odd call length
+    // alternates them)
+    std::vector<uintptr_t> sig(3 * (size_t)n);
+    for (int c = 0; c < n; ++c) {
+        const mrlbm_handle* h = b->h[c];
+        sig[3 * c] = (uintptr_t)h->cur;
+        sig[3 * c + 1] = h->has_uin ? (uintptr_t)h->d_uin : 0;
+        sig[3 * c + 2] = h->has_body ? (uintptr_t)h->d_body : 0;
+    }
+    mrlbm_batch::StreamsGraph* g = nullptr;
+    for (auto& q : b->sg)
+        if (q.exec && q.cfg == b->tile_cfg && q.steps == steps && q.sig == sig) g = &q;
+    if (!g) {
+        g = &b->sg[b->sg_next];
+        b->sg_next ^= 1;
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        g->exec = nullptr;
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = cudaEventRecord(b->fork_ev, b->stream) == cudaSuccess ? 0 : -1;
+        for (int c = 0; c < n && rc == 0; ++c) {
+            rc = cudaStreamWaitEvent(b->cstream[c], b->fork_ev, 0) == cudaSuccess ? 0 : -1;
+            if (rc == 0) rc = fp64 ? streams_launch_case<double>(b, c, steps) : streams_launch_case<float>(b, c, steps);
+            if (rc == 0) rc = cudaEventRecord(b->join_ev[c], b->cstream[c]) == cudaSuccess ? 0 : -1;
+            if (rc == 0) rc = cudaStreamWaitEvent(b->stream, b->join_ev[c], 0) == cudaSuccess ? 0 : -1;
+        }
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+        if (rc != 0 || e != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+            return bfail(b, rc == -2 ? MRLBM_EUNSUPPORTED : MRLBM_ECUDA, "capturing the per-case streams graph failed");
+        }
+        e = cudaGraphInstantiate(&g->exec, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return bfail(b, MRLBM_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        g->cfg = b->tile_cfg;
+        g->steps = steps;
+        g->sig = sig;
+    }
+    BCK(cudaGraphLaunch(g->exec, b->stream));
+    for (mrlbm_handle* h : b->h) {
+        h->ring_n += stats_in(h->cfg, h->iter + 1, h->iter + steps);
+        h->iter += steps;
+        h->cur ^= steps & 1;
+        b->launches += (int64_t)steps * step_launches(!fp64, b->tile_cfg);
+    }
+    return MRLBM_OK;
+}
+
 // One call of `steps` steps (at most RING_CAP stats records per case).
 int batch_call(mrlbm_batch* b, int steps, int want_macro) {
     const int n = (int)b->h.size();
+    if (b->schedule == MRLBM_BATCH_STREAMS && streams_call_ok(b, steps, want_macro)) return batch_call_streams(b, steps);
     for (mrlbm_handle* h : b->h) {
         if (h->ring_n + stats_in(h->cfg, h->iter + 1, h->iter + steps) > RING_CAP) {
             int rc = drain_ring(h);
@@ -1911,6 +2046,16 @@ int batch_call(mrlbm_batch* b, int steps, int want_macro) {
 
 void batch_free(mrlbm_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto& q : b->sg)
+        if (q.exec) cudaGraphExecDestroy(q.exec);
+    for (cudaStream_t s : b->cstream)
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->join_ev)
+        if (e) cudaEventDestroy(e);
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    if (b->call_staged) cudaEventDestroy(b->call_staged);
+    if (b->d_call) cudaFree(b->d_call);
+    if (b->h_call) cudaFreeHost(b->h_call);
     for (mrlbm_handle* h : b->h) {
         if (!h) continue;
         h->stream = nullptr;
@@ -1991,10 +2136,12 @@ int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h) {
 int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch) {
     // the persistent schedule takes the vector shapes; split steps (graph schedule) also the
     // one-tile-per-block shapes
-    const bool shape_ok = is_vec_cfg(tile_cfg) || (schedule == MRLBM_BATCH_GRAPH && tile_cfg >= 0 && tile_cfg < N_TILE_CFGS);
-    if (!b || !shape_ok || steps_per_launch < 1 || steps_per_launch > RING_CAP ||
-        (schedule != MRLBM_BATCH_PERSISTENT && schedule != MRLBM_BATCH_GRAPH))
-        return MRLBM_EINVAL;
+    const bool tile = tile_cfg >= 0 && tile_cfg < N_TILE_CFGS;
+    const bool shape_ok = schedule == MRLBM_BATCH_PERSISTENT ? is_vec_cfg(tile_cfg)
+                          : schedule == MRLBM_BATCH_GRAPH     ? is_vec_cfg(tile_cfg) || tile
+                          : schedule == MRLBM_BATCH_STREAMS   ? tile
+                                                              : false;
+    if (!b || !shape_ok || steps_per_launch < 1 || steps_per_launch > RING_CAP) return MRLBM_EINVAL;
     b->tile_cfg = tile_cfg;
     b->schedule = schedule;
     b->steps_per_launch = steps_per_launch;
@@ -2109,11 +2256,12 @@ int mrlbm_batch_autotune(mrlbm_batch* b, int32_t trial_steps, double* best_ms_pe
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int steps = std::min(trial_steps, RING_CAP);
+    const int steps = std::min((trial_steps + 1) & ~1, RING_CAP);   // even: a call ends on its start level
     for (int cfg = 0; cfg < PIPE_CFG0 && rc == MRLBM_OK; ++cfg) {
         if (cfg >= N_TILE_CFGS && cfg < VEC_CFG0) continue;     // TMA shapes are single-case only
-        for (int sched = MRLBM_BATCH_PERSISTENT; sched <= MRLBM_BATCH_GRAPH && rc == MRLBM_OK; ++sched) {
+        for (int sched = MRLBM_BATCH_PERSISTENT; sched <= MRLBM_BATCH_STREAMS && rc == MRLBM_OK; ++sched) {
             if (!is_vec_cfg(cfg) && sched == MRLBM_BATCH_PERSISTENT) continue;
+            if (is_vec_cfg(cfg) && sched == MRLBM_BATCH_STREAMS) continue;
             b->tile_cfg = cfg;
             b->schedule = sched;
             b->steps_per_launch = steps;

@@ -80,6 +80,7 @@ MRLBM_HD SrcSlot stream_source(int nx, int ny, int i, int j, int k, bool xper, b
 // Node class inside the cylinder bounding box (values >= 0 are boundary-node indices).
 constexpr int CLS_FLUID = -1;
 constexpr int CLS_SOLID = -2;
+constexpr int CLS_SOLID_ZERO = -3;   // a solid node of a replayed launch's plot step: u = 0 before collision
 
 // Boundary condition variants of the curved wall (2d_mrlbm.f90:280-311).
 enum Closure : int {

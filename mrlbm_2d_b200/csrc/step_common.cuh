@@ -246,10 +246,28 @@ __device__ __forceinline__ double warp_ordered_sum(const double* v, int n, doubl
     return acc;
 }
 
+// The record fields of a step: the launch's own, or for a replayed launch (p.call set) the ones
+// its call state gives.
+struct StepRec {
+    int do_stats, iter;
+    double* rec;
+};
+template <class T>
+__device__ __forceinline__ StepRec step_rec(const StepParams<T>& p) {
+    if (!p.call) return StepRec{p.do_stats, p.iter, p.rec};
+    const int iter0 = __ldg(p.call), rn0 = __ldg(p.call + 1);
+    StepRec r;
+    r.iter = iter0 + p.bstep + 1;
+    r.do_stats = r.iter >= p.stats_lo && r.iter <= p.stats_hi;
+    const int before = max(0, min(r.iter - 1, p.stats_hi) - max(iter0 + 1, p.stats_lo) + 1);
+    r.rec = r.do_stats ? p.ring + (size_t)(rn0 + before) * REC_WORDS : nullptr;
+    return r;
+}
+
 // Force tail, called by every boundary block once its nodes' forces are in p.partials.
 template <class Phys>
-__device__ __forceinline__ void force_tail(const typename Phys::P& p, unsigned char* smem) {
-    if (!p.do_stats) return;
+__device__ __forceinline__ void force_tail(const typename Phys::P& p, const StepRec& sr, unsigned char* smem) {
+    if (!sr.do_stats) return;
     if (!last_to_arrive(p.counter, p.nbblk)) return;
     __shared__ double sm[2];
     const int tid = threadIdx.x, lane = tid & 31;
@@ -259,11 +277,11 @@ __device__ __forceinline__ void force_tail(const typename Phys::P& p, unsigned c
     }
     __syncthreads();
     if (tid == 0) {
-        if (p.rec) {
-            p.rec[0] = (double)p.iter;
-            p.rec[1] = sm[0];
-            p.rec[2] = sm[1];
-            if (p.halo_l) p.rec[3] = 0.0;                   // an x-slab without column 1 adds 0
+        if (sr.rec) {
+            sr.rec[0] = (double)sr.iter;
+            sr.rec[1] = sm[0];
+            sr.rec[2] = sm[1];
+            if (p.halo_l) sr.rec[3] = 0.0;                  // an x-slab without column 1 adds 0
         }
         p.counter[0] = 0u;
     }
@@ -292,8 +310,8 @@ __device__ __forceinline__ int inlet_blocks(int ny, int halo_l) {
 
 // Inlet tail, called by every edge block once its inlet nodes' rho are in p.partials.
 template <class Phys>
-__device__ __forceinline__ void inlet_tail(const typename Phys::P& p, unsigned char* smem, int eb) {
-    if (!p.do_stats) return;
+__device__ __forceinline__ void inlet_tail(const typename Phys::P& p, const StepRec& sr, unsigned char* smem, int eb) {
+    if (!sr.do_stats) return;
     const int nin = inlet_blocks(p.L.ny, p.halo_l);
     if (eb >= nin) return;
     if (!last_to_arrive(p.counter + 1, nin)) return;
@@ -301,7 +319,7 @@ __device__ __forceinline__ void inlet_tail(const typename Phys::P& p, unsigned c
     if (tid < 32) {
         const double sum = warp_ordered_sum(p.partials + 2 * p.nb, p.L.ny, reinterpret_cast<double*>(smem), tid);
         if (tid == 0) {
-            if (p.rec) p.rec[3] = sum;
+            if (sr.rec) sr.rec[3] = sum;
             p.counter[1] = 0u;
         }
     }
@@ -344,6 +362,7 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
         for (int u = 0; u < IU; ++u)
             if (tid + u * nthr < I_NFIELDS * bn) sgi[tid + u * nthr] = iv[u];
     }
+    const StepRec sr = step_rec(p);
     const int li = tid / BLANES, lane = tid % BLANES;
     const int l = l0 + li;
     const bool active = l < p.nb;
@@ -393,9 +412,9 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
     if (active && lane == 0) {
         if constexpr (WIDE) Phys::boundary_close_pre(p, tb, li, l, fown, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
         else Phys::boundary_close(p, tb, li, l, ux, uy, mx, my, ux3, uy3, mx3, my3, Fx, Fy);
-        if (p.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
+        if (sr.do_stats) { p.partials[l] = Fx; p.partials[p.nb + l] = Fy; }
     }
-    if (!p.defer) force_tail<Phys>(p, smem);
+    if (!p.defer) force_tail<Phys>(p, sr, smem);
 }
 
 // Edge blocks: one thread per domain-edge node, so the edge closures (outlet neighbour gather,
@@ -406,6 +425,7 @@ __device__ __forceinline__ void boundary_block(const typename Phys::P& p, unsign
 template <class Phys>
 __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, unsigned char* smem) {
     const int nx = p.L.nx, ny = p.L.ny;
+    const StepRec sr = step_rec(p);
     const int e = eb * (int)blockDim.x + (int)threadIdx.x;
     const int cl = p.halo_l ? 0 : 1, cr = p.halo_r ? 0 : 1;         // edge columns of this lattice
     const int nl = cl * ny, nr = cr * ny, nrow = nx - cl - cr;
@@ -419,9 +439,9 @@ __device__ __forceinline__ void edge_block(const typename Phys::P& p, int eb, un
             j = q < nrow ? 1 : ny;
         }
         const double rho = Phys::edge_bulk_node(p, i, j, CLS_FLUID);
-        if (p.do_stats && i == 1 && !p.halo_l) p.partials[2 * p.nb + j - 1] = rho;
+        if (sr.do_stats && i == 1 && !p.halo_l) p.partials[2 * p.nb + j - 1] = rho;
     }
-    if (!p.defer) inlet_tail<Phys>(p, smem, eb);
+    if (!p.defer) inlet_tail<Phys>(p, sr, smem, eb);
     else if (eb == 0 && p.prev_rec) record_sums(p.prev_partials, p.nb, p.L.ny, p.halo_l, p.prev_rec, p.prev_iter, smem);
 }
 
@@ -549,6 +569,9 @@ __device__ __forceinline__ void tile_body(const typename Phys::P& p, int t) {
         cls[r] = CLS_FLUID;
         if (j <= ny) {
             cls[r] = node_class(p, i, j);
+            if (cls[r] == CLS_SOLID && p.call && p.plot_every > 0 &&
+                (__ldg(p.call) + p.bstep + 1) % p.plot_every == 0)
+                cls[r] = CLS_SOLID_ZERO;                      // a replayed launch's plot step
             if (cls[r] < 0 && is_interior(p, i, j)) {
                 gather_interior(p, i, j, f[r]);
                 interior |= 1u << r;

@@ -283,7 +283,7 @@ __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int c
     gather(p, i, j, g);
     Mac m = moments(p, g);
     edge_node(p, i, j, g, m);
-    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
+    if ((cls == CLS_SOLID && p.zero_solid_u) || cls == CLS_SOLID_ZERO) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) flag_bad_density(p);
     if (FULL && p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     if (FULL && p.fstat) accumulate_fields(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy);
@@ -300,7 +300,7 @@ __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const
     FieldPre pre;
     if (FULL && p.fstat) fields_load(p, i, j, pre);
     Mac m = moments(p, g);
-    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.f; m.uy = 0.f; }
+    if ((cls == CLS_SOLID && p.zero_solid_u) || cls == CLS_SOLID_ZERO) { m.ux = 0.f; m.uy = 0.f; }
     if (!(m.rho > 0.0f)) flag_bad_density(p);
     if (FULL && p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     if (FULL && p.fstat) fields_store(p, i, j, pre, 1.0 + (double)m.drho, m.ux, m.uy);

@@ -417,7 +417,7 @@ __device__ __forceinline__ double edge_bulk_node(const P& p, int i, int j, int c
     gather(p, i, j, f);
     Mac m = moments(f, p.hm, p.hp);
     edge_node(p, i, j, f, m);
-    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
+    if ((cls == CLS_SOLID && p.zero_solid_u) || cls == CLS_SOLID_ZERO) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) flag_bad_density(p);
     if (FULL && p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     if (FULL && p.fstat) accumulate_fields(p, i, j, m.rho, m.ux, m.uy);
@@ -435,7 +435,7 @@ __device__ __forceinline__ void compute(const P& p, int i, int j, int cls, const
     FieldPre pre;
     if (FULL && p.fstat) fields_load(p, i, j, pre);
     Mac m = moments(f, p.hm, p.hp);
-    if (cls == CLS_SOLID && p.zero_solid_u) { m.ux = 0.0; m.uy = 0.0; }
+    if ((cls == CLS_SOLID && p.zero_solid_u) || cls == CLS_SOLID_ZERO) { m.ux = 0.0; m.uy = 0.0; }
     if (!(m.rho > 0.0)) flag_bad_density(p);
     if (FULL && p.macro) store_macro(p, i, j, m.rho, m.ux, m.uy, m.mxx, m.myy, m.mxy);
     if (FULL && p.fstat) fields_store(p, i, j, pre, m.rho, m.ux, m.uy);

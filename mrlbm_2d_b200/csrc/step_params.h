@@ -82,6 +82,14 @@ struct alignas(64) StepParams {
     int prev_iter;
     double* node_force;           // optional per-boundary-node (Fx, Fy) [2 * nb], or null
     int iter;
+    // A launch captured once into a replayed graph (a batch's per-case streams schedule): `call`
+    // points at the state {iter0, ring_n0} uploaded before each replay, and the record fields
+    // (iter, do_stats, rec) come from it instead (step_rec): iteration iter0 + bstep + 1, a
+    // record when it lies in [stats_lo, stats_hi], in `ring` after the call's earlier records.
+    const int* call;
+    int bstep, stats_lo, stats_hi;
+    double* ring;
+    int plot_every;               // replayed launches: solid velocities zeroed when iter % plot_every == 0 (0: never)
     int* errflag;
     // optional macroscopic output (Fortran order nx*ny): rho, ux, uy, mxx, myy, mxy
     double* macro;                // [6 * nx * ny] or null

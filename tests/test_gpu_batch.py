@@ -1,6 +1,7 @@
 """Batched cases: one kernel advancing several independent cases (persistent cooperative
 launches, or CUDA-graph replays of split steps: an auxiliary launch and a bulk launch per step,
-with vector or one-tile-per-block bulk shapes) gives every case exactly the bits it gets when
+with vector or one-tile-per-block bulk shapes), or each case's own step launches on per-case
+streams captured into one replayed graph, gives every case exactly the bits it gets when
 stepped alone."""
 import numpy as np
 import pytest
@@ -34,7 +35,8 @@ def _alone(mrlbm, cfg, prec, steps, macro=False, fields=None):
 
 @pytest.mark.parametrize("prec", [64, 32])
 @pytest.mark.parametrize("tile,sched,spl", [(18, 0, 7), (16, 1, 5), (21, 0, 1), (17, 1, 13), (20, 0, 23),
-                                            (9, 1, 5), (6, 1, 23), (0, 1, 1), (3, 1, 7)])
+                                            (9, 1, 5), (6, 1, 23), (0, 1, 1), (3, 1, 7),
+                                            (9, 2, 5), (7, 2, 8), (0, 2, 23), (6, 2, 1)])
 def test_batch_matches_single_cases(mrlbm, prec, tile, sched, spl):
     cfgs = _cfgs()
     b = mrlbm.Batch(cfgs, precision=prec)
@@ -87,8 +89,9 @@ def test_batch_autotune_restores_state(mrlbm):
     b.step(4)
     before = [c.get_state() for c in b.cases]
     (tile, sched, spl), ms = b.autotune(trial_steps=8)
-    # vector shapes under either schedule; one-tile-per-block shapes only as split (graph) steps
-    assert (16 <= tile <= 21 and sched in (0, 1)) or (0 <= tile < 10 and sched == 1)
+    # vector shapes under the persistent or split-graph schedule; one-tile-per-block shapes as
+    # split-graph steps or per-case streams
+    assert (16 <= tile <= 21 and sched in (0, 1)) or (0 <= tile < 10 and sched in (1, 2))
     assert ms > 0
     for c, f in zip(b.cases, before):
         assert np.array_equal(c.get_state(), f)
@@ -99,4 +102,41 @@ def test_batch_autotune_restores_state(mrlbm):
         assert np.array_equal(c.get_state(), ref["f"])
         assert np.array_equal(c.forces()[1], ref["forces"][1])
     assert b.status() == 0
+    b.close()
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_batch_streams_calls_interleave_with_split_calls(mrlbm, prec):
+    """Per-case streams calls replay captured launches with each call's iteration and record
+    slots; calls they cannot take (a field-statistics window, macroscopic output) run as split
+    steps in between, and the records, fields and states still equal stepping each case alone."""
+    cfgs = _cfgs()
+    b = mrlbm.Batch(cfgs, precision=prec)
+    b.set_schedule(9, mrlbm.BATCH_STREAMS, 6)
+    for c in b.cases:
+        c.field_stats_window(14, 19)
+    b.step(6)                                    # iterations 2..7: the periodic case's first step
+                                                 # carries its corner overrides: split steps
+    n0 = b.launch_count()
+    b.step(6)                                    # 8..13: one replay
+    per_step = 1 if prec == 32 else 2            # FP32 tile shapes: one launch per step
+    assert b.launch_count() - n0 == 6 * len(cfgs) * per_step
+    b.step(9)                                    # iterations 14..19 in the window: split; 20..22 replayed,
+                                                 # plot step 21 included
+    b.step(8, macro=True)                        # 23..28 replayed; 29..30 with fields: split
+    assert b.status() == 0
+    for cfg, c in zip(cfgs, b.cases):
+        ref = _alone(mrlbm, cfg, prec, 29, macro=True, fields=(14, 19))
+        assert np.array_equal(c.get_state(), ref["f"])
+        it, fd, fl, rin = c.forces()
+        assert np.array_equal(it, ref["forces"][0])
+        assert np.array_equal(fd, ref["forces"][1]) and np.array_equal(fl, ref["forces"][2])
+        assert np.array_equal(rin, ref["forces"][3])
+        m1, m2 = c.macro(), ref["macro"]
+        for k in m1:
+            assert np.array_equal(m1[k], m2[k]), k
+        f1, f2 = c.field_stats(), ref["fields"]
+        assert f1["n"] == f2["n"] == 6
+        for k in ("mean_u", "rms_v", "mean_p"):
+            assert np.array_equal(f1[k], f2[k]), k
     b.close()
