@@ -11,9 +11,10 @@
 // launch with three kinds of blocks, each node's contribution added atomically to
 // lambda^{n-1} at the slots it pulled (a slot can feed several nodes: stencils, the outlet
 // copy, corner wraps):
-//   * bulk nodes (fluid and solid, not edge columns, not curved-wall nodes): reverse mode
+//   * bulk nodes (fluid and solid, not edge nodes, not curved-wall nodes): reverse mode
 //     written out by hand: reconstruction -> collision -> moments (adjoint_bulk_node);
-//   * edge columns (inlet i = 1, outlet i = nx): one thread per (node, input), the node's
+//   * edge nodes (inlet column i = 1, outlet column i = nx, and with no-slip reference walls
+//     rows 1 and ny): one thread per (node, input), the node's
 //     local map evaluated on dual numbers carrying the derivative along that input, then
 //     contracted with lambda^n (the transposed Jacobian column); the inlet's extra input is
 //     u_in(j), whose column gives the inlet-profile gradient;
@@ -21,8 +22,9 @@
 //     bilinear stencil nodes, with the drag contribution of the node in the same pass.
 // The local maps below restate the FP64 step's arithmetic (step_fp64.cuh) for a generic
 // scalar; they cover the closures the adjoint supports: rotated strong curved-wall closure
-// with velocity and moment extrapolation, inlet and outlet edge closures (apply_bc), free-slip
-// or y-periodic top and bottom, no incompressible variants.
+// with velocity and moment extrapolation; inlet and outlet edge closures and no-slip
+// reference walls, each in its apply_bc and apply_bc_incomp form; free-slip or y-periodic top
+// and bottom; the incomp_bulk collision.
 #pragma once
 #include "adjoint.h"
 #include "step_fp64.cuh"
@@ -98,13 +100,19 @@ __device__ __forceinline__ MacS<S> moments_s(const S f[Q], double hm, double hp)
     return m;
 }
 
-// Collision and Hermite reconstruction (2d_mrlbm.f90:407-415, 445-457), no incomp_bulk.
+// Collision (2d_mrlbm.f90:407-415, incomp_bulk 419-428) and Hermite reconstruction
+// (2d_mrlbm.f90:445-457).
 template <class P, class S>
 __device__ __forceinline__ void collide_s(const P& p, const MacS<S>& m, S fo[Q]) {
     const double om = p.omega, om1 = p.omega1;
-    const S mxx = om1 * m.mxx + om * m.ux * m.ux;
-    const S myy = om1 * m.myy + om * m.uy * m.uy;
+    S mxx = om1 * m.mxx + om * m.ux * m.ux;
+    S myy = om1 * m.myy + om * m.uy * m.uy;
     const S mxy = om1 * m.mxy + om * m.ux * m.uy;
+    if (p.incomp_bulk) {
+        const S t = 0.5 * (((mxx + myy) - m.ux * m.ux) - m.uy * m.uy);
+        mxx = mxx - t;
+        myy = myy - t;
+    }
     const S a = 4.5 * mxx, b = 4.5 * myy, c = 9.0 * mxy;
     const S am = a * p.hm, ap = a * p.hp, bm = b * p.hm, bp = b * p.hp;
     const S t1 = 3.0 * m.ux, t2 = 3.0 * m.uy, t5 = 3.0 * (m.ux + m.uy), t8 = 3.0 * (m.ux - m.uy);
@@ -142,35 +150,87 @@ __device__ __forceinline__ void incoming_s(const S f[Q], int mask, double hm, do
     mxyI = c * inv;
 }
 
-// Edge column node (i = 1 inlet or i = nx outlet) of a free-slip / y-periodic case:
-// moments, Dirichlet values and the apply_bc closure (2d_mrlbm.f90:249-272, 1237-1366).
+// Domain-edge node (i, j): moments, Dirichlet values and the apply_bc / apply_bc_incomp closure
+// (2d_mrlbm.f90:249-272, 1237-1494): inlet column i = 1, outlet column i = nx (fn: the inputs
+// of node (nx - 1, j), whose moments it copies), and with no-slip reference walls rows 1 and
+// ny, whose closure wins at the corners.
 template <class P, class S>
-__device__ __forceinline__ void edge_map(const P& p, int i, const S f[Q], const S fn[Q], S uin, S fo[Q]) {
-    MacS<S> m = moments_s(f, p.hm, p.hp);
-    S rhoI, mxxI, myyI, mxyI;
-    if (i == 1) {
-        m.ux = uin;
-        m.uy = S(p.vinlet);
-        incoming_s(f, fp64::M_INLET, p.hm, p.hp, rhoI, mxxI, myyI, mxyI);
-        m.rho = (4.0 * rhoI + 3.0 * rhoI * mxxI) / (3.0 - 3.0 * m.ux);
-        const S rp = m.rho;
-        m.mxx = (rp + 9.0 * rhoI * mxxI + 3.0 * rp * m.ux) / (6.0 * rp);
-        m.myy = 6.0 * rhoI * myyI / (5.0 * rp);
-        m.mxy = 2.0 * rhoI * mxyI / rp;
-    } else {
+__device__ __forceinline__ void edge_map(const P& p, int i, int j, const S f[Q], const S fn[Q], S uin, S fo[Q]) {
+    const bool outlet = i == p.L.nx, inlet = i == 1;
+    const bool top = p.walls_ref && j == p.L.ny, bottom = p.walls_ref && j == 1;
+    const double hm = p.hm, hp = p.hp, om = p.omega;
+    MacS<S> m = moments_s(f, hm, hp);
+    if (outlet) {
         S r = fn[0];
         for (int k = 1; k < Q; ++k) r = r + fn[k];
         const S inv = 1.0 / r;
         m.rho = r;
         m.ux = (((((fn[1] - fn[3]) + fn[5]) - fn[6]) - fn[7]) + fn[8]) * inv;
         m.uy = (((((fn[2] - fn[4]) + fn[5]) + fn[6]) - fn[7]) - fn[8]) * inv;
-        incoming_s(f, fp64::M_OUTLET, p.hm, p.hp, rhoI, mxxI, myyI, mxyI);
+    }
+    if (inlet) {
+        m.ux = uin;
+        m.uy = S(p.vinlet);
+    }
+    S rhoI, mxxI, myyI, mxyI;
+    if (top || bottom) {
+        m.ux = S(0.0);
+        m.uy = S(0.0);
+        incoming_s(f, top ? fp64::M_TOP : fp64::M_BOTTOM, hm, hp, rhoI, mxxI, myyI, mxyI);
+        if (!p.incomp_bc) {
+            m.rho = 3.0 * rhoI * (4.0 + 3.0 * (1.0 - om) * myyI) / (9.0 + om);
+            const S rp = m.rho;
+            m.mxx = 6.0 * rhoI * mxxI / (5.0 * rp);
+            m.myy = (rp + 9.0 * rhoI * myyI) / (6.0 * rp);
+            m.mxy = 2.0 * rhoI * mxyI / rp;
+        } else {
+            m.rho = 6.0 * rhoI / 5.0;
+            m.mxx = S(0.0);
+            m.myy = S(0.0);
+            m.mxy = 5.0 * mxyI / 3.0;
+        }
+    } else if (inlet) {
+        incoming_s(f, fp64::M_INLET, hm, hp, rhoI, mxxI, myyI, mxyI);
+        if (!p.incomp_bc) {
+            m.rho = (4.0 * rhoI + 3.0 * rhoI * mxxI) / (3.0 - 3.0 * m.ux);
+            const S rp = m.rho;
+            m.mxx = (rp + 9.0 * rhoI * mxxI + 3.0 * rp * m.ux) / (6.0 * rp);
+            m.myy = 6.0 * rhoI * myyI / (5.0 * rp);
+            m.mxy = 2.0 * rhoI * mxyI / rp;
+        } else {
+            m.rho = 6.0 * rhoI / ((5.0 - 3.0 * m.ux) - 3.0 * (m.ux * m.ux));
+            const S rp = m.rho;
+            m.mxx = m.ux * m.ux;
+            m.myy = S(0.0);
+            m.mxy = 2.0 * rhoI * mxyI / rp;
+        }
+    } else if (outlet) {
+        incoming_s(f, fp64::M_OUTLET, hm, hp, rhoI, mxxI, myyI, mxyI);
         const S rp = m.rho;
-        m.mxx = (rp + 9.0 * rhoI * mxxI - 3.0 * rp * m.ux) / (6.0 * rp);
-        m.myy = 6.0 * rhoI * myyI / (5.0 * rp);
+        if (!p.incomp_bc) {
+            m.mxx = (rp + 9.0 * rhoI * mxxI - 3.0 * rp * m.ux) / (6.0 * rp);
+            m.myy = 6.0 * rhoI * myyI / (5.0 * rp);
+        } else {
+            m.mxx = m.ux * m.ux;
+            m.myy = m.uy * m.uy;
+        }
         m.mxy = (6.0 * rhoI * mxyI - rp * m.uy) / (3.0 * rp);
     }
     collide_s(p, m, fo);
+}
+
+// Edge node e of the adjoint's enumeration: column 1 (j = 1..ny), column nx, then, with
+// no-slip reference walls, rows 1 and ny without the corners.
+template <class P>
+__device__ __forceinline__ void edge_node_ij(const P& p, int e, int& i, int& j) {
+    const int nx = p.L.nx, ny = p.L.ny;
+    if (e < ny) { i = 1; j = e + 1; }
+    else if (e < 2 * ny) { i = nx; j = e - ny + 1; }
+    else {
+        const int q = e - 2 * ny, nr = nx - 2;
+        i = 2 + (q < nr ? q : q - nr);
+        j = q < nr ? 1 : ny;
+    }
 }
 
 template <class P>
@@ -311,6 +371,7 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int t
     if (t >= nx * ny) return;
     const int j = 1 + t / nx, i = t - (j - 1) * nx + 1;
     if (!p.xper && (i == 1 || i == nx)) return;            // edge columns: adjoint_edge
+    if (p.walls_ref && (j == 1 || j == ny)) return;        // no-slip wall rows: adjoint_edge
     const int cls = node_class(p, i, j);
     if (cls >= 0) return;                                  // curved-wall node: adjoint_wall
     const int64_t own = p.L.at(i, j, 0), plane = p.L.plane;
@@ -331,7 +392,13 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int t
     const bool u_zero = cls == CLS_SOLID && p.zero_solid_u;
     const double ux = u_zero ? 0.0 : m.ux, uy = u_zero ? 0.0 : m.uy;
     const double om = p.omega, om1 = p.omega1;
-    const double mxx = om1 * m.mxx + om * ux * ux, myy = om1 * m.myy + om * uy * uy, mxy = om1 * m.mxy + om * ux * uy;
+    double mxx = om1 * m.mxx + om * ux * ux, myy = om1 * m.myy + om * uy * uy;
+    const double mxy = om1 * m.mxy + om * ux * uy;
+    if (p.incomp_bulk) {                                   // m'' = m' - t I, t = (tr m' - |u|^2) / 2
+        const double t = 0.5 * (((mxx + myy) - ux * ux) - uy * uy);
+        mxx -= t;
+        myy -= t;
+    }
     double rb = 0.0, uxb = 0.0, uyb = 0.0, mxxb = 0.0, myyb = 0.0, mxyb = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
@@ -344,6 +411,13 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int t
         mxxb += 4.5 * hxx * Ab;
         myyb += 4.5 * hyy * Ab;
         mxyb += 9.0 * hxy * Ab;
+    }
+    if (p.incomp_bulk) {
+        const double tb = -(mxxb + myyb);
+        mxxb += 0.5 * tb;
+        myyb += 0.5 * tb;
+        uxb -= tb * ux;
+        uyb -= tb * uy;
     }
     // collision: m' = (1 - w) m + w u u
     uxb += om * (2.0 * ux * mxxb + uy * mxyb);
@@ -382,33 +456,35 @@ __device__ __forceinline__ void adjoint_bulk(const P& p, const AdjArgs& a, int t
     }
 }
 
-// Edge columns: thread (e, q), e over the 2 ny nodes of columns 1 and nx, q over 18 inputs:
-// own inputs 0..8; at the outlet the copied neighbour's inputs 9..17; at the inlet q = 9 is u_in(j).
+// Edge nodes: thread (e, q), e over the n_edge nodes of edge_node_ij, q over 18 inputs: own
+// inputs 0..8; at the outlet the copied neighbour's inputs 9..17; at the inlet q = 9 is u_in(j).
 template <class P>
 __device__ __forceinline__ void adjoint_edge(const P& p, const AdjArgs& a, int e, int q, const double* lam) {
     if (e >= a.n_edge) return;
-    const int ny = p.L.ny, nx = p.L.nx;
-    const int i = e < ny ? 1 : nx, j = 1 + (e < ny ? e : e - ny);
-    const bool inlet = i == 1;
-    if (inlet && q > 9) return;
+    const int nx = p.L.nx;
+    int i, j;
+    edge_node_ij(p, e, i, j);
+    const bool inlet = i == 1, outlet = i == nx;
+    if (q > 9 && !outlet) return;
+    if (q == 9 && !outlet && !inlet) return;
     double g[Q], gn[Q];
     gather_d(p, i, j, g);
-    if (!inlet) gather_d(p, nx - 1, j, gn);
+    if (outlet) gather_d(p, nx - 1, j, gn);
     Dual f[Q], fn[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         f[k] = Dual(g[k], q == k ? 1.0 : 0.0);
-        fn[k] = Dual(inlet ? 0.0 : gn[k], (!inlet && q == 9 + k) ? 1.0 : 0.0);
+        fn[k] = Dual(outlet ? gn[k] : 0.0, (outlet && q == 9 + k) ? 1.0 : 0.0);
     }
     const double u0 = p.u_in ? (double)p.u_in[j - 1] : (double)p.uinlet;
     const Dual uin(u0, (inlet && q == 9) ? 1.0 : 0.0);
     Dual fo[Q];
-    edge_map(p, i, f, fn, uin, fo);
+    edge_map(p, i, j, f, fn, uin, fo);
     double c = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) c += lam[k] * fo[k].d;
     if (q < 9) scatter(p, a, i, j, q, c);
-    else if (!inlet) scatter(p, a, nx - 1, j, q - 9, c);
+    else if (outlet) scatter(p, a, nx - 1, j, q - 9, c);
     else if (a.grad_uin) a.grad_uin[j - 1] += c;
     if (q == 0 && p.body) body_grad(p, a, i, j, lam);
 }
@@ -491,7 +567,8 @@ __global__ void __launch_bounds__(128) adjoint_aux(const __grid_constant__ P p, 
     if (t < 7 * Q) {
         const int e = e0 + t / Q, k = t % Q;
         if (e < a.n_edge) {
-            const int i = e < p.L.ny ? 1 : p.L.nx, j = 1 + (e < p.L.ny ? e : e - p.L.ny);
+            int i, j;
+            edge_node_ij(p, e, i, j);
             const int64_t at = p.L.at(i, j, k);
             lam[t / Q][k] = a.lam_in[at];
             a.lam_in[at] = 0.0;

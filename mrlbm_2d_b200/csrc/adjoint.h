@@ -12,7 +12,7 @@ struct AdjArgs {
     double* grad_body;         // [2 N] accumulated dJ/d(body force), or null
     double* grad_uin;          // [ny] accumulated dJ/d(u_in), or null
     double wJ;                 // weight of this step's drag in J (1/T inside the window, else 0)
-    int n_edge;                // edge-column nodes: 2 ny
+    int n_edge;                // edge nodes: 2 ny (columns 1 and nx), + 2 (nx - 2) with no-slip reference walls
     unsigned* done;            // bulk blocks of the step's bulk launch that have finished (zero between steps)
     // Bounding box of the curved-wall stencil nodes (empty: sx0 > sx1).  A slot of lambda^{n-1}
     // is pulled by one node only, except the slots a stencil node pulls (its wall node reads them

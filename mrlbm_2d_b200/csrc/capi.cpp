@@ -1476,10 +1476,10 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     if (!h || nsteps < 1 || window < 1 || window > nsteps || checkpoint_every < 1 || !J) return MRLBM_EINVAL;
     if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
     const mrlbm_config& c = h->cfg;
-    if (c.x_periodic || (c.wall_mode == MRLBM_WALL_REFERENCE && !c.y_periodic) || c.incomp_bc || c.incomp_bulk ||
+    if (c.x_periodic || h->halo_l || h->halo_r ||
         (h->geo.nb > 0 && (h->closure != CLOSURE_STRONG || !c.vel_interp || !c.mom_interp)))
-        return fail(h, MRLBM_EUNSUPPORTED,
-                    "adjoint: needs inlet/outlet columns, free-slip or y-periodic walls and the rotated strong closure");
+        return fail(h, MRLBM_EUNSUPPORTED, "adjoint: needs inlet/outlet columns and the rotated strong closure");
+    const bool walls_ref = c.wall_mode == MRLBM_WALL_REFERENCE && !c.y_periodic;
     CK(cudaSetDevice(h->device));
     int rc = drain_ring(h);
     if (rc != MRLBM_OK) return rc;
@@ -1611,7 +1611,7 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
             a.grad_body = gb;
             a.grad_uin = gu;
             a.wJ = n > N - T ? 1.0 / T : 0.0;
-            a.n_edge = 2 * h->L.ny;
+            a.n_edge = 2 * h->L.ny + (walls_ref ? 2 * (h->L.nx - 2) : 0);
             a.done = d_done;
             a.sx0 = sx0; a.sx1 = sx1; a.sy0 = sy0; a.sy1 = sy1;
             const bool ovr = n == 1 && h->ovr_live;

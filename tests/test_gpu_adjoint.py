@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from cases import CASES
-from mrlbm_2d_b200.config import cylinder_case
+from mrlbm_2d_b200.config import WALL_REFERENCE, cylinder_case
 
 pytestmark = pytest.mark.gpu
 
@@ -176,4 +176,34 @@ def test_adjoint_y_periodic_case_matches_central_differences(mrlbm):
     fd = (vals[0] - vals[1]) / (2 * eps)
     ad = float((gu * du).sum())
     assert abs(ad - fd) <= 1e-3 * abs(fd), (ad, fd)
+    s.close()
+
+
+@pytest.mark.parametrize("kw", [dict(wall_mode=WALL_REFERENCE), dict(incomp_bc=1, incomp_bulk=1),
+                                dict(wall_mode=WALL_REFERENCE, incomp_bc=1, incomp_bulk=1)])
+def test_adjoint_wall_and_incompressible_variants_match_central_differences(mrlbm, kw):
+    """No-slip reference walls (apply_bc wall rows, 2d_mrlbm.f90:1327-1359, their closure
+    winning at the corners) and the incompressible edge closures and bulk collision
+    (apply_bc_incomp, 2d_mrlbm.f90:1368-1494; 419-428): both parameter blocks against central
+    differences."""
+    s = mrlbm.Simulation(_case().replace(**kw))
+    body, uin = _params(s, 12)
+    s.set_body_force(body)
+    s.set_inlet_profile(uin)
+    N, T, K = 150, 60, 50
+    J, gb, gu = s.adjoint_drag(N, T, K)
+    assert np.all(np.isfinite(gb)) and np.all(np.isfinite(gu))
+    rng = np.random.default_rng(21)
+    eps = 1e-4
+    for _ in range(2):
+        db = 1e-5 * rng.standard_normal(body.shape)
+        du = 1e-3 * rng.standard_normal(uin.shape)
+        vals = []
+        for sgn in (1.0, -1.0):
+            s.set_body_force(body + sgn * eps * db)
+            s.set_inlet_profile(uin + sgn * eps * du)
+            vals.append(s.adjoint_drag(N, T, K, grads=False))
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        ad = float((gb * db).sum() + (gu * du).sum())
+        assert abs(ad - fd) <= 1e-3 * abs(fd) + 1e-15, (ad, fd)
     s.close()
