@@ -297,8 +297,9 @@ int mrlbm_set_body_force(mrlbm_handle* h, const double* g);
  * profile is set).  Discrete adjoint of the FP64 step: a forward pass keeps a checkpoint every
  * checkpoint_every steps; the backward pass recomputes each segment from its checkpoint and runs
  * the adjoint kernels step by step.  Either gradient pointer may be NULL; both NULL computes J
- * only.  Handles with inlet/outlet columns, free-slip or y-periodic walls and the rotated strong
- * closure (the defaults); MRLBM_EUNSUPPORTED otherwise.  On an FP32 handle the trajectory is the
+ * only.  Every wall, edge-closure, collision and curved-wall closure option of the step is
+ * differentiated; x-periodic lattices (no inlet or outlet) and x-slab handles return
+ * MRLBM_EUNSUPPORTED.  On an FP32 handle the trajectory is the
  * FP32 step's (checkpoints in FP32) and the adjoint arithmetic is FP64.  The device workspace
  * (nsteps / checkpoint_every + 2 x checkpoint_every population levels, two FP64 adjoint levels)
  * is allocated by the first call, grown when a later call needs more, and kept until

@@ -21,8 +21,9 @@
 //   * curved-wall nodes: likewise, over the node's 9 own inputs and the 72 inputs of its 8
 //     bilinear stencil nodes, with the drag contribution of the node in the same pass.
 // The local maps below restate the FP64 step's arithmetic (step_fp64.cuh) for a generic
-// scalar; they cover the closures the adjoint supports: rotated strong curved-wall closure
-// with velocity and moment extrapolation; inlet and outlet edge closures and no-slip
+// scalar; they cover every closure of the FP64 step: the curved-wall closures (rotated
+// strong, weak and rho_eq, unrotated with Cramer's rule, none) with or without velocity and
+// moment extrapolation; inlet and outlet edge closures and no-slip
 // reference walls, each in its apply_bc and apply_bc_incomp form; free-slip or y-periodic top
 // and bottom; the incomp_bulk collision.
 #pragma once
@@ -249,14 +250,123 @@ __device__ __forceinline__ void stencil_quad(const P& p, int l, int s, const S f
     my = m.mxx * s2q + m.myy * c2 - m.mxy * sn2;
 }
 
+// Rotated closures (2d_mrlbm.f90:1635-1765 strong, 1767-1871 weak, 1873-1972 rho_eq) of wall
+// node l for a generic scalar, as closure_rotated_body in step_fp64.cuh: density and the
+// rotated shear moment from the incoming populations, the extrapolated rotated normal moments
+// Mxx, Myy, then the moments rotated back.
+template <int variant, class P, class S>
+__device__ __forceinline__ void closure_rotated_s(const P& p, int l, const S f[Q], S uxp, S uyp, S Mxx, S Myy, MacS<S>& m) {
+    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const double omega = p.omega;
+    S rhoI = 0.0, mxyI = 0.0, A_p = 0.0, E_p = 0.0, D_xy = 0.0;
+    double B11 = 0, B22 = 0, B12 = 0, F11 = 0, F22 = 0, F12 = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double cxp = gf(p, G_CXP + k, l), cyp = gf(p, G_CYP + k, l);
+        const double hxx = gf(p, G_HXXP + k, l), hyy = gf(p, G_HYYP + k, l), hxy = gf(p, G_HXYP + k, l);
+        const double wk = p.w[k];
+        const S A_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp);
+        const S E_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp + 4.5 * (uxp * uxp) * hxx + 4.5 * (uyp * uyp) * hyy +
+                            9.0 * (uxp * uyp) * hxy);
+        const double B11_i = 4.5 * wk * hxx, B22_i = 4.5 * wk * hyy, B12_i = 4.5 * wk * hxy;
+        const bool o = (Os >> k) & 1, in = (Is >> k) & 1;
+        if constexpr (variant == CLOSURE_STRONG) if (o) { A_p = A_p + A_i; E_p = E_p + E_i; B11 += B11_i; B22 += B22_i; B12 += B12_i; }
+        if (in) {
+            rhoI = rhoI + f[k];
+            mxyI = mxyI + f[k] * hxy;
+            if constexpr (variant == CLOSURE_WEAK) { A_p = A_p + A_i; B11 += B11_i; B22 += B22_i; B12 += B12_i; }
+            if constexpr (variant == CLOSURE_RHOEQ) E_p = E_p + E_i;
+            D_xy = D_xy + A_i * hxy;
+            F11 += B11_i * hxy;
+            F22 += B22_i * hxy;
+            F12 += B12_i * hxy;
+        }
+    }
+    mxyI = mxyI / rhoI;
+    S Mxy;
+    if constexpr (variant == CLOSURE_STRONG) {
+        const S G_p = (1.0 - omega) * A_p + omega * E_p;
+        const double J11 = (1.0 - omega) * B11, J22 = (1.0 - omega) * B22, J12 = (1.0 - omega) * B12;
+        const S L11 = J11 * mxyI - F11, L22 = J22 * mxyI - F22, L12 = 2.0 * (J12 * mxyI - F12);
+        const S R = D_xy - G_p * mxyI;
+        Mxy = (R - Mxx * L11 - Myy * L22) / L12;
+        const S den = (1.0 - omega) * A_p + (1.0 - omega) * (Mxx * B11 + Myy * B22 + 2.0 * Mxy * B12) + omega * E_p;
+        m.rho = rhoI / den;
+    } else if constexpr (variant == CLOSURE_WEAK) {
+        const S L11 = B11 * mxyI - F11, L22 = B22 * mxyI - F22, L12 = 2.0 * (B12 * mxyI - F12);
+        const S R = D_xy - A_p * mxyI;
+        Mxy = (R - Mxx * L11 - Myy * L22) / L12;
+        const S den = A_p + (Mxx * B11 + Myy * B22 + 2.0 * Mxy * B12);
+        m.rho = rhoI / den;
+    } else {                                               // CLOSURE_RHOEQ
+        const S R = E_p * mxyI - D_xy;
+        Mxy = (R - Mxx * F11 - Myy * F22) / (2.0 * F12);
+        m.rho = rhoI / E_p;
+    }
+    const double cc = gf(p, G_CC, l), ss = gf(p, G_SS, l), s2 = gf(p, G_S2TH, l), c2 = gf(p, G_C2TH, l);
+    m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
+    m.myy = Mxx * ss + Myy * cc + Mxy * s2;
+    m.mxy = (Mxx - Myy) * 0.5 * s2 + Mxy * c2;
+}
+
+// Unrotated closure with Cramer's rule (2d_mrlbm.f90:1496-1633, 1974-2003) for a generic
+// scalar, as closure_unrotated in step_fp64.cuh.
+template <class P, class S>
+__device__ __forceinline__ void closure_unrotated_s(const P& p, int l, const S f[Q], S ux, S uy, MacS<S>& m) {
+    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
+    const double omega = p.omega, hm = p.hm, hp = p.hp;
+    S rhoI = 0.0, mxxI = 0.0, myyI = 0.0, mxyI = 0.0, A_p = 0.0, E_p = 0.0, D_xx = 0.0, D_yy = 0.0, D_xy = 0.0;
+    double B11 = 0, B22 = 0, B12 = 0, F11_xx = 0, F12_xx = 0, F22_xx = 0, F11_yy = 0, F12_yy = 0, F22_yy = 0;
+    double F11_xy = 0, F12_xy = 0, F22_xy = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double hxx = ex(k) != 0 ? hp : hm, hyy = ey(k) != 0 ? hp : hm, hxy = (double)(ex(k) * ey(k));
+        const double wk = p.w[k];
+        const S A_i = wk * (1.0 + 3.0 * ux * (double)ex(k) + 3.0 * uy * (double)ey(k));
+        const S E_i = wk * (1.0 + 3.0 * ux * (double)ex(k) + 3.0 * uy * (double)ey(k) + 4.5 * (ux * ux) * hxx +
+                            4.5 * (uy * uy) * hyy + 9.0 * (ux * uy) * hxy);
+        const double B11_i = 4.5 * wk * hxx, B22_i = 4.5 * wk * hyy, B12_i = 4.5 * wk * hxy;
+        if ((Os >> k) & 1) { A_p = A_p + A_i; E_p = E_p + E_i; B11 += B11_i; B22 += B22_i; B12 += B12_i; }
+        if ((Is >> k) & 1) {
+            rhoI = rhoI + f[k];
+            mxxI = mxxI + f[k] * hxx;
+            myyI = myyI + f[k] * hyy;
+            mxyI = mxyI + f[k] * hxy;
+            D_xx = D_xx + A_i * hxx; D_yy = D_yy + A_i * hyy; D_xy = D_xy + A_i * hxy;
+            F11_xx += B11_i * hxx; F22_xx += B22_i * hxx; F12_xx += B12_i * hxx;
+            F11_yy += B11_i * hyy; F22_yy += B22_i * hyy; F12_yy += B12_i * hyy;
+            F11_xy += B11_i * hxy; F22_xy += B22_i * hxy; F12_xy += B12_i * hxy;
+        }
+    }
+    const S inv = 1.0 / rhoI;
+    mxxI = mxxI * inv;
+    myyI = myyI * inv;
+    mxyI = mxyI * inv;
+    const S G_p = (1.0 - omega) * A_p + omega * E_p;
+    const double J11 = (1.0 - omega) * B11, J22 = (1.0 - omega) * B22, J12 = (1.0 - omega) * B12;
+    const S a1 = J11 * mxxI - F11_xx, b1 = J22 * mxxI - F22_xx, c1 = 2.0 * (J12 * mxxI - F12_xx);
+    const S a2 = J11 * myyI - F11_yy, b2 = J22 * myyI - F22_yy, c2 = 2.0 * (J12 * myyI - F12_yy);
+    const S a3 = J11 * mxyI - F11_xy, b3 = J22 * mxyI - F22_xy, c3 = 2.0 * (J12 * mxyI - F12_xy);
+    const S d1 = D_xx - G_p * mxxI, d2 = D_yy - G_p * myyI, d3 = D_xy - G_p * mxyI;
+    const S denom = a3 * b2 * c1 - a2 * b3 * c1 - a3 * b1 * c2 + a1 * b3 * c2 + a2 * b1 * c3 - a1 * b2 * c3;
+    const S Mxx = -((-b3 * c2 * d1 + b2 * c3 * d1 + b3 * c1 * d2 - b1 * c3 * d2 - b2 * c1 * d3 + b1 * c2 * d3) / denom);
+    const S Myy = -((a3 * c2 * d1 - a2 * c3 * d1 - a3 * c1 * d2 + a1 * c3 * d2 + a2 * c1 * d3 - a1 * c2 * d3) / denom);
+    const S Mxy = -((-a3 * b2 * d1 + a2 * b3 * d1 + a3 * b1 * d2 - a1 * b3 * d2 - a2 * b1 * d3 + a1 * b2 * d3) / denom);
+    const S den = (1.0 - omega) * A_p + (1.0 - omega) * (Mxx * B11 + Myy * B22 + 2.0 * Mxy * B12) + omega * E_p;
+    m.rho = rhoI / den;
+    m.mxx = Mxx;
+    m.myy = Myy;
+    m.mxy = Mxy;
+}
+
 // Curved-wall node l from its own inputs f and its 8 stencil nodes' (u, v, mx, my): bilinear
-// interpolation at reference points 2 and 3, extrapolation to the node, rotated strong
-// closure, collision (2d_mrlbm.f90:294-311, 768-928, 1635-1765, 407-457) and the node's drag
-// term (2d_mrlbm.f90:558-591).
+// interpolation at reference points 2 and 3, extrapolation to the node, the closure the case
+// selects, collision (2d_mrlbm.f90:294-311, 768-928, 1496-2003, 407-457; the order of
+// boundary_close_core in step_fp64.cuh) and the node's drag term (2d_mrlbm.f90:558-591).
 // The eight stencil nodes' u, v and rotated moments come as plain values (qd[kind][t]); the
 // one stencil node s whose inputs carry the derivative (s < 0: none) comes as duals.  Each
 // operand is formed where it is used, so no per-thread array of stencil duals exists.
-template <class P, class S>
+template <int CL, class P, class S>
 __device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const double (*qd)[8], int s, S us, S vs,
                                          S mxs, S mys, S fo[Q], S& drag) {
     auto val = [&](int kind, int t) -> S {
@@ -282,50 +392,27 @@ __device__ __forceinline__ void wall_map(const P& p, int l, const S f[Q], const 
         my[r] = (1.0 - yd) * row_my[0] + yd * row_my[1];
     }
     const double t2 = gf(p, G_T2, l), t3 = gf(p, G_T3, l);
+    constexpr bool rotated = CL != CLOSURE_UNROTATED;
+    // the node's own moments survive only where no closure or extrapolation replaces them
     MacS<S> m;
-    m.ux = t2 * u[0] - t3 * u[1];
-    m.uy = t2 * v[0] - t3 * v[1];
-    const S Mxx = t2 * mx[0] - t3 * mx[1];
-    const S Myy = t2 * my[0] - t3 * my[1];
-    const double c = gf(p, G_CTH, l), sn = gf(p, G_STH, l);
-    const S uxp = m.ux * c + m.uy * sn;
-    const S uyp = m.uy * c - m.ux * sn;
-    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
-    const double omega = p.omega;
-    S rhoI = 0.0, mxyI = 0.0, A_p = 0.0, E_p = 0.0, D_xy = 0.0;
-    double B11 = 0, B22 = 0, B12 = 0, F11 = 0, F22 = 0, F12 = 0;
-#pragma unroll
-    for (int k = 0; k < Q; ++k) {
-        const double cxp = gf(p, G_CXP + k, l), cyp = gf(p, G_CYP + k, l);
-        const double hxx = gf(p, G_HXXP + k, l), hyy = gf(p, G_HYYP + k, l), hxy = gf(p, G_HXYP + k, l);
-        const double wk = p.w[k];
-        const S A_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp);
-        const S E_i = wk * (1.0 + 3.0 * uxp * cxp + 3.0 * uyp * cyp + 4.5 * (uxp * uxp) * hxx + 4.5 * (uyp * uyp) * hyy +
-                            9.0 * (uxp * uyp) * hxy);
-        const double B11_i = 4.5 * wk * hxx, B22_i = 4.5 * wk * hyy, B12_i = 4.5 * wk * hxy;
-        if ((Os >> k) & 1) { A_p = A_p + A_i; E_p = E_p + E_i; B11 += B11_i; B22 += B22_i; B12 += B12_i; }
-        if ((Is >> k) & 1) {
-            rhoI = rhoI + f[k];
-            mxyI = mxyI + f[k] * hxy;
-            D_xy = D_xy + A_i * hxy;
-            F11 += B11_i * hxy;
-            F22 += B22_i * hxy;
-            F12 += B12_i * hxy;
-        }
+    if (CL == CLOSURE_NONE || (rotated && !p.vel_interp)) m = moments_s(f, p.hm, p.hp);
+    if (!rotated || p.vel_interp) {
+        m.ux = t2 * u[0] - t3 * u[1];
+        m.uy = t2 * v[0] - t3 * v[1];
     }
-    mxyI = mxyI / rhoI;
-    const S G_p = (1.0 - omega) * A_p + omega * E_p;
-    const double J11 = (1.0 - omega) * B11, J22 = (1.0 - omega) * B22, J12 = (1.0 - omega) * B12;
-    const S L11 = J11 * mxyI - F11, L22 = J22 * mxyI - F22, L12 = 2.0 * (J12 * mxyI - F12);
-    const S R = D_xy - G_p * mxyI;
-    const S Mxy = (R - Mxx * L11 - Myy * L22) / L12;
-    const S den = (1.0 - omega) * A_p + (1.0 - omega) * (Mxx * B11 + Myy * B22 + 2.0 * Mxy * B12) + omega * E_p;
-    m.rho = rhoI / den;
-    const double cc = gf(p, G_CC, l), ss = gf(p, G_SS, l), s2 = gf(p, G_S2TH, l), c2 = gf(p, G_C2TH, l);
-    m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
-    m.myy = Mxx * ss + Myy * cc + Mxy * s2;
-    m.mxy = (Mxx - Myy) * 0.5 * s2 + Mxy * c2;
+    S Mxx = 0.0, Myy = 0.0;
+    if (rotated && p.mom_interp) {
+        Mxx = t2 * mx[0] - t3 * mx[1];
+        Myy = t2 * my[0] - t3 * my[1];
+    }
+    if constexpr (CL == CLOSURE_UNROTATED) {
+        closure_unrotated_s(p, l, f, m.ux, m.uy, m);
+    } else if constexpr (CL != CLOSURE_NONE) {
+        const double c = gf(p, G_CTH, l), sn = gf(p, G_STH, l);
+        closure_rotated_s<CL>(p, l, f, m.ux * c + m.uy * sn, m.uy * c - m.ux * sn, Mxx, Myy, m);
+    }
     collide_s(p, m, fo);
+    const int Is = gi(p, I_IS, l), Os = gi(p, I_OS, l);
     S fxo = 0.0, fxi = 0.0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
@@ -493,7 +580,7 @@ __device__ __forceinline__ void adjoint_edge(const P& p, const AdjArgs& a, int e
 // its 8 stencil nodes) and the stencil quantities in shared memory; thread q < 81 then runs
 // the node's map with the derivative along input q (only its stencil node's quantities carry
 // a derivative) and scatters the contracted column.
-template <class P>
+template <int CL, class P>
 __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l) {
     __shared__ double in[81], lam[Q], qd[4][8];
     __shared__ int slot[81];
@@ -541,7 +628,7 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
         stencil_quad(p, l, s, g, us, vs, mxs, mys);    // only stencil s depends on input q
     }
     Dual fo[Q], drag;
-    wall_map(p, l, f, qd, s, us, vs, mxs, mys, fo, drag);
+    wall_map<CL>(p, l, f, qd, s, us, vs, mxs, mys, fo, drag);
     double c = a.wJ * drag.d;
 #pragma unroll
     for (int k = 0; k < Q; ++k) c += lam[k] * fo[k].d;
@@ -553,12 +640,12 @@ __device__ __forceinline__ void adjoint_wall(const P& p, const AdjArgs& a, int l
 // maps get the registers they need, then the bulk blocks (128 nodes each), which start once the
 // first launch has waited for the previous step and run beside it; the last bulk block to finish
 // waits for the first launch, so the step completes as a whole.
-template <class P>
+template <class P, int CL>
 __global__ void __launch_bounds__(128) adjoint_aux(const __grid_constant__ P p, const __grid_constant__ AdjArgs a) {
     wait_prior_grid();
     const int b = (int)blockIdx.x;
     if (b < p.nb) {
-        adjoint_wall(p, a, b);
+        adjoint_wall<CL>(p, a, b);
         return;
     }
     // lambda^n of the block's 7 edge nodes, staged once and cleared for reuse

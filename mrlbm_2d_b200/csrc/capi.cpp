@@ -643,8 +643,6 @@ static int create_impl(const mrlbm_config* cfg, int precision, int device, int s
     else h->closure = CLOSURE_NONE;
     if (!make_dev_consts(h) && precision == MRLBM_FP32)
         return bail(MRLBM_EUNSUPPORTED, "FP32 closure needs equal Is/Os weight sums for every label");
-    if (precision == MRLBM_FP32 && c.channel_with_cylinder && h->closure != CLOSURE_STRONG && h->closure != CLOSURE_NONE)
-        return bail(MRLBM_EUNSUPPORTED, "the FP32 step implements only the default rotated strong-mass closure");
 
     h->L = make_layout(nx, ny, precision == MRLBM_FP64 ? 16 : 32);
     if (h->L.total() >= (int64_t)1 << 31) return bail(MRLBM_EINVAL, "grid too large for one handle (2^31 populations)");
@@ -1476,9 +1474,8 @@ extern "C" int mrlbm_adjoint_drag(mrlbm_handle* h, int32_t nsteps, int32_t windo
     if (!h || nsteps < 1 || window < 1 || window > nsteps || checkpoint_every < 1 || !J) return MRLBM_EINVAL;
     if (h->host_only) return fail(h, MRLBM_ENODEVICE, "host-only handle (created with device -1)");
     const mrlbm_config& c = h->cfg;
-    if (c.x_periodic || h->halo_l || h->halo_r ||
-        (h->geo.nb > 0 && (h->closure != CLOSURE_STRONG || !c.vel_interp || !c.mom_interp)))
-        return fail(h, MRLBM_EUNSUPPORTED, "adjoint: needs inlet/outlet columns and the rotated strong closure");
+    if (c.x_periodic || h->halo_l || h->halo_r)
+        return fail(h, MRLBM_EUNSUPPORTED, "adjoint: needs inlet/outlet columns and a whole (not x-slab) lattice");
     const bool walls_ref = c.wall_mode == MRLBM_WALL_REFERENCE && !c.y_periodic;
     CK(cudaSetDevice(h->device));
     int rc = drain_ring(h);

@@ -7,8 +7,8 @@
 // arithmetic but not with single-rounded weights) are folded into constants computed once
 // in FP64 on the host (DevConsts).  The mass drift the reference has because
 // sum(w) = 1 + 7.45e-9 is kept (eps_mass).  Forces are accumulated in FP64 from
-// w_k + g_k.  Only the default curved-wall closure (numerical_boundary_cases_rotation,
-// 2d_mrlbm.f90:1635-1765) has an FP32 form.
+// w_k + g_k.  Every curved-wall closure of the FP64 step has an FP32 form (rotated strong,
+// weak and rho_eq, unrotated with Cramer's rule, none).
 #pragma once
 #include "step_common.cuh"
 
@@ -186,13 +186,19 @@ __device__ __forceinline__ void stencil_node(const P& p, int si, int sj, float c
     my = m.mxx * ss + m.myy * cc - m.mxy * s2;
 }
 
-// numerical_boundary_cases_rotation (2d_mrlbm.f90:1635-1765) in deviation form.  With
-// W = sum_{Is} w = sum_{Os} w (equal for every handled label), the closure's O(1) parts
-// cancel exactly:  rho_I = W + G,  G' = W + (a1 + omega e2),  D_xy = SW_xy + d1, so
-//   R_xy = d1 - SG_xy - S_xy (a1 + omega e2 - G) / rho_I,
-//   den  = W + dden,  dden = a1 + (1-omega)(M'.B') + omega e2,  drho = (G - dden) / den.
-__device__ __forceinline__ void closure_strong(const P& p, const BTab<float>& tb, int li, const float g[Q], float uxp,
-                                            float uyp, float Mxx, float Myy, Mac& m) {
+// The rotated closures in deviation form: numerical_boundary_cases_rotation (strong,
+// 2d_mrlbm.f90:1635-1765), _weak (1767-1871) and _rhoeq (1873-1972).  With
+// W = sum_{Is} w = sum_{Os} w (equal for every handled label), a_k = 3 w_k c'.u' and
+// e_k = 4.5 w_k (u'u' : H'_k), the closures' O(1) parts cancel exactly:  rho_I = W + G and
+// D_xy = SW_xy + d1 (d1 = sum_{Is} a_k H'xy_k); with gp the small part of the closure's
+// reference sum (strong: G' = W + a1 + omega e2 over Os; weak: A' = W + a1 over Is; rho_eq:
+// E' = W + a1 + e2 over Is),
+//   R_xy = d1 - SG_xy - S_xy (gp - G) / rho_I   (rho_eq: its negative),
+//   den  = W + dden,  drho = (G - dden) / den,
+// dden = gp (+ (1 - omega) M'.B' strong, + M'.B' weak), B' summed where the closure sums it.
+template <int VARIANT>
+__device__ __forceinline__ void closure_rotated32(const P& p, const BTab<float>& tb, int li, const float g[Q], float uxp,
+                                                  float uyp, float Mxx, float Myy, Mac& m) {
     const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
     const int label = tb.gi(I_LABEL, li);
     const float om = p.omega, om1 = p.omega1;
@@ -206,7 +212,8 @@ __device__ __forceinline__ void closure_strong(const P& p, const BTab<float>& tb
         const float ak = 3.0f * wk * (uxp * cxp + uyp * cyp);
         const float ek = 4.5f * wk * ((uxp * uxp) * hxx + (uyp * uyp) * hyy + 2.0f * (uxp * uyp) * hxy);
         const float b11 = 4.5f * wk * hxx, b22 = 4.5f * wk * hyy, b12 = 4.5f * wk * hxy;
-        if ((Os >> k) & 1) { a1 += ak; e2 += ek; B11 += b11; B22 += b22; B12 += b12; }
+        const bool sum_here = VARIANT == CLOSURE_STRONG ? ((Os >> k) & 1) : ((Is >> k) & 1);
+        if (sum_here) { a1 += ak; e2 += ek; B11 += b11; B22 += b22; B12 += b12; }
         if ((Is >> k) & 1) {
             G += g[k];
             SWxy += wk * hxy;
@@ -221,16 +228,107 @@ __device__ __forceinline__ void closure_strong(const P& p, const BTab<float>& tb
     const float rhoI = W + G;
     const float Sxy = SWxy + SGxy;
     const float mxyI = Sxy / rhoI;
-    const float L11 = om1 * B11 * mxyI - F11, L22 = om1 * B22 * mxyI - F22, L12 = 2.0f * (om1 * B12 * mxyI - F12);
-    const float R = d1 - SGxy - Sxy * ((a1 + om * e2) - G) / rhoI;
-    const float Mxy = (R - Mxx * L11 - Myy * L22) / L12;
-    const float dden = a1 + om1 * (Mxx * B11 + Myy * B22 + 2.0f * Mxy * B12) + om * e2;
+    float Mxy, dden;
+    if constexpr (VARIANT == CLOSURE_STRONG) {
+        const float L11 = om1 * B11 * mxyI - F11, L22 = om1 * B22 * mxyI - F22, L12 = 2.0f * (om1 * B12 * mxyI - F12);
+        const float R = d1 - SGxy - Sxy * ((a1 + om * e2) - G) / rhoI;
+        Mxy = (R - Mxx * L11 - Myy * L22) / L12;
+        dden = a1 + om1 * (Mxx * B11 + Myy * B22 + 2.0f * Mxy * B12) + om * e2;
+    } else if constexpr (VARIANT == CLOSURE_WEAK) {
+        const float L11 = B11 * mxyI - F11, L22 = B22 * mxyI - F22, L12 = 2.0f * (B12 * mxyI - F12);
+        const float R = d1 - SGxy - Sxy * (a1 - G) / rhoI;
+        Mxy = (R - Mxx * L11 - Myy * L22) / L12;
+        dden = a1 + (Mxx * B11 + Myy * B22 + 2.0f * Mxy * B12);
+    } else {                                                // CLOSURE_RHOEQ
+        const float R = SGxy - d1 + Sxy * ((a1 + e2) - G) / rhoI;
+        Mxy = (R - Mxx * F11 - Myy * F22) / (2.0f * F12);
+        dden = a1 + e2;
+    }
     m.drho = (G - dden) / (W + dden);
     m.rho = 1.0f + m.drho;
     const float cc = tb.gf(G_CC, li), ss = tb.gf(G_SS, li), s2 = tb.gf(G_S2TH, li), c2 = tb.gf(G_C2TH, li);
     m.mxx = Mxx * cc + Myy * ss - Mxy * s2;
     m.myy = Mxx * ss + Myy * cc + Mxy * s2;
     m.mxy = (Mxx - Myy) * 0.5f * s2 + Mxy * c2;
+}
+
+// numerical_boundary_cases + solve_system (2d_mrlbm.f90:1496-1633, 1974-2003) in deviation
+// form: the same 3 x 3 system for (Mxx, Myy, Mxy) by Cramer's rule, its coefficients O(1) and
+// its right-hand side rearranged so the O(1) parts cancel exactly (S_ab = SW_ab + SG_ab,
+// D_ab = SW_ab + d_ab, G' = W + gp with gp = a1 + omega e2 over Os):
+//   rhs_ab = d_ab + (SW_ab (G - gp) - (W + gp) SG_ab) / rho_I,
+// so a node at rest gives M = 0 exactly; drho = (G - dden) / (W + dden) with
+// dden = gp + (1 - omega) M.B.
+__device__ __forceinline__ void closure_unrotated32(const P& p, const BTab<float>& tb, int li, const float g[Q], float ux,
+                                                    float uy, Mac& m) {
+    const int Is = tb.gi(I_IS, li), Os = tb.gi(I_OS, li);
+    const int label = tb.gi(I_LABEL, li);
+    const float om = p.omega, om1 = p.omega1, hm = p.hm, hp = p.hp;
+    float a1 = 0.f, e2 = 0.f, B11 = 0.f, B22 = 0.f, B12 = 0.f, G = 0.f;
+    float SW[3] = {0.f, 0.f, 0.f}, SG[3] = {0.f, 0.f, 0.f}, dd[3] = {0.f, 0.f, 0.f};
+    float F11[3] = {0.f, 0.f, 0.f}, F22[3] = {0.f, 0.f, 0.f}, F12[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const float h[3] = {hxx_of(k, hm, hp), hyy_of(k, hm, hp), (float)(ex(k) * ey(k))};
+        const float wk = p.w[k];
+        const float ak = 3.0f * wk * (ux * (float)ex(k) + uy * (float)ey(k));
+        const float ek = 4.5f * wk * ((ux * ux) * h[0] + (uy * uy) * h[1] + 2.0f * (ux * uy) * h[2]);
+        const float b11 = 4.5f * wk * h[0], b22 = 4.5f * wk * h[1], b12 = 4.5f * wk * h[2];
+        if ((Os >> k) & 1) { a1 += ak; e2 += ek; B11 += b11; B22 += b22; B12 += b12; }
+        if ((Is >> k) & 1) {
+            G += g[k];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                SW[r] += wk * h[r];
+                SG[r] += g[k] * h[r];
+                dd[r] += ak * h[r];
+                F11[r] += b11 * h[r];
+                F22[r] += b22 * h[r];
+                F12[r] += b12 * h[r];
+            }
+        }
+    }
+    const float W = p.dc.lab_w[label];
+    const float rhoI = W + G;
+    const float gp = a1 + om * e2;
+    float A[3], Bc[3], C[3], D[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const float mI = (SW[r] + SG[r]) / rhoI;
+        A[r] = om1 * B11 * mI - F11[r];
+        Bc[r] = om1 * B22 * mI - F22[r];
+        C[r] = 2.0f * (om1 * B12 * mI - F12[r]);
+        D[r] = dd[r] + (SW[r] * (G - gp) - (W + gp) * SG[r]) / rhoI;
+    }
+    const float a1_ = A[0], b1 = Bc[0], c1 = C[0], a2 = A[1], b2 = Bc[1], c2 = C[1], a3 = A[2], b3 = Bc[2], c3 = C[2];
+    const float d1 = D[0], d2 = D[1], d3 = D[2];
+    const float denom = a3 * b2 * c1 - a2 * b3 * c1 - a3 * b1 * c2 + a1_ * b3 * c2 + a2 * b1 * c3 - a1_ * b2 * c3;
+    const float Mxx = -((-b3 * c2 * d1 + b2 * c3 * d1 + b3 * c1 * d2 - b1 * c3 * d2 - b2 * c1 * d3 + b1 * c2 * d3) / denom);
+    const float Myy = -((a3 * c2 * d1 - a2 * c3 * d1 - a3 * c1 * d2 + a1_ * c3 * d2 + a2 * c1 * d3 - a1_ * c2 * d3) / denom);
+    const float Mxy = -((-a3 * b2 * d1 + a2 * b3 * d1 + a3 * b1 * d2 - a1_ * b3 * d2 - a2 * b1 * d3 + a1_ * b2 * d3) / denom);
+    const float dden = gp + om1 * (Mxx * B11 + Myy * B22 + 2.0f * Mxy * B12);
+    m.drho = (G - dden) / (W + dden);
+    m.rho = 1.0f + m.drho;
+    m.mxx = Mxx;
+    m.myy = Myy;
+    m.mxy = Mxy;
+}
+
+// The closures other than the default one, out of line: inlined, their registers would be
+// reserved in every kernel that carries the wall path, the bulk tiles of one-launch steps
+// included.  The populations travel by value.
+struct Pops32 { float v[Q]; };
+static __device__ __noinline__ Mac closure_other32(const P& p, const BTab<float>& tb, int li, Pops32 g, float ux, float uy,
+                                                   float mxxp, float myyp, Mac m) {
+    if (p.closure == CLOSURE_UNROTATED) {
+        closure_unrotated32(p, tb, li, g.v, ux, uy, m);
+    } else {
+        const float c = tb.gf(G_CTH, li), s = tb.gf(G_STH, li);
+        const float uxp = ux * c + uy * s, uyp = uy * c - ux * s;
+        if (p.closure == CLOSURE_WEAK) closure_rotated32<CLOSURE_WEAK>(p, tb, li, g.v, uxp, uyp, mxxp, myyp, m);
+        else closure_rotated32<CLOSURE_RHOEQ>(p, tb, li, g.v, uxp, uyp, mxxp, myyp, m);
+    }
+    return m;
 }
 
 // Lane 0 of a boundary node: extrapolation (wall value 0), closure, collision, store and
@@ -250,11 +348,17 @@ __device__ __forceinline__ void boundary_close(const P& p, const BTab<float>& tb
     Mac m = moments(p, g);
     float mxxp = 0.f, myyp = 0.f;
     const float t2 = tb.gf(G_T2, li), t3 = tb.gf(G_T3, li);
-    if (p.vel_interp) { m.ux = t2 * ux2 - t3 * ux3; m.uy = t2 * uy2 - t3 * uy3; }
-    if (p.mom_interp) { mxxp = t2 * mx2 - t3 * mx3; myyp = t2 * my2 - t3 * my3; }
+    const bool rotated = p.closure != CLOSURE_UNROTATED;
+    if (!rotated || p.vel_interp) { m.ux = t2 * ux2 - t3 * ux3; m.uy = t2 * uy2 - t3 * uy3; }
+    if (rotated && p.mom_interp) { mxxp = t2 * mx2 - t3 * mx3; myyp = t2 * my2 - t3 * my3; }
     if (p.closure == CLOSURE_STRONG) {
         const float c = tb.gf(G_CTH, li), s = tb.gf(G_STH, li);
-        closure_strong(p, tb, li, g, m.ux * c + m.uy * s, m.uy * c - m.ux * s, mxxp, myyp, m);
+        closure_rotated32<CLOSURE_STRONG>(p, tb, li, g, m.ux * c + m.uy * s, m.uy * c - m.ux * s, mxxp, myyp, m);
+    } else if (p.closure != CLOSURE_NONE) {
+        Pops32 gv;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) gv.v[k] = g[k];
+        m = closure_other32(p, tb, li, gv, m.ux, m.uy, mxxp, myyp, m);
     }
     if (!(m.rho > 0.0f)) flag_bad_density(p);
     if (FULL && p.macro) store_macro(p, i, j, 1.0 + (double)m.drho, m.ux, m.uy, m.mxx, m.myy, m.mxy);

@@ -152,6 +152,7 @@ def test_fp32_adjoint_tracks_fp64_adjoint(mrlbm):
 
 
 def test_adjoint_rejects_unsupported_cases(mrlbm):
+    """x-periodic lattices have no inlet or outlet to differentiate through."""
     s = mrlbm.Simulation(CASES["freeslip_xperiodic"]())
     with pytest.raises(mrlbm.MrlbmError):
         s.adjoint_drag(10, 5, 5)
@@ -180,11 +181,15 @@ def test_adjoint_y_periodic_case_matches_central_differences(mrlbm):
 
 
 @pytest.mark.parametrize("kw", [dict(wall_mode=WALL_REFERENCE), dict(incomp_bc=1, incomp_bulk=1),
-                                dict(wall_mode=WALL_REFERENCE, incomp_bc=1, incomp_bulk=1)])
-def test_adjoint_wall_and_incompressible_variants_match_central_differences(mrlbm, kw):
+                                dict(wall_mode=WALL_REFERENCE, incomp_bc=1, incomp_bulk=1),
+                                dict(strong_mass_bc=0, weak_mass_bc=1), dict(strong_mass_bc=0, eq_mass_bc=1),
+                                dict(rotated_coordinate=0), dict(vel_interp=0), dict(strong_mass_bc=0)])
+def test_adjoint_wall_and_closure_variants_match_central_differences(mrlbm, kw):
     """No-slip reference walls (apply_bc wall rows, 2d_mrlbm.f90:1327-1359, their closure
-    winning at the corners) and the incompressible edge closures and bulk collision
-    (apply_bc_incomp, 2d_mrlbm.f90:1368-1494; 419-428): both parameter blocks against central
+    winning at the corners), the incompressible edge closures and bulk collision
+    (apply_bc_incomp, 2d_mrlbm.f90:1368-1494; 419-428), and the curved-wall closure variants
+    (weak 1767-1871, rho_eq 1873-1972, unrotated with Cramer's rule 1496-1633 and 1974-2003, no
+    velocity extrapolation, no mass closure): both parameter blocks against central
     differences."""
     s = mrlbm.Simulation(_case().replace(**kw))
     body, uin = _params(s, 12)

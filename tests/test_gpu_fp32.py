@@ -41,7 +41,8 @@ def test_fp32_tracks_fp64_benchmark_small(mrlbm):
 
 
 @pytest.mark.parametrize("name", ["reference_default_bcs", "reference_walls", "reference_walls_incomp",
-                                  "x_and_y_periodic", "freeslip_label15", "periodic_channel_no_cylinder"])
+                                  "x_and_y_periodic", "freeslip_label15", "periodic_channel_no_cylinder",
+                                  "closure_weak", "closure_rhoeq", "closure_unrotated", "no_velocity_interp"])
 def test_fp32_boundary_variants_track_fp64(mrlbm, name):
     cfg = CASES[name]()
     r = _pair(mrlbm, cfg, 200)
@@ -50,9 +51,3 @@ def test_fp32_boundary_variants_track_fp64(mrlbm, name):
     assert np.abs(m32["ux"] - m64["ux"]).max() / scale < 1e-4
     assert np.abs(m32["uy"] - m64["uy"]).max() / scale < 1e-4
     assert np.abs(m32["rho"] - m64["rho"]).max() < 1e-5
-
-
-def test_fp32_rejects_other_closures(mrlbm):
-    with pytest.raises(mrlbm.MrlbmError) as e:
-        mrlbm.Simulation(CASES["closure_weak"](), precision=mrlbm.FP32)
-    assert e.value.code == 4
