@@ -357,7 +357,9 @@ int mrlbm_slabs_step(mrlbm_handle** hs, int32_t n, int32_t nsteps);
  * MRLBM_BATCH_GRAPH instead).  Each case's results are bit-identical to stepping it alone.  The
  * cases are ordinary handles owned by the batch (mrlbm_batch_case): read their forces,
  * fields and state, load states, set inlet profiles and field-statistics windows with the
- * single-case calls, but step them only through mrlbm_batch_step and do not destroy them. */
+ * single-case calls, but step them only through mrlbm_batch_step and do not destroy them.
+ * Surface-pressure records (mrlbm_surface_enable) are taken by single-case steps only: a
+ * batch step with such a case returns MRLBM_EUNSUPPORTED. */
 typedef struct mrlbm_batch mrlbm_batch;
 #define MRLBM_BATCH_PERSISTENT 0
 #define MRLBM_BATCH_GRAPH      1

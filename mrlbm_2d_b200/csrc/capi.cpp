@@ -1906,6 +1906,10 @@ int batch_call_streams(mrlbm_batch* b, int steps) {
 // One call of `steps` steps (at most RING_CAP stats records per case).
 int batch_call(mrlbm_batch* b, int steps, int want_macro) {
     const int n = (int)b->h.size();
+    for (int c = 0; c < n; ++c)
+        if (b->h[c]->surf_on)
+            return bfail(b, MRLBM_EUNSUPPORTED, "case " + std::to_string(c) +
+                                                    ": surface-pressure records are taken by single-case steps only");
     if (b->schedule == MRLBM_BATCH_STREAMS && streams_call_ok(b, steps, want_macro)) return batch_call_streams(b, steps);
     for (mrlbm_handle* h : b->h) {
         if (h->ring_n + stats_in(h->cfg, h->iter + 1, h->iter + steps) > RING_CAP) {

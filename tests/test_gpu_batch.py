@@ -140,3 +140,17 @@ def test_batch_streams_calls_interleave_with_split_calls(mrlbm, prec):
         for k in ("mean_u", "rms_v", "mean_p"):
             assert np.array_equal(f1[k], f2[k]), k
     b.close()
+
+
+def test_batch_step_rejects_surface_records(mrlbm):
+    """Surface-pressure records come from single-case steps; a batch step refuses a case that
+    has them switched on instead of silently skipping them."""
+    b = mrlbm.Batch(_cfgs()[:2], precision=64)
+    b.cases[0].surface_enable()
+    with pytest.raises(mrlbm.MrlbmError) as e:
+        b.step(2)
+    assert e.value.code == 4
+    b.cases[0].surface_enable(False)
+    b.step(2)
+    assert b.status() == 0
+    b.close()
