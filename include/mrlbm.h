@@ -372,7 +372,8 @@ int mrlbm_batch_case(mrlbm_batch* b, int32_t c, mrlbm_handle** h);
 int mrlbm_batch_step(mrlbm_batch* b, int32_t nsteps, int32_t flags);
 /* tile_cfg: a 128-bit vector shape (16..21) for MRLBM_BATCH_PERSISTENT; a vector or a
  * one-tile-per-block shape (0..9) for MRLBM_BATCH_GRAPH; a one-tile-per-block shape for
- * MRLBM_BATCH_STREAMS. */
+ * MRLBM_BATCH_STREAMS.  steps_per_launch: 1..8192 (1..1024 for MRLBM_BATCH_STREAMS, whose graph
+ * holds a launch per case and step). */
 int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule, int32_t steps_per_launch);
 int mrlbm_batch_get_schedule(const mrlbm_batch* b, int32_t* tile_cfg, int32_t* schedule, int32_t* steps_per_launch);
 /* Time every shape under every schedule that takes it for trial_steps steps (rounded up to

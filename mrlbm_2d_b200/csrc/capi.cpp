@@ -27,6 +27,7 @@ using namespace mrlbm;
 namespace {
 thread_local std::string g_create_error;
 constexpr int RING_CAP = 8192;                // stats records buffered on the device
+constexpr int STREAMS_MAX_STEPS = 1024;       // steps per launch of the per-case streams schedule
 }
 
 struct mrlbm_handle {
@@ -2142,7 +2143,10 @@ int mrlbm_batch_set_schedule(mrlbm_batch* b, int32_t tile_cfg, int32_t schedule,
                           : schedule == MRLBM_BATCH_GRAPH     ? is_vec_cfg(tile_cfg) || tile
                           : schedule == MRLBM_BATCH_STREAMS   ? tile
                                                               : false;
-    if (!b || !shape_ok || steps_per_launch < 1 || steps_per_launch > RING_CAP) return MRLBM_EINVAL;
+    // a per-case streams graph holds cases x steps_per_launch step launches: bounded so that its
+    // capture and instantiation stay short
+    const int max_spl = schedule == MRLBM_BATCH_STREAMS ? STREAMS_MAX_STEPS : RING_CAP;
+    if (!b || !shape_ok || steps_per_launch < 1 || steps_per_launch > max_spl) return MRLBM_EINVAL;
     b->tile_cfg = tile_cfg;
     b->schedule = schedule;
     b->steps_per_launch = steps_per_launch;
