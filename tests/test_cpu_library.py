@@ -184,3 +184,24 @@ def test_no_device_fails_loudly(mrlbm):
     with pytest.raises(mrlbm.MrlbmError) as e:
         mrlbm.Simulation(case_small(), device=0)
     assert e.value.code in (-3, -1)
+
+
+def test_header_constants_match_the_python_layer(mrlbm):
+    """The #define values of include/mrlbm.h that the ctypes layer mirrors."""
+    text = open(os.path.join(ROOT, "include", "mrlbm.h")).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(MRLBM_\w+)\s+(-?\d+)", text)}
+    api = mrlbm.api
+    assert defs["MRLBM_BATCH_PERSISTENT"] == api.BATCH_PERSISTENT
+    assert defs["MRLBM_BATCH_GRAPH"] == api.BATCH_GRAPH
+    assert defs["MRLBM_BATCH_STREAMS"] == api.BATCH_STREAMS
+    assert defs["MRLBM_FP64"] == api.FP64 and defs["MRLBM_FP32"] == api.FP32
+
+
+def test_batch_calls_reject_a_null_batch(mrlbm):
+    """Argument checks that need no device: a NULL batch is MRLBM_EINVAL for every schedule."""
+    L = mrlbm.load_library()
+    text = open(os.path.join(ROOT, "include", "mrlbm.h")).read()
+    einval = int(re.search(r"#define\s+MRLBM_EINVAL\s+(\d+)", text).group(1))
+    for sched in (mrlbm.api.BATCH_PERSISTENT, mrlbm.api.BATCH_GRAPH, mrlbm.api.BATCH_STREAMS):
+        assert L.mrlbm_batch_set_schedule(None, 7, sched, 20) == einval
+    assert L.mrlbm_batch_step(None, 1, 0) == einval
