@@ -6,7 +6,7 @@ sums and the inlet density sums):
   * 2048 x 512, D = 80 at (320.0, 256.5), Re = 200: 20 steps;
   * 512 x 128, D = 32 at (128.0, 64.5), Re = 100 (the adjoint case): 50 steps;
   * three cases of the 64-case sweep (the smallest, the median and a 1024 x 256 one), stepped
-    through the batched kernel under both schedules.
+    through the batch under all three schedules.
 FP32 deviation form against the FP64 GPU step on the same cases (and on 16384 x 4096): the
 mean drag coefficient within |dCd|/Cd <= 1e-3 and the velocity field within 1e-3 relative L2,
 the accuracy bar the FP32 form is built to (the oracle's arithmetic is the FP64 step's, pinned
@@ -63,8 +63,8 @@ def test_adjoint_case_50_steps(mrlbm, oracle_mod):
 
 
 def test_sweep_cases_through_the_batch(mrlbm, oracle_mod):
-    """Batched kernel (persistent schedule, then graph schedule) against the oracle stepping
-    each case alone."""
+    """The batch (persistent schedule, then split graph steps, then per-case streams) against
+    the oracle stepping each case alone."""
     from mrlbm_2d_b200.config import sweep_cases
     cfgs = sweep_cases(64)
     order = sorted(range(len(cfgs)), key=lambda i: cfgs[i].nx * cfgs[i].ny)
@@ -76,10 +76,12 @@ def test_sweep_cases_through_the_batch(mrlbm, oracle_mod):
     b.step(12)
     b.set_schedule(17, mrlbm.BATCH_GRAPH, 4)
     b.step(8)
+    b.set_schedule(7, mrlbm.BATCH_STREAMS, 5)
+    b.step(10)
     assert b.status() == 0
     for c, cfg in enumerate(sel):
         o = oracle_mod.Oracle(cfg)
-        o.step(20)
+        o.step(30)
         h = b.cases[c]
         _assert_exact(h.get_state(), o.field("f"), f"sweep case {pick[c]} ({cfg.nx} x {cfg.ny})")
         it_o, fd_o, fl_o, rin_o = o.forces()
