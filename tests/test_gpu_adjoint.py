@@ -130,12 +130,13 @@ def test_torch_autograd_bridge(mrlbm):
     s.close()
 
 
-def test_fp32_adjoint_tracks_fp64_adjoint(mrlbm):
+@pytest.mark.parametrize("kw", [dict(), dict(strong_mass_bc=0, weak_mass_bc=1), dict(rotated_coordinate=0)])
+def test_fp32_adjoint_tracks_fp64_adjoint(mrlbm, kw):
     """FP32 trajectory with FP64 adjoint arithmetic against the FP64 adjoint: the directional
-    derivatives agree to 1e-3 relative."""
+    derivatives agree to 1e-3 relative (default, weak and unrotated curved-wall closures)."""
     out = {}
     for prec in (64, 32):
-        s = mrlbm.Simulation(_case(), precision=prec)
+        s = mrlbm.Simulation(_case().replace(**kw), precision=prec)
         body, uin = _params(s, 6)
         s.set_body_force(body)
         s.set_inlet_profile(uin)
