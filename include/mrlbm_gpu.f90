@@ -30,6 +30,8 @@ module mrlbm_gpu
   integer(c_int32_t), parameter :: MRLBM_LABEL15_REJECT = 0, MRLBM_LABEL15_ALLNINE = 1
   integer(c_int32_t), parameter :: MRLBM_NU_REFERENCE = 0, MRLBM_NU_DIAMETER = 1
   integer(c_int32_t), parameter :: MRLBM_INIT_REFERENCE = 0, MRLBM_INIT_NOISE = 1
+  ! batch schedules (mrlbm_batch_set_schedule)
+  integer(c_int32_t), parameter :: MRLBM_BATCH_PERSISTENT = 0, MRLBM_BATCH_GRAPH = 1, MRLBM_BATCH_STREAMS = 2
 
   ! struct mrlbm_config: the namelists DomainSize, Cylinder, Numbers, Parallel, Controls and
   ! LogicalControls (2d_mrlbm.f90:2227-2233) plus the extension switches
@@ -259,6 +261,129 @@ module mrlbm_gpu
        integer(c_int32_t), value :: nsteps, window, checkpoint_every
        real(c_double) :: J
        type(c_ptr), value :: grad_body, grad_uin
+     end function
+     integer(c_int) function mrlbm_get_tile_config(h, cfg) bind(c)
+       import
+       type(c_ptr), value :: h
+       integer(c_int32_t) :: cfg
+     end function
+     integer(c_int) function mrlbm_get_probe_nodes(h, pi, pj) bind(c)
+       import
+       type(c_ptr), value :: h
+       integer(c_int32_t), dimension(*) :: pi, pj
+     end function
+     integer(c_int) function mrlbm_get_launch_count(h, n) bind(c)
+       import
+       type(c_ptr), value :: h
+       integer(c_int64_t) :: n
+     end function
+     ! x-slabs of one domain: global columns gx0..gx1 of the case, faces exchanged by the host
+     integer(c_int) function mrlbm_create_slab(cfg, precision, device, gx0, gx1, h) bind(c)
+       import
+       type(mrlbm_config), intent(in) :: cfg
+       integer(c_int), value :: precision, device
+       integer(c_int32_t), value :: gx0, gx1
+       type(c_ptr) :: h
+     end function
+     integer(c_int) function mrlbm_halo_size(h, n_values, elem_bytes) bind(c)
+       import
+       type(c_ptr), value :: h
+       integer(c_int64_t) :: n_values
+       integer(c_int32_t) :: elem_bytes
+     end function
+     integer(c_int) function mrlbm_halo_pack(h, side, dst) bind(c)
+       import
+       type(c_ptr), value :: h, dst
+       integer(c_int32_t), value :: side
+     end function
+     integer(c_int) function mrlbm_halo_unpack(h, side, src) bind(c)
+       import
+       type(c_ptr), value :: h, src
+       integer(c_int32_t), value :: side
+     end function
+     integer(c_int) function mrlbm_step_faces(h) bind(c)
+       import
+       type(c_ptr), value :: h
+     end function
+     integer(c_int) function mrlbm_halo_pack_next(h, side, dst) bind(c)
+       import
+       type(c_ptr), value :: h, dst
+       integer(c_int32_t), value :: side
+     end function
+     integer(c_int) function mrlbm_halo_unpack_next(h, side, src) bind(c)
+       import
+       type(c_ptr), value :: h, src
+       integer(c_int32_t), value :: side
+     end function
+     ! hs: an array of n slab handles, left to right
+     integer(c_int) function mrlbm_slabs_step(hs, n, nsteps) bind(c)
+       import
+       type(c_ptr), dimension(*) :: hs
+       integer(c_int32_t), value :: n, nsteps
+     end function
+     ! batched cases: cfgs is an array of ncases configurations
+     integer(c_int) function mrlbm_batch_create(cfgs, ncases, precision, device, b) bind(c)
+       import
+       type(mrlbm_config), dimension(*), intent(in) :: cfgs
+       integer(c_int32_t), value :: ncases
+       integer(c_int), value :: precision, device
+       type(c_ptr) :: b
+     end function
+     integer(c_int) function mrlbm_batch_destroy(b) bind(c)
+       import
+       type(c_ptr), value :: b
+     end function
+     integer(c_int) function mrlbm_batch_case(b, c, h) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int32_t), value :: c
+       type(c_ptr) :: h
+     end function
+     integer(c_int) function mrlbm_batch_step(b, nsteps, flags) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int32_t), value :: nsteps, flags
+     end function
+     integer(c_int) function mrlbm_batch_set_schedule(b, tile_cfg, schedule, steps_per_launch) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int32_t), value :: tile_cfg, schedule, steps_per_launch
+     end function
+     integer(c_int) function mrlbm_batch_get_schedule(b, tile_cfg, schedule, steps_per_launch) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int32_t) :: tile_cfg, schedule, steps_per_launch
+     end function
+     integer(c_int) function mrlbm_batch_autotune(b, trial_steps, best_ms_per_step) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int32_t), value :: trial_steps
+       real(c_double) :: best_ms_per_step
+     end function
+     integer(c_int) function mrlbm_batch_set_wait_limit(b, polls) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int64_t), value :: polls
+     end function
+     integer(c_int) function mrlbm_batch_status(b) bind(c)
+       import
+       type(c_ptr), value :: b
+     end function
+     integer(c_int) function mrlbm_batch_last_error(b, buf, len) bind(c)
+       import
+       type(c_ptr), value :: b
+       character(kind=c_char), dimension(*) :: buf
+       integer(c_size_t), value :: len
+     end function
+     integer(c_int) function mrlbm_batch_launch_count(b, n) bind(c)
+       import
+       type(c_ptr), value :: b
+       integer(c_int64_t) :: n
+     end function
+     integer(c_int) function mrlbm_batch_get_stream(b, stream) bind(c)
+       import
+       type(c_ptr), value :: b
+       type(c_ptr) :: stream
      end function
   end interface
 end module mrlbm_gpu

@@ -102,3 +102,27 @@ def test_interfaces_match_header_and_library(mrlbm):
         assert name in protos, name
         assert protos[name] == n, (name, protos[name], n)
         assert hasattr(lib, name), name
+
+
+def test_module_constants_match_the_header():
+    """Every named constant of the module carries the value of the header's #define."""
+    src = _strip_comments(open(F90).read())
+    hdr = open(HDR).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(MRLBM_\w+)\s+(-?\d+)", hdr)}
+    consts = {}
+    for decl in re.findall(r"parameter\s*::\s*(.*)", src, re.I):
+        for item in decl.split(","):
+            name, _, value = item.partition("=")
+            consts[name.strip()] = int(value.strip().split("_")[0])
+    assert len(consts) >= 20
+    for name, value in consts.items():
+        assert name in defs, name
+        assert defs[name] == value, (name, defs[name], value)
+
+
+def test_module_covers_every_header_function():
+    src = _strip_comments(open(F90).read())
+    hdr = re.sub(r"/\*.*?\*/", "", open(HDR).read(), flags=re.S)
+    declared = set(re.findall(r"\b(?:int|size_t)\s+(mrlbm_\w+)\s*\(", hdr))
+    bound = set(re.findall(r"function\s+(mrlbm_\w+)\s*\(", src, re.I))
+    assert declared == bound, sorted(declared ^ bound)
