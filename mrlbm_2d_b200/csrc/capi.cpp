@@ -1875,10 +1875,13 @@ int batch_call_streams(mrlbm_batch* b, int steps) {
         BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int rc = cudaEventRecord(b->fork_ev, b->stream) == cudaSuccess ? 0 : -1;
         for (int c = 0; c < n && rc == 0; ++c) {
-            rc = cudaStreamWaitEvent(b->cstream[c], b->fork_ev, 0) == cudaSuccess ? 0 : -1;
-            if (rc == 0) rc = fp64 ? streams_launch_case<double>(b, c, steps) : streams_launch_case<float>(b, c, steps);
-            if (rc == 0) rc = cudaEventRecord(b->join_ev[c], b->cstream[c]) == cudaSuccess ? 0 : -1;
-            if (rc == 0) rc = cudaStreamWaitEvent(b->stream, b->join_ev[c], 0) == cudaSuccess ? 0 : -1;
+            if (cudaStreamWaitEvent(b->cstream[c], b->fork_ev, 0) != cudaSuccess) { rc = -1; break; }
+            rc = fp64 ? streams_launch_case<double>(b, c, steps) : streams_launch_case<float>(b, c, steps);
+            // every forked stream is joined back, also after a failed launch, so that ending the
+            // capture leaves no stream in capture mode
+            const bool joined = cudaEventRecord(b->join_ev[c], b->cstream[c]) == cudaSuccess &&
+                                cudaStreamWaitEvent(b->stream, b->join_ev[c], 0) == cudaSuccess;
+            if (rc == 0 && !joined) rc = -1;
         }
         cudaGraph_t gr = nullptr;
         cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
