@@ -154,3 +154,21 @@ def test_batch_step_rejects_surface_records(mrlbm):
     b.step(2)
     assert b.status() == 0
     b.close()
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("sched,tile", [(1, 9), (2, 7), (0, 18)])
+def test_batch_closure_variants_match_single_cases(mrlbm, prec, sched, tile):
+    """The curved-wall closure variants (weak, rho_eq, unrotated, none, no velocity
+    extrapolation) through every batch schedule, bit for bit against stepping alone."""
+    names = ["closure_weak", "closure_rhoeq", "closure_unrotated", "no_velocity_interp"]
+    cfgs = [CASES[n]() for n in names] + [CASES["reference_default_bcs"]().replace(strong_mass_bc=0)]
+    b = mrlbm.Batch(cfgs, precision=prec)
+    b.set_schedule(tile, sched, 6)
+    b.step(15)
+    assert b.status() == 0
+    for cfg, c in zip(cfgs, b.cases):
+        ref = _alone(mrlbm, cfg, prec, 15)
+        assert np.array_equal(c.get_state(), ref["f"])
+        assert np.array_equal(c.forces()[1], ref["forces"][1])
+    b.close()
