@@ -37,6 +37,33 @@ def test_all_tile_shapes_bit_identical(mrlbm, prec):
 
 
 @pytest.mark.parametrize("prec", [64, 32])
+@pytest.mark.parametrize("name", ["closure_weak", "closure_rhoeq", "closure_unrotated"])
+def test_closure_variants_same_bits_in_every_launch_structure(mrlbm, prec, name):
+    """A closure variant gives the same bits whether its wall blocks run inside the one-launch
+    step (FP32 tile shapes) or in the auxiliary launch (vector, pipelined and TMA shapes, FP64)."""
+    cfg = CASES[name]()
+    ref = None
+    for c in (0, 9, 7, 18, 22, 15, 27):
+        s = mrlbm.Simulation(cfg, precision=prec)
+        s.tile_config = c
+        try:
+            s.step(20)
+        except mrlbm.MrlbmError as e:
+            assert e.code == 4 and c >= 10 and c not in (18, 22), (c, str(e))
+            s.close()
+            continue
+        assert s.status() == 0
+        st = s.get_state()
+        fd = s.forces()[1]
+        s.close()
+        if ref is None:
+            ref = (st, fd)
+        else:
+            assert np.array_equal(st, ref[0]), f"{name}: tile shape {c}"
+            assert np.array_equal(fd, ref[1]), f"{name}: tile shape {c}"
+
+
+@pytest.mark.parametrize("prec", [64, 32])
 def test_tma_shapes_many_steps(mrlbm, oracle_mod, prec):
     """The persistent tile counter keeps its running base across many launches: a TMA shape
     stepped 300 times in separate calls matches a one-tile-per-block shape."""
