@@ -172,3 +172,22 @@ def test_batch_closure_variants_match_single_cases(mrlbm, prec, sched, tile):
         assert np.array_equal(c.get_state(), ref["f"])
         assert np.array_equal(c.forces()[1], ref["forces"][1])
     b.close()
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_batch_streams_statistics_window_inside_calls(mrlbm, prec):
+    """A statistics window that opens and closes inside replayed calls: each replay derives
+    which of its steps keep a record, and in which ring slot, from the uploaded call state."""
+    cfgs = [c.replace(statsbegin=10, statsend=25) for c in _cfgs()]
+    b = mrlbm.Batch(cfgs, precision=prec)
+    b.set_schedule(9, mrlbm.BATCH_STREAMS, 7)
+    b.step(7)                                    # the periodic case's overrides: split steps
+    b.step(23)                                   # replays (7, 7, 7) and a 2-step call
+    assert b.status() == 0
+    for cfg, c in zip(cfgs, b.cases):
+        ref = _alone(mrlbm, cfg, prec, 30)
+        assert np.array_equal(c.get_state(), ref["f"])
+        it, fd, fl, rin = c.forces()
+        assert np.array_equal(it, ref["forces"][0]) and it[0] == 10 and it[-1] == 25
+        assert np.array_equal(fd, ref["forces"][1]) and np.array_equal(rin, ref["forces"][3])
+    b.close()
