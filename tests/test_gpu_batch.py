@@ -191,3 +191,21 @@ def test_batch_streams_statistics_window_inside_calls(mrlbm, prec):
         assert np.array_equal(it, ref["forces"][0]) and it[0] == 10 and it[-1] == 25
         assert np.array_equal(fd, ref["forces"][1]) and np.array_equal(rin, ref["forces"][3])
     b.close()
+
+
+def test_batch_streams_ring_drains_between_replays(mrlbm):
+    """More records than the device ring holds (8192): the streams schedule drains the ring
+    between replays and the history still equals stepping alone."""
+    cfgs = [CASES["reference_default_bcs"](), CASES["freeslip_label15"]()]
+    b = mrlbm.Batch(cfgs, precision=32)
+    b.set_schedule(0, mrlbm.BATCH_STREAMS, 100)
+    b.step(8300)
+    assert b.status() == 0
+    for cfg, c in zip(cfgs, b.cases):
+        ref = _alone(mrlbm, cfg, 32, 8300)
+        it, fd, fl, rin = c.forces()
+        assert len(it) == 8300
+        assert np.array_equal(it, ref["forces"][0])
+        assert np.array_equal(fd, ref["forces"][1]) and np.array_equal(fl, ref["forces"][2])
+        assert np.array_equal(c.get_state(), ref["f"])
+    b.close()
