@@ -2,6 +2,7 @@
 
     python -m mrlbm_2d_b200.batch_sweep [--cases 64] [--steps 20000] [--seq-steps 2000]
                                         [--precision 32] [--trial-steps 50]
+    python -m mrlbm_2d_b200.batch_sweep --compare-fp64 20000     # FP32 against FP64 mean drag per case
 
 The cases are config.sweep_cases(n): nx uniform in [256, 1024] (multiples of 32), ny = nx/4,
 D = ny/5 at (nx/5, ny/2 + 0.5), Re uniform in [40, 200], U = 0.05, seeded.  The batch is
@@ -87,6 +88,36 @@ def sweep(cases=64, steps=20000, seq_steps=2000, precision=32, trial_steps=50, s
     return out
 
 
+def precision_check(cases=64, steps=20000, seed=4242, trial_steps=10):
+    """FP32 against FP64 on every case of the sweep, each precision stepped as one batch: the
+    mean drag coefficient over the second half of `steps` steps per case, and its relative
+    difference (cases whose density went non-positive in either precision are left out)."""
+    cfgs = sweep_cases(cases, seed=seed)
+    cd = {}
+    for prec in (64, 32):
+        b = api.Batch(cfgs, precision=prec)
+        b.autotune(trial_steps=trial_steps)
+        b.step(steps)
+        vals = []
+        for cfg, c in zip(cfgs, b.cases):
+            _, fd, _, _ = c.forces()
+            ok = c.status() == 0 and len(fd) > 1
+            norm = 0.5 * cfg.rho_infty * cfg.uo ** 2 * (2.0 * cfg.r_c)
+            vals.append(float(fd[len(fd) // 2:].mean() / norm) if ok else float("nan"))
+        cd[prec] = np.array(vals)
+        b.close()
+    good = np.isfinite(cd[64]) & np.isfinite(cd[32])
+    rel = np.full(len(cfgs), np.nan)
+    rel[good] = np.abs(cd[32][good] - cd[64][good]) / np.abs(cd[64][good])
+    worst = int(np.nanargmax(rel))
+    return {"cases": cases, "steps": steps, "compared_cases": int(good.sum()),
+            "rel_err_Cd_max": float(np.nanmax(rel)), "rel_err_Cd_median": float(np.nanmedian(rel)),
+            "cases_above_1e-3": int(np.sum(rel[good] > 1e-3)),
+            "worst_case": {"case": worst, "nx": cfgs[worst].nx, "ny": cfgs[worst].ny, "Re": round(cfgs[worst].Re, 2),
+                           "Cd_fp64": float(cd[64][worst]), "Cd_fp32": float(cd[32][worst])},
+            "Cd_fp64_range": [float(cd[64][good].min()), float(cd[64][good].max())]}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--cases", type=int, default=64)
@@ -96,7 +127,13 @@ def main(argv=None):
     ap.add_argument("--trial-steps", type=int, default=50)
     ap.add_argument("--seed", type=int, default=4242)
     ap.add_argument("--no-sequential", action="store_true", help="skip the one-case-at-a-time baseline")
+    ap.add_argument("--compare-fp64", type=int, default=0, metavar="STEPS",
+                    help="instead of timing: FP32 against FP64 mean drag on every case over STEPS steps")
     a = ap.parse_args(argv)
+    if a.compare_fp64 > 0:
+        out = precision_check(a.cases, a.compare_fp64, a.seed)
+        print(json.dumps(out), flush=True)
+        return out
     out = sweep(a.cases, a.steps, a.seq_steps, a.precision, a.trial_steps, a.seed, not a.no_sequential)
     print(json.dumps(out), flush=True)
     return out
