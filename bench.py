@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--adjoint-directions", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--batch-seq-steps", type=int, default=200)
+    ap.add_argument("--batch-precision-steps", type=int, default=40000,
+                    help="FP32 against FP64 mean drag on every sweep case over this many steps (0: skip)")
     ap.add_argument("--decomp", choices=["replicas", "slabs"], default="replicas",
                     help="replicas: one independent case per rank (weak scaling); slabs: the 16384 x 4096 "
                          "case split into x-slabs across the ranks with the halo exchange (strong scaling)")
@@ -637,7 +639,8 @@ def main():
 def run_studies(args, peak):
     """The rest of the benchmark metric, measured in the same run: FP32 against FP64 on the
     2048 x 512 case (and with field statistics on 16384 x 4096), the adjoint's cost and its check
-    against central differences on 512 x 128, and the 64-case batched sweep."""
+    against central differences on 512 x 128, and the 64-case batched sweep with its FP32
+    against FP64 mean drag per case."""
     out = {}
     from mrlbm_2d_b200 import adjoint_check, batch_sweep, precision_study
     t0 = time.perf_counter()
@@ -692,6 +695,9 @@ def run_studies(args, peak):
                         "hbm_gbs_alg": gbs, "frac_of_peak": gbs / peak, "bytes_per_lu": BYTES_PER_LU[32],
                         "sequential_mlups": b["sequential"]["mlups"], "speedup_vs_sequential": b["speedup"],
                         "unstable_cases": len(b["unstable_cases"]), "l2": "working set 554 MB (4.4x the L2), no flush"}
+        if args.batch_precision_steps > 0:
+            out["batch"]["precision"] = batch_sweep.precision_check(64, args.batch_precision_steps)
+            out["batch"]["precision"]["targets"] = {"rel_err_Cd": 1e-3}
         out["batch"]["seconds"] = time.perf_counter() - t0
     except Exception as ex:
         out["batch"] = {"error": str(ex)}
